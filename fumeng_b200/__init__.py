@@ -1,0 +1,214 @@
+"""fumeng_b200: B200 path-tracing core behind a C-ABI (ctypes binding).
+
+The product is the shared library ``libfumeng_b200.so`` (CUDA kernels for sm_100a plus
+the C++ host layer); this module only binds its C entry points (include/fumeng_b200.h)
+for Python callers such as the tests and bench.py.  Every call goes to the CUDA
+library; there is no CPU fallback, and loading fails loudly when the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libfumeng_b200.so"
+
+FM_OK, FM_ERR_INVALID, FM_ERR_OOM, FM_ERR_CUDA, FM_ERR_QUEUE_OVERFLOW, FM_ERR_TIMEOUT, FM_ERR_NO_DEVICE = range(7)
+FM_FLAG_DEVICE_PTRS = 1
+FM_WRAP_REPEAT, FM_WRAP_CLAMP = 0, 1
+FM_FILTER_LINEAR, FM_FILTER_NEAREST = 0, 1
+FM_MAT_LAMBERT, FM_MAT_SPEC_REFL, FM_MAT_SPEC_TRANS, FM_MAT_DISNEY = 0, 1, 2, 3
+FM_LIGHT_ENV, FM_LIGHT_DIRECTIONAL = 0, 1
+FM_CAMERA_PINHOLE, FM_CAMERA_THIN_LENS = 0, 1
+FM_MODE_MEGAKERNEL, FM_MODE_WAVEFRONT = 0, 1
+
+_f3 = C.c_float * 3
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int32)
+_u8p = C.POINTER(C.c_uint8)
+
+
+class TexRef(C.Structure):
+    _fields_ = [("texture", C.c_int32), ("value", _f3)]
+
+
+class TextureDesc(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("texels", _fp), ("wrap_u", C.c_int32),
+                ("wrap_v", C.c_int32), ("filter", C.c_int32)]
+
+
+MAT_PARAMS = ["basecolor", "metallic", "specular", "specular_tint", "roughness", "anisotropic", "sheen",
+              "sheen_tint", "clearcoat", "clearcoat_gloss", "spec_trans", "spec_trans_roughness", "diff_trans",
+              "flatness", "ior"]
+
+
+class MaterialDesc(C.Structure):
+    _fields_ = ([("type", C.c_int32), ("thin", C.c_int32)] + [(p, TexRef) for p in MAT_PARAMS] +
+                [("reflect_color", _f3), ("refract_color", _f3), ("eta_i", C.c_float), ("eta_t", C.c_float),
+                 ("color", _f3), ("cond_eta_i", _f3), ("cond_eta_t", _f3), ("cond_k", _f3),
+                 ("vattr_offset", C.c_int32)])
+
+
+class LightDesc(C.Structure):
+    _fields_ = [("type", C.c_int32), ("texture", C.c_int32), ("rotation", _f3), ("factor", C.c_float),
+                ("radiance", _f3), ("direction", _f3)]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("num_objects", C.c_int64), ("obj_material", _ip), ("obj_emission", _fp),
+                ("num_triangles", C.c_int64), ("tri_pos", _fp), ("tri_normal", _fp), ("tri_has_normal", _u8p),
+                ("tri_uv", _fp), ("tri_object", _ip), ("tri_vattr", _fp), ("vattr_dim", C.c_int32),
+                ("num_rects", C.c_int64), ("rect_pts", _fp), ("rect_object", _ip),
+                ("num_spheres", C.c_int64), ("sphere_radius", _fp), ("sphere_xform", _fp), ("sphere_object", _ip),
+                ("num_materials", C.c_int32), ("materials", C.POINTER(MaterialDesc)),
+                ("num_textures", C.c_int32), ("textures", C.POINTER(TextureDesc)),
+                ("num_lights", C.c_int32), ("lights", C.POINTER(LightDesc))]
+
+
+class Camera(C.Structure):
+    _fields_ = [("type", C.c_int32), ("pos", _f3), ("look_at", _f3), ("up", _f3), ("fov", C.c_float),
+                ("aspect", C.c_float), ("focal_distance", C.c_float), ("lens_radius", C.c_float)]
+
+
+class RenderParams(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32), ("depth", C.c_int32),
+                ("direct_loop", C.c_int32), ("rr_depth", C.c_int32), ("rr_coef", C.c_float), ("seed", C.c_uint64),
+                ("mode", C.c_int32), ("sample_offset", C.c_int32)]
+
+
+class RenderStats(C.Structure):
+    _fields_ = [("paths", C.c_int64), ("closest_rays", C.c_int64), ("shadow_rays", C.c_int64),
+                ("bounces", C.c_int64), ("nan_samples", C.c_int64), ("kernel_ms", C.c_double)]
+
+
+class FumengError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"fumeng_b200 error {status}: {message}")
+        self.status = status
+
+
+_lib = None
+
+
+def load_library() -> C.CDLL:
+    """Load libfumeng_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = Path(os.environ.get("FUMENG_B200_LIB", LIB_PATH))
+    if not path.exists():
+        raise FileNotFoundError(f"{path} is missing: build it with `python -m fumeng_b200.build`")
+    lib = C.CDLL(str(path))
+    vp = C.c_void_p
+    sig = {
+        "fm_ctx_create": ([C.c_int, C.POINTER(vp)], C.c_int),
+        "fm_ctx_destroy": ([vp], None),
+        "fm_last_error": ([vp], C.c_char_p),
+        "fm_scene_create": ([vp, C.POINTER(SceneDesc), C.POINTER(vp)], C.c_int),
+        "fm_scene_destroy": ([vp, vp], C.c_int),
+        "fm_scene_bvh_stats": ([vp, vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32),
+                                C.POINTER(C.c_double)], C.c_int),
+        "fm_trace_closest": ([vp, vp, vp, C.c_int64, vp, vp, C.c_int32], C.c_int),
+        "fm_trace_any": ([vp, vp, vp, C.c_int64, vp, C.c_int32], C.c_int),
+        "fm_render": ([vp, vp, C.POINTER(Camera), C.POINTER(RenderParams), vp, vp, vp, C.c_int32,
+                       C.POINTER(RenderStats)], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+EXPORTED_SYMBOLS = ["fm_ctx_create", "fm_ctx_destroy", "fm_last_error", "fm_scene_create", "fm_scene_destroy",
+                    "fm_scene_bvh_stats", "fm_trace_closest", "fm_trace_any", "fm_render"]
+
+
+def _ptr(a, ctype=C.c_void_p):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctype)
+
+
+class Context:
+    """One CUDA device context (owns a stream); not thread-safe."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        st = self.lib.fm_ctx_create(device, C.byref(h))
+        if st != FM_OK:
+            raise FumengError(st, "fm_ctx_create failed (no usable CUDA device?)")
+        self.h = h
+
+    def check(self, st: int) -> None:
+        if st != FM_OK:
+            raise FumengError(st, self.lib.fm_last_error(self.h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.fm_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def create_scene(self, desc_holder) -> "Scene":
+        h = C.c_void_p()
+        self.check(self.lib.fm_scene_create(self.h, C.byref(desc_holder.desc), C.byref(h)))
+        return Scene(self, h, desc_holder)
+
+
+class Scene:
+    def __init__(self, ctx: Context, h, holder):
+        self.ctx, self.h, self._holder = ctx, h, holder
+
+    def destroy(self) -> None:
+        if self.h:
+            self.ctx.check(self.ctx.lib.fm_scene_destroy(self.ctx.h, self.h))
+            self.h = None
+
+    def bvh_stats(self) -> dict:
+        n, p, d, ms = C.c_int64(), C.c_int64(), C.c_int32(), C.c_double()
+        self.ctx.check(self.ctx.lib.fm_scene_bvh_stats(self.ctx.h, self.h, C.byref(n), C.byref(p), C.byref(d),
+                                                       C.byref(ms)))
+        return {"nodes": n.value, "prims": p.value, "depth": d.value, "build_ms": ms.value}
+
+    def trace_closest(self, rays: np.ndarray):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        obj = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        self.ctx.check(self.ctx.lib.fm_trace_closest(self.ctx.h, self.h, _ptr(rays), n, _ptr(obj), _ptr(t), 0))
+        return obj, t
+
+    def trace_any(self, rays: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        occ = np.empty(n, np.uint8)
+        self.ctx.check(self.ctx.lib.fm_trace_any(self.ctx.h, self.h, _ptr(rays), n, _ptr(occ), 0))
+        return occ
+
+    def render(self, camera: Camera, params: RenderParams, want_aov: bool = True):
+        """Returns (rgb, albedo, normal, stats) as HxWx3 float32 arrays (row 0 = top)."""
+        h, w = params.height, params.width
+        rgb = np.empty((h, w, 3), np.float32)
+        alb = np.empty((h, w, 3), np.float32) if want_aov else None
+        nrm = np.empty((h, w, 3), np.float32) if want_aov else None
+        stats = RenderStats()
+        self.ctx.check(self.ctx.lib.fm_render(self.ctx.h, self.h, C.byref(camera), C.byref(params), _ptr(rgb),
+                                              _ptr(alb), _ptr(nrm), 0, C.byref(stats)))
+        return rgb, alb, nrm, stats

@@ -1,0 +1,187 @@
+// 8-wide compressed BVH: node format and traversal.
+//
+// Node (80 bytes = 5 x uint4), one per internal node of the wide tree:
+//   w0: origin p.xyz (float), byte-packed [ex, ey, ez, imask]
+//   w1: child_base, prim_base, meta[0..3], meta[4..7]
+//   w2: qlo_x[0..7], qlo_y[0..7]      w3: qlo_z[0..7], qhi_x[0..7]
+//   w4: qhi_y[0..7], qhi_z[0..7]
+// Child i's box is p + q * 2^(e-127) per axis; the quantized box is rounded outward, so
+// it always contains the exact box.  imask bit i marks child i as an internal node; the
+// internal children are stored contiguously from child_base in slot order.  A leaf child
+// holds 1-3 primitives at prim_base + (meta & 31); meta >> 5 is the unary count
+// (1 -> 0b001, 2 -> 0b011, 3 -> 0b111).  Empty slots have meta 0.
+//
+// Slots are assigned by octant of the child's centroid relative to the node centre at
+// build time, so that visiting slots in the order key = slot ^ ray_octant (highest
+// first) is approximately front to back.
+//
+// Traversal keeps a short stack of node groups (child_base, hit bits << 24 | imask),
+// one entry per tree level at most, and tests each node's leaf primitives as soon as
+// the node is intersected.
+#pragma once
+#include "fm_common.cuh"
+#include "fm_scene.cuh"
+#include "fm_triangle.cuh"
+
+namespace fm {
+
+constexpr int kTraversalStack = 32;   // the builder rejects trees deeper than this
+constexpr uint32_t kSphereFlag = 0x80000000u;
+
+struct Hit {
+    float t;
+    int32_t prim;   // -1 on a miss
+    float b1, b2;   // barycentrics of v1 and v2 (triangles)
+};
+
+FM_D float byte_f(uint32_t w, int k) { return (float)((w >> (8 * k)) & 0xffu); }
+
+// Intersect the 8 children of `node`; returns the internal hit bits (<< 24, keyed by
+// slot ^ oct) | imask in node_bits, and the primitive hit bits in prim_bits.
+FM_D void intersect_node(const uint4* __restrict__ nodes, int node, f3 o, f3 idir, uint32_t oct, float tmin,
+                         float tmax, uint32_t& child_base, uint32_t& node_bits, uint32_t& prim_base,
+                         uint32_t& prim_bits)
+{
+    const uint4* np = nodes + 5 * (size_t)node;
+    const uint4 w0 = __ldg(np + 0);
+    const uint4 w1 = __ldg(np + 1);
+    const uint4 w2 = __ldg(np + 2);
+    const uint4 w3 = __ldg(np + 3);
+    const uint4 w4 = __ldg(np + 4);
+    const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
+    const uint32_t ex = w0.w & 0xffu, ey = (w0.w >> 8) & 0xffu, ez = (w0.w >> 16) & 0xffu;
+    const uint32_t imask = w0.w >> 24;
+    const float ax = __uint_as_float(ex << 23) * idir.x;
+    const float ay = __uint_as_float(ey << 23) * idir.y;
+    const float az = __uint_as_float(ez << 23) * idir.z;
+    const float bx = (px - o.x) * idir.x;
+    const float by = (py - o.y) * idir.y;
+    const float bz = (pz - o.z) * idir.z;
+    uint32_t nbits = 0, pbits = 0;
+    const float tfar_limit = tmax;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const uint32_t wm = i < 4 ? w1.z : w1.w;
+        const uint32_t meta = (wm >> (8 * (i & 3))) & 0xffu;
+        if (meta == 0) continue;
+        const int k = i & 3;
+        const float qlx = byte_f(i < 4 ? w2.x : w2.y, k), qly = byte_f(i < 4 ? w2.z : w2.w, k);
+        const float qlz = byte_f(i < 4 ? w3.x : w3.y, k), qhx = byte_f(i < 4 ? w3.z : w3.w, k);
+        const float qhy = byte_f(i < 4 ? w4.x : w4.y, k), qhz = byte_f(i < 4 ? w4.z : w4.w, k);
+        const float tx0 = fmaf(qlx, ax, bx), tx1 = fmaf(qhx, ax, bx);
+        const float ty0 = fmaf(qly, ay, by), ty1 = fmaf(qhy, ay, by);
+        const float tz0 = fmaf(qlz, az, bz), tz1 = fmaf(qhz, az, bz);
+        const float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
+        const float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tfar_limit));
+        // Widen the interval by a few ulps so that rounding in the slab arithmetic can
+        // never reject a box that the exact box test accepts.
+        if (tn <= tf * 1.0000010f + 1e-30f) {
+            if ((imask >> i) & 1u)
+                nbits |= 1u << (24 + (i ^ oct));
+            else
+                pbits |= (meta >> 5) << (meta & 31u);
+        }
+    }
+    child_base = w1.x;
+    prim_base = w1.y;
+    node_bits = nbits | imask;
+    prim_bits = pbits;
+}
+
+// Leaf primitive test.  Closest-hit acceptance follows the reference: a triangle of a
+// mesh is accepted when IntersectTriangle(t_min, t_best) succeeds and not
+// (t > t_best || t <= 0) (triangle.cpp:211-225, bvh_aggregate.cpp:108-115); rectangle
+// halves skip the second check (rectangle.cpp:42-56); spheres use the inclusive range
+// (sphere.cpp:116-127).
+template <bool ANY>
+FM_D bool test_prim(const DevScene& S, const RayPre& rp, f3 o, f3 d, int slot, float tmin, float& tbest,
+                    Hit& hit)
+{
+    const float4 a = __ldg(S.leaf + 3 * (size_t)slot);
+    const uint32_t tag = __float_as_uint(a.w);
+    if (tag & kSphereFlag) {
+        const int sidx = (int)__float_as_uint(a.x);
+        const SphereDev& sp = S.spheres[sidx];
+        float t;
+        if (!intersect_sphere(sp.w2o, sp.radius, o, d, tmin, tbest, t)) return false;
+        if (!ANY) {
+            tbest = t;
+            hit.t = t;
+            hit.prim = (int)(tag & ~kSphereFlag);
+            hit.b1 = hit.b2 = 0.0f;
+        }
+        return true;
+    }
+    const float4 b = __ldg(S.leaf + 3 * (size_t)slot + 1);
+    const float4 c = __ldg(S.leaf + 3 * (size_t)slot + 2);
+    float t, b0, b1, b2;
+    if (!intersect_triangle(rp, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, f3{c.x, c.y, c.z}, tmin, tbest, t, b0, b1, b2))
+        return false;
+    if (ANY) return true;
+    const int prim = (int)tag;
+    if (prim < S.num_tris && (t > tbest || t <= 0.0f)) return false;
+    tbest = t;
+    hit.t = t;
+    hit.prim = prim;
+    hit.b1 = b1;
+    hit.b2 = b2;
+    return true;
+}
+
+// Closest hit (ANY = false) or occlusion (ANY = true) query.  Returns true on a hit.
+// *overflow is set when the traversal stack would overflow (the builder bounds the tree
+// depth so that this cannot happen for trees it accepted).
+template <bool ANY>
+FM_D bool trace_ray(const DevScene& S, f3 o, f3 d, float tmin, float tmax, Hit& hit, uint32_t* overflow)
+{
+    hit.t = tmax;
+    hit.prim = -1;
+    if (S.num_nodes == 0) return false;
+    const RayPre rp = ray_pre(o, d);
+    const float sdx = fabsf(d.x) < 1e-20f ? copysignf(1e-20f, d.x) : d.x;
+    const float sdy = fabsf(d.y) < 1e-20f ? copysignf(1e-20f, d.y) : d.y;
+    const float sdz = fabsf(d.z) < 1e-20f ? copysignf(1e-20f, d.z) : d.z;
+    const f3 idir = f3{1.0f / sdx, 1.0f / sdy, 1.0f / sdz};
+    const uint32_t oct = (d.x >= 0.0f ? 1u : 0u) | (d.y >= 0.0f ? 2u : 0u) | (d.z >= 0.0f ? 4u : 0u);
+    uint2 stack[kTraversalStack];
+    int sp = 0;
+    // Virtual parent of the root: one internal child in slot 0.
+    uint2 ngrp = make_uint2(0u, (1u << (24 + (0u ^ oct))) | 1u);
+    uint2 pgrp = make_uint2(0u, 0u);
+    float tbest = tmax;
+    bool found = false;
+    for (;;) {
+        if (ngrp.y > 0x00ffffffu) {
+            const uint32_t key = 31u - __clz(ngrp.y) - 24u;
+            ngrp.y &= ~(1u << (24u + key));
+            const uint32_t slot = key ^ oct;
+            const uint32_t imask = ngrp.y & 0xffu;
+            const int child = (int)(ngrp.x + __popc(imask & ((1u << slot) - 1u)));
+            if (ngrp.y > 0x00ffffffu) {
+                if (sp < kTraversalStack)
+                    stack[sp++] = ngrp;
+                else if (overflow)
+                    atomicOr(overflow, 1u);
+            }
+            uint32_t cb, nb, pb, pbits;
+            intersect_node(S.nodes, child, o, idir, oct, tmin, tbest, cb, nb, pb, pbits);
+            ngrp = make_uint2(cb, nb);
+            pgrp = make_uint2(pb, pbits);
+        }
+        while (pgrp.y != 0u) {
+            const int bit = __ffs(pgrp.y) - 1;
+            pgrp.y &= pgrp.y - 1u;
+            if (test_prim<ANY>(S, rp, o, d, (int)pgrp.x + bit, tmin, tbest, hit)) {
+                found = true;
+                if (ANY) return true;
+            }
+        }
+        if (ngrp.y <= 0x00ffffffu) {
+            if (sp == 0) break;
+            ngrp = stack[--sp];
+        }
+    }
+    return found;
+}
+
+}  // namespace fm

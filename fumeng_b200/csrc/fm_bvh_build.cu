@@ -1,0 +1,1103 @@
+// Device BVH construction: binned SAH (top-down, breadth first) into a binary tree, an
+// exact-SAH sweep for clusters of <= 32 primitives, then collapse into the 8-wide
+// compressed node format of fm_bvh.cuh.
+//
+// The reference builds a median-split binary BVH on the CPU (accelerator/
+// bvh_aggregate.cpp:38-79, leaf <= 5).  The tree shape does not change closest-hit
+// results (every primitive whose exact box the ray enters is tested, and the
+// primitive test is the reference's), so the device builder is free to optimise for
+// traversal cost.
+//
+// Determinism: bins are accumulated with integer and order-preserving float atomics,
+// whose results do not depend on scheduling; the partition is a stable scatter driven by
+// a device-wide exclusive scan.  Node numbering uses atomic counters and therefore
+// varies between builds, which changes no query result.
+#include "fm_bvh_build.h"
+
+#include <vector>
+
+namespace fm {
+
+namespace {
+
+constexpr int kBins = 16;
+constexpr int kSmall = 32;     // clusters of <= kSmall primitives are built by one thread
+constexpr int kLeafMax = 3;    // primitives per leaf (a wide-node leaf slot holds <= 3)
+constexpr int kScanBlock = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanBlock * kScanItems;
+
+struct BNode {
+    float lo[3], hi[3];
+    int32_t a, b;   // internal: children; leaf: a = ~begin (< 0), b = count
+};
+
+struct Task {
+    int32_t node, begin, count, pad;
+    float cmin[3], cmax[3];
+};
+
+// Per-task bins: for each axis and bin, count, box (lo/hi) and centroid box, as ordered
+// uints for atomic min/max.
+struct Bins {
+    uint32_t cnt[3][kBins];
+    uint32_t lo[3][kBins][3], hi[3][kBins][3];
+    uint32_t clo[3][kBins][3], chi[3][kBins][3];
+};
+
+struct Split {
+    int32_t axis;   // -1: median split by position
+    int32_t bin;    // left = bins [0, bin]
+    int32_t nl;
+    int32_t child_task[2];   // -1 when the child is a small cluster
+};
+
+FM_D int bin_of(float c, float cmin, float scale)
+{
+    int b = (int)((c - cmin) * scale);
+    return b < 0 ? 0 : (b >= kBins ? kBins - 1 : b);
+}
+
+FM_HD float half_area(const float* lo, const float* hi)
+{
+    const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+    if (!(dx >= 0.0f) || !(dy >= 0.0f) || !(dz >= 0.0f)) return 0.0f;
+    return dx * dy + dy * dz + dz * dx;
+}
+
+__global__ void k_init_bins(Bins* bins, int ntasks)
+{
+    const int t = blockIdx.x;
+    if (t >= ntasks) return;
+    uint32_t* w = reinterpret_cast<uint32_t*>(bins + t);
+    const int nw = sizeof(Bins) / 4;
+    const int ncnt = 3 * kBins;
+    const int nlo = ncnt + 3 * kBins * 3;
+    const int nhi = nlo + 3 * kBins * 3;
+    const int nclo = nhi + 3 * kBins * 3;
+    for (int i = threadIdx.x; i < nw; i += blockDim.x) {
+        uint32_t v;
+        if (i < ncnt) v = 0u;
+        else if (i < nlo) v = 0xffffffffu;   // min slots start at +max
+        else if (i < nhi) v = 0u;            // max slots start at -max
+        else if (i < nclo) v = 0xffffffffu;
+        else v = 0u;
+        w[i] = v;
+    }
+}
+
+__global__ void k_root_bounds(const float4* __restrict__ plo, const float4* __restrict__ phi, int n, uint32_t* out)
+{
+    // out: [0..2] centroid min, [3..5] centroid max, [6..8] box min, [9..11] box max
+    float cmn[3] = {kRealMax, kRealMax, kRealMax}, cmx[3] = {-kRealMax, -kRealMax, -kRealMax};
+    float bmn[3] = {kRealMax, kRealMax, kRealMax}, bmx[3] = {-kRealMax, -kRealMax, -kRealMax};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 l = plo[i], h = phi[i];
+        const float c[3] = {0.5f * (l.x + h.x), 0.5f * (l.y + h.y), 0.5f * (l.z + h.z)};
+        const float lv[3] = {l.x, l.y, l.z}, hv[3] = {h.x, h.y, h.z};
+        for (int a = 0; a < 3; ++a) {
+            cmn[a] = fminf(cmn[a], c[a]);
+            cmx[a] = fmaxf(cmx[a], c[a]);
+            bmn[a] = fminf(bmn[a], lv[a]);
+            bmx[a] = fmaxf(bmx[a], hv[a]);
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        for (int off = 16; off > 0; off >>= 1) {
+            cmn[a] = fminf(cmn[a], __shfl_xor_sync(0xffffffffu, cmn[a], off));
+            cmx[a] = fmaxf(cmx[a], __shfl_xor_sync(0xffffffffu, cmx[a], off));
+            bmn[a] = fminf(bmn[a], __shfl_xor_sync(0xffffffffu, bmn[a], off));
+            bmx[a] = fmaxf(bmx[a], __shfl_xor_sync(0xffffffffu, bmx[a], off));
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(out + a, f2ord(cmn[a]));
+            atomicMax(out + 3 + a, f2ord(cmx[a]));
+            atomicMin(out + 6 + a, f2ord(bmn[a]));
+            atomicMax(out + 9 + a, f2ord(bmx[a]));
+        }
+    }
+}
+
+__global__ void k_make_root(const uint32_t* rb, int n, BNode* nodes, Task* tasks, int32_t* pos_task,
+                            int32_t* small_list, int32_t* counters)
+{
+    // counters: [0] node count, [1] next-level task count, [2] small-cluster count
+    BNode root;
+    for (int a = 0; a < 3; ++a) {
+        root.lo[a] = ord2f(rb[6 + a]);
+        root.hi[a] = ord2f(rb[9 + a]);
+    }
+    root.a = 0;
+    root.b = 0;
+    nodes[0] = root;
+    counters[0] = 1;
+    if (n <= kSmall) {
+        small_list[0] = 0;   // node
+        small_list[1] = 0;   // begin
+        small_list[2] = n;   // count
+        counters[2] = 1;
+        counters[1] = 0;
+    } else {
+        Task t;
+        t.node = 0;
+        t.begin = 0;
+        t.count = n;
+        t.pad = 0;
+        for (int a = 0; a < 3; ++a) {
+            t.cmin[a] = ord2f(rb[a]);
+            t.cmax[a] = ord2f(rb[3 + a]);
+        }
+        tasks[0] = t;
+        counters[1] = 1;
+        counters[2] = 0;
+    }
+}
+
+__global__ void k_fill_pos_task(int32_t* pos_task, int32_t* pidx, int n, int root_task)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        pos_task[i] = root_task;
+        pidx[i] = i;
+    }
+}
+
+// Binning.  Each block covers a contiguous range of positions; when the whole range
+// belongs to one task (the common case in the upper levels) the block accumulates in
+// shared memory and merges once, otherwise it falls back to global atomics.
+__global__ void k_bin(const float4* __restrict__ plo, const float4* __restrict__ phi, const int32_t* __restrict__ pidx,
+                      const int32_t* __restrict__ pos_task, const Task* __restrict__ tasks, Bins* bins, int n)
+{
+    __shared__ Bins sb;
+    __shared__ int s_task;
+    const int begin = blockIdx.x * blockDim.x * 4;
+    if (begin >= n) return;
+    const int end = min(n, begin + (int)blockDim.x * 4);
+    if (threadIdx.x == 0) {
+        const int t0 = pos_task[begin], t1 = pos_task[end - 1];
+        // A run of positions between two of the same task belongs to that task (task
+        // ranges are contiguous); finished positions (-1) can surround active ones.
+        s_task = (t0 == t1 && t0 >= 0) ? t0 : -2;
+    }
+    __syncthreads();
+    const int shared_task = s_task;
+    const bool use_smem = shared_task >= 0;
+    if (use_smem) {
+        uint32_t* w = reinterpret_cast<uint32_t*>(&sb);
+        const int nw = sizeof(Bins) / 4;
+        const int ncnt = 3 * kBins;
+        const int nlo = ncnt + 3 * kBins * 3;
+        const int nhi = nlo + 3 * kBins * 3;
+        const int nclo = nhi + 3 * kBins * 3;
+        for (int i = threadIdx.x; i < nw; i += blockDim.x)
+            w[i] = (i < ncnt) ? 0u : (i < nlo ? 0xffffffffu : (i < nhi ? 0u : (i < nclo ? 0xffffffffu : 0u)));
+        __syncthreads();
+    }
+    for (int i = begin + threadIdx.x; i < end; i += blockDim.x) {
+        const int t = pos_task[i];
+        if (t < 0) continue;
+        const Task& tk = tasks[t];
+        const int p = pidx[i];
+        const float4 l = plo[p], h = phi[p];
+        const float lv[3] = {l.x, l.y, l.z}, hv[3] = {h.x, h.y, h.z};
+        Bins* B = use_smem ? &sb : bins + t;
+        for (int a = 0; a < 3; ++a) {
+            const float ext = tk.cmax[a] - tk.cmin[a];
+            if (!(ext > 0.0f)) continue;
+            const float c = 0.5f * (lv[a] + hv[a]);
+            const float scale = (float)kBins * (1.0f - 1e-6f) / ext;
+            const int b = bin_of(c, tk.cmin[a], scale);
+            atomicAdd(&B->cnt[a][b], 1u);
+            for (int k = 0; k < 3; ++k) {
+                const float ck = 0.5f * (lv[k] + hv[k]);
+                atomicMin(&B->lo[a][b][k], f2ord(lv[k]));
+                atomicMax(&B->hi[a][b][k], f2ord(hv[k]));
+                atomicMin(&B->clo[a][b][k], f2ord(ck));
+                atomicMax(&B->chi[a][b][k], f2ord(ck));
+            }
+        }
+    }
+    if (use_smem) {
+        __syncthreads();
+        Bins* G = bins + shared_task;
+        for (int a = 0; a < 3; ++a)
+            for (int b = threadIdx.x; b < kBins; b += blockDim.x) {
+                if (sb.cnt[a][b] == 0u) continue;
+                atomicAdd(&G->cnt[a][b], sb.cnt[a][b]);
+                for (int k = 0; k < 3; ++k) {
+                    atomicMin(&G->lo[a][b][k], sb.lo[a][b][k]);
+                    atomicMax(&G->hi[a][b][k], sb.hi[a][b][k]);
+                    atomicMin(&G->clo[a][b][k], sb.clo[a][b][k]);
+                    atomicMax(&G->chi[a][b][k], sb.chi[a][b][k]);
+                }
+            }
+    }
+}
+
+// One thread per task: choose the SAH split from the bins, create the two child nodes
+// (exact boxes from the bins) and either a next-level task or a small cluster for each.
+__global__ void k_sah(const Task* __restrict__ tasks, int ntasks, const Bins* __restrict__ bins, Split* splits,
+                      BNode* nodes, Task* next_tasks, int32_t* small_list, int32_t* counters, int32_t* pending_bounds)
+{
+    const int ti = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ti >= ntasks) return;
+    const Task tk = tasks[ti];
+    const Bins& B = bins[ti];
+    float best = kRealMax;
+    int best_axis = -1, best_bin = -1, best_nl = 0;
+    for (int a = 0; a < 3; ++a) {
+        if (!(tk.cmax[a] - tk.cmin[a] > 0.0f)) continue;
+        // suffix areas
+        float rlo[3] = {kRealMax, kRealMax, kRealMax}, rhi[3] = {-kRealMax, -kRealMax, -kRealMax};
+        float rarea[kBins];
+        int rcnt[kBins];
+        int acc = 0;
+        for (int b = kBins - 1; b >= 0; --b) {
+            if (B.cnt[a][b]) {
+                for (int k = 0; k < 3; ++k) {
+                    rlo[k] = fminf(rlo[k], ord2f(B.lo[a][b][k]));
+                    rhi[k] = fmaxf(rhi[k], ord2f(B.hi[a][b][k]));
+                }
+            }
+            acc += (int)B.cnt[a][b];
+            rarea[b] = half_area(rlo, rhi);
+            rcnt[b] = acc;
+        }
+        float llo[3] = {kRealMax, kRealMax, kRealMax}, lhi[3] = {-kRealMax, -kRealMax, -kRealMax};
+        int lacc = 0;
+        for (int b = 0; b < kBins - 1; ++b) {
+            if (B.cnt[a][b]) {
+                for (int k = 0; k < 3; ++k) {
+                    llo[k] = fminf(llo[k], ord2f(B.lo[a][b][k]));
+                    lhi[k] = fmaxf(lhi[k], ord2f(B.hi[a][b][k]));
+                }
+            }
+            lacc += (int)B.cnt[a][b];
+            const int nr = rcnt[b + 1];
+            if (lacc == 0 || nr == 0) continue;
+            const float cost = half_area(llo, lhi) * (float)lacc + rarea[b + 1] * (float)nr;
+            if (cost < best) {
+                best = cost;
+                best_axis = a;
+                best_bin = b;
+                best_nl = lacc;
+            }
+        }
+    }
+    Split sp;
+    int nl, nr;
+    float clo[2][3], chi[2][3], ccl[2][3], cch[2][3];
+    bool child_bounds_known = true;
+    if (best_axis < 0) {
+        // Every centroid falls in one bin on every axis: split the range in half.
+        sp.axis = -1;
+        sp.bin = 0;
+        nl = tk.count / 2;
+        child_bounds_known = false;
+    } else {
+        sp.axis = best_axis;
+        sp.bin = best_bin;
+        nl = best_nl;
+        for (int s = 0; s < 2; ++s)
+            for (int k = 0; k < 3; ++k) {
+                clo[s][k] = kRealMax;
+                chi[s][k] = -kRealMax;
+                ccl[s][k] = kRealMax;
+                cch[s][k] = -kRealMax;
+            }
+        for (int b = 0; b < kBins; ++b) {
+            if (!B.cnt[best_axis][b]) continue;
+            const int s = b <= best_bin ? 0 : 1;
+            for (int k = 0; k < 3; ++k) {
+                clo[s][k] = fminf(clo[s][k], ord2f(B.lo[best_axis][b][k]));
+                chi[s][k] = fmaxf(chi[s][k], ord2f(B.hi[best_axis][b][k]));
+                ccl[s][k] = fminf(ccl[s][k], ord2f(B.clo[best_axis][b][k]));
+                cch[s][k] = fmaxf(cch[s][k], ord2f(B.chi[best_axis][b][k]));
+            }
+        }
+    }
+    nr = tk.count - nl;
+    sp.nl = nl;
+    const int c0 = atomicAdd(&counters[0], 2);
+    nodes[tk.node].a = c0;
+    nodes[tk.node].b = c0 + 1;
+    const int cnt[2] = {nl, nr};
+    const int beg[2] = {tk.begin, tk.begin + nl};
+    for (int s = 0; s < 2; ++s) {
+        BNode cn;
+        for (int k = 0; k < 3; ++k) {
+            cn.lo[k] = child_bounds_known ? clo[s][k] : kRealMax;
+            cn.hi[k] = child_bounds_known ? chi[s][k] : -kRealMax;
+        }
+        cn.a = 0;
+        cn.b = 0;
+        nodes[c0 + s] = cn;
+        if (cnt[s] <= kSmall) {
+            const int q = atomicAdd(&counters[2], 1);
+            small_list[3 * q + 0] = c0 + s;
+            small_list[3 * q + 1] = beg[s];
+            small_list[3 * q + 2] = cnt[s];
+            sp.child_task[s] = -1;
+        } else {
+            const int q = atomicAdd(&counters[1], 1);
+            Task nt;
+            nt.node = c0 + s;
+            nt.begin = beg[s];
+            nt.count = cnt[s];
+            nt.pad = child_bounds_known ? 0 : 1;
+            for (int k = 0; k < 3; ++k) {
+                nt.cmin[k] = child_bounds_known ? ccl[s][k] : kRealMax;
+                nt.cmax[k] = child_bounds_known ? cch[s][k] : -kRealMax;
+            }
+            next_tasks[q] = nt;
+            sp.child_task[s] = q;
+        }
+    }
+    if (!child_bounds_known) atomicAdd(pending_bounds, 1);
+    splits[ti] = sp;
+}
+
+__global__ void k_flags(const float4* __restrict__ plo, const float4* __restrict__ phi, const int32_t* __restrict__ pidx,
+                        const int32_t* __restrict__ pos_task, const Task* __restrict__ tasks,
+                        const Split* __restrict__ splits, int32_t* flags, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int t = pos_task[i];
+        int f = 0;
+        if (t >= 0) {
+            const Split sp = splits[t];
+            const Task& tk = tasks[t];
+            if (sp.axis < 0) {
+                f = (i - tk.begin) < sp.nl ? 1 : 0;
+            } else {
+                const int a = sp.axis;
+                const int p = pidx[i];
+                const float c = 0.5f * ((&plo[p].x)[a] + (&phi[p].x)[a]);
+                const float ext = tk.cmax[a] - tk.cmin[a];
+                const float scale = (float)kBins * (1.0f - 1e-6f) / ext;
+                f = bin_of(c, tk.cmin[a], scale) <= sp.bin ? 1 : 0;
+            }
+        }
+        flags[i] = f;
+    }
+}
+
+// Exclusive scan, three phases.
+__global__ void k_scan_tiles(const int32_t* in, int32_t* out, int32_t* tile_sums, int n)
+{
+    __shared__ int32_t s[kScanBlock];
+    const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    int v[kScanItems];
+    int sum = 0;
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = (base + k < n) ? in[base + k] : 0;
+        sum += v[k];
+    }
+    s[threadIdx.x] = sum;
+    __syncthreads();
+    for (int off = 1; off < kScanBlock; off <<= 1) {
+        const int x = threadIdx.x >= off ? s[threadIdx.x - off] : 0;
+        __syncthreads();
+        s[threadIdx.x] += x;
+        __syncthreads();
+    }
+    int run = s[threadIdx.x] - sum;
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) out[base + k] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == kScanBlock - 1) tile_sums[blockIdx.x] = s[threadIdx.x];
+}
+
+__global__ void k_scan_sums(int32_t* sums, int ntiles, int32_t* total)
+{
+    __shared__ int32_t s[kScanBlock];
+    int carry = 0;
+    for (int base = 0; base < ntiles; base += kScanBlock) {
+        const int i = base + threadIdx.x;
+        const int v = i < ntiles ? sums[i] : 0;
+        s[threadIdx.x] = v;
+        __syncthreads();
+        for (int off = 1; off < kScanBlock; off <<= 1) {
+            const int x = threadIdx.x >= off ? s[threadIdx.x - off] : 0;
+            __syncthreads();
+            s[threadIdx.x] += x;
+            __syncthreads();
+        }
+        if (i < ntiles) sums[i] = carry + s[threadIdx.x] - v;
+        const int tot = s[kScanBlock - 1];
+        __syncthreads();
+        carry += tot;
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void k_scan_add(int32_t* out, const int32_t* sums, int n)
+{
+    const int base = blockIdx.x * kScanTile;
+    const int add = sums[blockIdx.x];
+    for (int k = threadIdx.x; k < kScanTile; k += blockDim.x) {
+        const int i = base + k;
+        if (i < n) out[i] += add;
+    }
+}
+
+__global__ void k_scatter(const int32_t* __restrict__ pidx, const int32_t* __restrict__ pos_task,
+                          const Task* __restrict__ tasks, const Split* __restrict__ splits,
+                          const int32_t* __restrict__ flags, const int32_t* __restrict__ scan,
+                          int32_t* pidx_out, int32_t* pos_task_out, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int t = pos_task[i];
+        if (t < 0) {
+            pidx_out[i] = pidx[i];
+            pos_task_out[i] = -1;
+            continue;
+        }
+        const Task& tk = tasks[t];
+        const Split& sp = splits[t];
+        const int lbefore = scan[i] - scan[tk.begin];
+        int np, child;
+        if (flags[i]) {
+            np = tk.begin + lbefore;
+            child = sp.child_task[0];
+        } else {
+            np = tk.begin + sp.nl + (i - tk.begin - lbefore);
+            child = sp.child_task[1];
+        }
+        pidx_out[np] = pidx[i];
+        pos_task_out[np] = child;
+    }
+}
+
+// Boxes of children created by a median split are accumulated here after the scatter.
+__global__ void k_pending_bounds(const float4* __restrict__ plo, const float4* __restrict__ phi,
+                                 const int32_t* __restrict__ pidx, const Task* __restrict__ tasks, const Split* splits,
+                                 int ntasks, BNode* nodes, Task* next_tasks, const int32_t* small_list, int nsmall_before,
+                                 int nsmall_after)
+{
+    // One block per task of the previous level whose split was a median split.
+    const int ti = blockIdx.x;
+    if (ti >= ntasks) return;
+    const Split sp = splits[ti];
+    if (sp.axis >= 0) return;
+    const Task tk = tasks[ti];
+    for (int s = 0; s < 2; ++s) {
+        const int beg = s == 0 ? tk.begin : tk.begin + sp.nl;
+        const int cnt = s == 0 ? sp.nl : tk.count - sp.nl;
+        const int node = nodes[tk.node].a + s;
+        uint32_t* nb = reinterpret_cast<uint32_t*>(&nodes[node]);
+        for (int i = beg + threadIdx.x; i < beg + cnt; i += blockDim.x) {
+            const int p = pidx[i];
+            const float4 l = plo[p], h = phi[p];
+            const float lv[3] = {l.x, l.y, l.z}, hv[3] = {h.x, h.y, h.z};
+            for (int k = 0; k < 3; ++k) {
+                // nodes hold floats; use a CAS loop through the ordered encoding
+                float* lo = &nodes[node].lo[k];
+                float* hi = &nodes[node].hi[k];
+                int* li = reinterpret_cast<int*>(lo);
+                int* hiI = reinterpret_cast<int*>(hi);
+                int old = *li;
+                while (lv[k] < __int_as_float(old)) {
+                    const int prev = atomicCAS(li, old, __float_as_int(lv[k]));
+                    if (prev == old) break;
+                    old = prev;
+                }
+                old = *hiI;
+                while (hv[k] > __int_as_float(old)) {
+                    const int prev = atomicCAS(hiI, old, __float_as_int(hv[k]));
+                    if (prev == old) break;
+                    old = prev;
+                }
+                if (sp.child_task[s] >= 0) {
+                    const float c = 0.5f * (lv[k] + hv[k]);
+                    Task& nt = next_tasks[sp.child_task[s]];
+                    int* cl = reinterpret_cast<int*>(&nt.cmin[k]);
+                    int* ch = reinterpret_cast<int*>(&nt.cmax[k]);
+                    old = *cl;
+                    while (c < __int_as_float(old)) {
+                        const int prev = atomicCAS(cl, old, __float_as_int(c));
+                        if (prev == old) break;
+                        old = prev;
+                    }
+                    old = *ch;
+                    while (c > __int_as_float(old)) {
+                        const int prev = atomicCAS(ch, old, __float_as_int(c));
+                        if (prev == old) break;
+                        old = prev;
+                    }
+                }
+            }
+        }
+        (void)nb;
+    }
+    (void)small_list;
+    (void)nsmall_before;
+    (void)nsmall_after;
+}
+
+// Sequential exact-SAH builder for one cluster of <= kSmall primitives per thread.
+__global__ void k_small(const float4* __restrict__ plo, const float4* __restrict__ phi, int32_t* pidx,
+                        const int32_t* __restrict__ small_list, int nsmall, BNode* nodes, int32_t* counters)
+{
+    const int ci = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ci >= nsmall) return;
+    const int root = small_list[3 * ci], begin = small_list[3 * ci + 1], count = small_list[3 * ci + 2];
+    int ids[kSmall];
+    for (int k = 0; k < count; ++k) ids[k] = pidx[begin + k];
+    // explicit stack of (node, lo, n) ranges within ids[]
+    int st_node[kSmall], st_lo[kSmall], st_n[kSmall];
+    int sp = 0;
+    st_node[0] = root;
+    st_lo[0] = 0;
+    st_n[0] = count;
+    sp = 1;
+    {
+        // the cluster root's box (may be unset after a median split higher up)
+        float lo[3] = {kRealMax, kRealMax, kRealMax}, hi[3] = {-kRealMax, -kRealMax, -kRealMax};
+        for (int k = 0; k < count; ++k) {
+            const float4 l = plo[ids[k]], h = phi[ids[k]];
+            lo[0] = fminf(lo[0], l.x); lo[1] = fminf(lo[1], l.y); lo[2] = fminf(lo[2], l.z);
+            hi[0] = fmaxf(hi[0], h.x); hi[1] = fmaxf(hi[1], h.y); hi[2] = fmaxf(hi[2], h.z);
+        }
+        for (int a = 0; a < 3; ++a) {
+            nodes[root].lo[a] = lo[a];
+            nodes[root].hi[a] = hi[a];
+        }
+    }
+    float racc[kSmall];
+    while (sp > 0) {
+        --sp;
+        const int node = st_node[sp], lo0 = st_lo[sp], n = st_n[sp];
+        float nlo[3], nhi[3];
+        for (int a = 0; a < 3; ++a) {
+            nlo[a] = nodes[node].lo[a];
+            nhi[a] = nodes[node].hi[a];
+        }
+        const float parent_area = half_area(nlo, nhi);
+        float best = kRealMax;
+        int best_axis = -1, best_k = 0;
+        if (n > 1) {
+            for (int a = 0; a < 3; ++a) {
+                // insertion sort of ids[lo0 .. lo0+n) by centroid along a
+                for (int i = lo0 + 1; i < lo0 + n; ++i) {
+                    const int v = ids[i];
+                    const float cv = (&plo[v].x)[a] + (&phi[v].x)[a];
+                    int j = i - 1;
+                    while (j >= lo0) {
+                        const int u = ids[j];
+                        if ((&plo[u].x)[a] + (&phi[u].x)[a] <= cv) break;
+                        ids[j + 1] = u;
+                        --j;
+                    }
+                    ids[j + 1] = v;
+                }
+                float rlo[3] = {kRealMax, kRealMax, kRealMax}, rhi[3] = {-kRealMax, -kRealMax, -kRealMax};
+                for (int i = n - 1; i >= 1; --i) {
+                    const float4 l = plo[ids[lo0 + i]], h = phi[ids[lo0 + i]];
+                    rlo[0] = fminf(rlo[0], l.x); rlo[1] = fminf(rlo[1], l.y); rlo[2] = fminf(rlo[2], l.z);
+                    rhi[0] = fmaxf(rhi[0], h.x); rhi[1] = fmaxf(rhi[1], h.y); rhi[2] = fmaxf(rhi[2], h.z);
+                    racc[i] = half_area(rlo, rhi);
+                }
+                float llo[3] = {kRealMax, kRealMax, kRealMax}, lhi[3] = {-kRealMax, -kRealMax, -kRealMax};
+                for (int i = 0; i < n - 1; ++i) {
+                    const float4 l = plo[ids[lo0 + i]], h = phi[ids[lo0 + i]];
+                    llo[0] = fminf(llo[0], l.x); llo[1] = fminf(llo[1], l.y); llo[2] = fminf(llo[2], l.z);
+                    lhi[0] = fmaxf(lhi[0], h.x); lhi[1] = fmaxf(lhi[1], h.y); lhi[2] = fmaxf(lhi[2], h.z);
+                    const float cost = half_area(llo, lhi) * (float)(i + 1) + racc[i + 1] * (float)(n - i - 1);
+                    if (cost < best) {
+                        best = cost;
+                        best_axis = a;
+                        best_k = i + 1;
+                    }
+                }
+            }
+        }
+        // SAH termination with unit costs (traversal step 1, primitive test 1).
+        const float split_cost = parent_area > 0.0f ? 1.0f + best / parent_area : kRealMax;
+        const bool make_leaf = n <= 1 || (n <= kLeafMax && (float)n <= split_cost);
+        if (make_leaf) {
+            for (int k = 0; k < n; ++k) pidx[begin + lo0 + k] = ids[lo0 + k];
+            nodes[node].a = ~(begin + lo0);
+            nodes[node].b = n;
+            continue;
+        }
+        if (best_axis < 0) {
+            best_axis = 0;
+            best_k = n / 2;
+        }
+        // re-sort along the chosen axis (the loop above left ids sorted along z)
+        if (best_axis != 2) {
+            const int a = best_axis;
+            for (int i = lo0 + 1; i < lo0 + n; ++i) {
+                const int v = ids[i];
+                const float cv = (&plo[v].x)[a] + (&phi[v].x)[a];
+                int j = i - 1;
+                while (j >= lo0) {
+                    const int u = ids[j];
+                    if ((&plo[u].x)[a] + (&phi[u].x)[a] <= cv) break;
+                    ids[j + 1] = u;
+                    --j;
+                }
+                ids[j + 1] = v;
+            }
+        }
+        const int c0 = atomicAdd(&counters[0], 2);
+        nodes[node].a = c0;
+        nodes[node].b = c0 + 1;
+        const int rng_lo[2] = {lo0, lo0 + best_k};
+        const int rng_n[2] = {best_k, n - best_k};
+        for (int s = 0; s < 2; ++s) {
+            float lo[3] = {kRealMax, kRealMax, kRealMax}, hi[3] = {-kRealMax, -kRealMax, -kRealMax};
+            for (int k = 0; k < rng_n[s]; ++k) {
+                const float4 l = plo[ids[rng_lo[s] + k]], h = phi[ids[rng_lo[s] + k]];
+                lo[0] = fminf(lo[0], l.x); lo[1] = fminf(lo[1], l.y); lo[2] = fminf(lo[2], l.z);
+                hi[0] = fmaxf(hi[0], h.x); hi[1] = fmaxf(hi[1], h.y); hi[2] = fmaxf(hi[2], h.z);
+            }
+            BNode cn;
+            for (int a = 0; a < 3; ++a) {
+                cn.lo[a] = lo[a];
+                cn.hi[a] = hi[a];
+            }
+            cn.a = 0;
+            cn.b = 0;
+            nodes[c0 + s] = cn;
+            st_node[sp] = c0 + s;
+            st_lo[sp] = rng_lo[s];
+            st_n[sp] = rng_n[s];
+            ++sp;
+        }
+    }
+}
+
+// ---- collapse to 8-wide nodes --------------------------------------------------
+
+FM_D float node_area(const BNode& b) { return half_area(b.lo, b.hi); }
+
+__global__ void k_collapse(const BNode* __restrict__ bnodes, const int32_t* __restrict__ pidx,
+                           const int2* __restrict__ frontier, int nfront, int2* next_frontier, int32_t* counters,
+                           uint4* wnodes, int32_t* leaf_prim)
+{
+    // counters: [0] wide node count, [1] leaf slot count, [2] next frontier count
+    const int fi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (fi >= nfront) return;
+    const int bn = frontier[fi].x, wslot = frontier[fi].y;
+    const BNode root = bnodes[bn];
+    int ch[8];
+    int nch = 0;
+    if (root.a < 0) {
+        ch[nch++] = bn;
+    } else {
+        ch[nch++] = root.a;
+        ch[nch++] = root.b;
+        while (nch < 8) {
+            int bi = -1;
+            float ba = -1.0f;
+            for (int k = 0; k < nch; ++k) {
+                const BNode& c = bnodes[ch[k]];
+                if (c.a >= 0) {
+                    const float ar = node_area(c);
+                    if (ar > ba) {
+                        ba = ar;
+                        bi = k;
+                    }
+                }
+            }
+            if (bi < 0) break;
+            const BNode c = bnodes[ch[bi]];
+            ch[bi] = c.a;
+            ch[nch++] = c.b;
+        }
+    }
+    // node box and centre
+    float lo[3] = {kRealMax, kRealMax, kRealMax}, hi[3] = {-kRealMax, -kRealMax, -kRealMax};
+    for (int k = 0; k < nch; ++k) {
+        const BNode& c = bnodes[ch[k]];
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = fminf(lo[a], c.lo[a]);
+            hi[a] = fmaxf(hi[a], c.hi[a]);
+        }
+    }
+    const float ctr[3] = {0.5f * (lo[0] + hi[0]), 0.5f * (lo[1] + hi[1]), 0.5f * (lo[2] + hi[2])};
+    // greedy octant slot assignment: farthest children first pick their best free slot
+    int slot_of[8];
+    bool used[8] = {false, false, false, false, false, false, false, false};
+    bool done[8] = {false, false, false, false, false, false, false, false};
+    for (int it = 0; it < nch; ++it) {
+        int pick = -1;
+        float pd = -1.0f;
+        for (int k = 0; k < nch; ++k) {
+            if (done[k]) continue;
+            const BNode& c = bnodes[ch[k]];
+            float d2 = 0.0f;
+            for (int a = 0; a < 3; ++a) {
+                const float dv = 0.5f * (c.lo[a] + c.hi[a]) - ctr[a];
+                d2 += dv * dv;
+            }
+            if (d2 > pd) {
+                pd = d2;
+                pick = k;
+            }
+        }
+        const BNode& c = bnodes[ch[pick]];
+        float best = -kRealMax;
+        int bs = 0;
+        for (int s = 0; s < 8; ++s) {
+            if (used[s]) continue;
+            float score = 0.0f;
+            for (int a = 0; a < 3; ++a) {
+                const float dv = 0.5f * (c.lo[a] + c.hi[a]) - ctr[a];
+                score += ((s >> a) & 1) ? dv : -dv;
+            }
+            if (score > best) {
+                best = score;
+                bs = s;
+            }
+        }
+        used[bs] = true;
+        done[pick] = true;
+        slot_of[pick] = bs;
+    }
+    int at_slot[8];
+    for (int s = 0; s < 8; ++s) at_slot[s] = -1;
+    for (int k = 0; k < nch; ++k) at_slot[slot_of[k]] = ch[k];
+    int n_int = 0, n_prim = 0;
+    for (int s = 0; s < 8; ++s) {
+        if (at_slot[s] < 0) continue;
+        const BNode& c = bnodes[at_slot[s]];
+        if (c.a >= 0) ++n_int;
+        else n_prim += c.b;
+    }
+    const int child_base = n_int ? atomicAdd(&counters[0], n_int) : 0;
+    const int prim_base = n_prim ? atomicAdd(&counters[1], n_prim) : 0;
+    // quantization
+    uint32_t e[3];
+    float scale[3];
+    for (int a = 0; a < 3; ++a) {
+        const float ext = hi[a] - lo[a];
+        float s = ext > 0.0f ? ext * (1.0f / 255.0f) * 1.0000005f : 0.0f;
+        uint32_t bits = __float_as_uint(s);
+        uint32_t ex = (bits >> 23) & 0xffu;
+        if (bits & 0x7fffffu) ++ex;   // round up to a power of two
+        if (ex < 1u) ex = 1u;
+        if (ex > 254u) ex = 254u;
+        e[a] = ex;
+        scale[a] = __uint_as_float(ex << 23);
+    }
+    uint32_t meta[8], ql[3][8], qh[3][8];
+    uint32_t imask = 0;
+    int int_rank = 0, prim_off = 0;
+    for (int s = 0; s < 8; ++s) {
+        meta[s] = 0;
+        for (int a = 0; a < 3; ++a) {
+            ql[a][s] = 0;
+            qh[a][s] = 0;
+        }
+        if (at_slot[s] < 0) continue;
+        const BNode& c = bnodes[at_slot[s]];
+        for (int a = 0; a < 3; ++a) {
+            float qlo = floorf(__fdiv_rd(__fsub_rd(c.lo[a], lo[a]), scale[a]));
+            float qhi = ceilf(__fdiv_ru(__fsub_ru(c.hi[a], lo[a]), scale[a]));
+            qlo = fminf(fmaxf(qlo, 0.0f), 255.0f);
+            qhi = fminf(fmaxf(qhi, 0.0f), 255.0f);
+            ql[a][s] = (uint32_t)qlo;
+            qh[a][s] = (uint32_t)qhi;
+        }
+        if (c.a >= 0) {
+            imask |= 1u << s;
+            meta[s] = 0x20u | (uint32_t)(24 + s);   // nonzero marker; traversal uses imask
+            const int q = atomicAdd(&counters[2], 1);
+            next_frontier[q] = make_int2(at_slot[s], child_base + int_rank);
+            ++int_rank;
+        } else {
+            const int cnt = c.b, beg = ~c.a;
+            meta[s] = (((1u << cnt) - 1u) << 5) | (uint32_t)prim_off;
+            for (int k = 0; k < cnt; ++k) leaf_prim[prim_base + prim_off + k] = pidx[beg + k];
+            prim_off += cnt;
+        }
+    }
+    auto pack4 = [](const uint32_t* v) { return v[0] | (v[1] << 8) | (v[2] << 16) | (v[3] << 24); };
+    uint4* np = wnodes + 5 * (size_t)wslot;
+    np[0] = make_uint4(__float_as_uint(lo[0]), __float_as_uint(lo[1]), __float_as_uint(lo[2]),
+                       e[0] | (e[1] << 8) | (e[2] << 16) | (imask << 24));
+    np[1] = make_uint4((uint32_t)child_base, (uint32_t)prim_base, pack4(meta), pack4(meta + 4));
+    np[2] = make_uint4(pack4(ql[0]), pack4(ql[0] + 4), pack4(ql[1]), pack4(ql[1] + 4));
+    np[3] = make_uint4(pack4(ql[2]), pack4(ql[2] + 4), pack4(qh[0]), pack4(qh[0] + 4));
+    np[4] = make_uint4(pack4(qh[1]), pack4(qh[1] + 4), pack4(qh[2]), pack4(qh[2] + 4));
+}
+
+__global__ void k_fill_leaf(const int32_t* __restrict__ leaf_prim, int nleaf, PrimSource src, float4* leaf)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nleaf; i += gridDim.x * blockDim.x) {
+        const int p = leaf_prim[i];
+        float4 a, b, c;
+        if (p < src.num_tris) {
+            const float* v = src.tri_pos + 9 * (size_t)p;
+            a = make_float4(v[0], v[1], v[2], __uint_as_float((uint32_t)p));
+            b = make_float4(v[3], v[4], v[5], 0.0f);
+            c = make_float4(v[6], v[7], v[8], 0.0f);
+        } else if (p < src.num_tris + 2 * src.num_rects) {
+            const int r = (p - src.num_tris) >> 1, h = (p - src.num_tris) & 1;
+            const RectDev& R = src.rects[r];
+            const float* q0 = h ? R.pc : R.pa;
+            const float* q1 = h ? R.pd : R.pb;
+            const float* q2 = h ? R.pa : R.pc;
+            a = make_float4(q0[0], q0[1], q0[2], __uint_as_float((uint32_t)p));
+            b = make_float4(q1[0], q1[1], q1[2], 0.0f);
+            c = make_float4(q2[0], q2[1], q2[2], 0.0f);
+        } else {
+            const int s = p - src.num_tris - 2 * src.num_rects;
+            a = make_float4(__uint_as_float((uint32_t)s), 0.0f, 0.0f, __uint_as_float((uint32_t)p | kSphereFlag));
+            b = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        leaf[3 * (size_t)i] = a;
+        leaf[3 * (size_t)i + 1] = b;
+        leaf[3 * (size_t)i + 2] = c;
+    }
+}
+
+__global__ void k_prim_bounds(PrimSource src, float4* plo, float4* phi)
+{
+    const int n = src.num_tris + 2 * src.num_rects + src.num_spheres;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        float lo[3], hi[3];
+        if (p < src.num_tris + 2 * src.num_rects) {
+            f3 v[3];
+            if (p < src.num_tris) {
+                const float* q = src.tri_pos + 9 * (size_t)p;
+                v[0] = ld3(q);
+                v[1] = ld3(q + 3);
+                v[2] = ld3(q + 6);
+            } else {
+                const int r = (p - src.num_tris) >> 1, h = (p - src.num_tris) & 1;
+                const RectDev& R = src.rects[r];
+                v[0] = ld3(h ? R.pc : R.pa);
+                v[1] = ld3(h ? R.pd : R.pb);
+                v[2] = ld3(h ? R.pa : R.pc);
+            }
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = fminf(fminf(comp(v[0], a), comp(v[1], a)), comp(v[2], a));
+                hi[a] = fmaxf(fmaxf(comp(v[0], a), comp(v[1], a)), comp(v[2], a));
+            }
+        } else {
+            const SphereDev& S = src.spheres[p - src.num_tris - 2 * src.num_rects];
+            const f3 c = f3{S.o2w.m[3], S.o2w.m[7], S.o2w.m[11]};
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = comp(c, a) - S.radius_world;
+                hi[a] = comp(c, a) + S.radius_world;
+            }
+        }
+        plo[p] = make_float4(lo[0], lo[1], lo[2], 0.0f);
+        phi[p] = make_float4(hi[0], hi[1], hi[2], 0.0f);
+    }
+}
+
+inline int grid_for(int64_t n, int block)
+{
+    int64_t g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > 148 * 32) g = 148 * 32;
+    return (int)g;
+}
+
+}  // namespace
+
+#define FM_BUILD_CHECK(x)                                                        \
+    do {                                                                         \
+        cudaError_t e__ = (x);                                                   \
+        if (e__ != cudaSuccess) {                                                \
+            err = std::string("bvh build: ") + cudaGetErrorString(e__);          \
+            goto fail;                                                           \
+        }                                                                        \
+    } while (0)
+
+int bvh_build(cudaStream_t stream, const PrimSource& src, BvhResult& out, std::string& err)
+{
+    const int n = src.num_tris + 2 * src.num_rects + src.num_spheres;
+    out = BvhResult{};
+    if (n == 0) return 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float4 *plo = nullptr, *phi = nullptr;
+    int32_t *pidx = nullptr, *pidx2 = nullptr, *pos_task = nullptr, *pos_task2 = nullptr, *flags = nullptr,
+            *scan = nullptr, *tile_sums = nullptr, *small_list = nullptr, *counters = nullptr, *leaf_prim = nullptr;
+    uint32_t* rb = nullptr;
+    BNode* bnodes = nullptr;
+    Task *tasks = nullptr, *tasks2 = nullptr;
+    Split* splits = nullptr;
+    Bins* bins = nullptr;
+    int2 *front = nullptr, *front2 = nullptr;
+    const int max_tasks = n / (kSmall + 1) + 2;
+    const int max_nodes = 2 * n + 2;
+    const int ntiles = (n + kScanTile - 1) / kScanTile;
+    int h_counters[4];
+    int ntasks = 0, nsmall = 0, depth = 0, nwide = 0, nleaf = 0;
+    FM_BUILD_CHECK(cudaEventCreate(&ev0));
+    FM_BUILD_CHECK(cudaEventCreate(&ev1));
+    FM_BUILD_CHECK(cudaEventRecord(ev0, stream));
+    FM_BUILD_CHECK(cudaMalloc(&plo, sizeof(float4) * n));
+    FM_BUILD_CHECK(cudaMalloc(&phi, sizeof(float4) * n));
+    FM_BUILD_CHECK(cudaMalloc(&pidx, sizeof(int32_t) * n));
+    FM_BUILD_CHECK(cudaMalloc(&pidx2, sizeof(int32_t) * n));
+    FM_BUILD_CHECK(cudaMalloc(&pos_task, sizeof(int32_t) * n));
+    FM_BUILD_CHECK(cudaMalloc(&pos_task2, sizeof(int32_t) * n));
+    FM_BUILD_CHECK(cudaMalloc(&flags, sizeof(int32_t) * n));
+    FM_BUILD_CHECK(cudaMalloc(&scan, sizeof(int32_t) * (n + 1)));
+    FM_BUILD_CHECK(cudaMalloc(&tile_sums, sizeof(int32_t) * (ntiles + 1)));
+    FM_BUILD_CHECK(cudaMalloc(&small_list, sizeof(int32_t) * 3 * (n + 1)));
+    FM_BUILD_CHECK(cudaMalloc(&counters, sizeof(int32_t) * 8));
+    FM_BUILD_CHECK(cudaMalloc(&rb, sizeof(uint32_t) * 12));
+    FM_BUILD_CHECK(cudaMalloc(&bnodes, sizeof(BNode) * max_nodes));
+    FM_BUILD_CHECK(cudaMalloc(&tasks, sizeof(Task) * max_tasks));
+    FM_BUILD_CHECK(cudaMalloc(&tasks2, sizeof(Task) * max_tasks));
+    FM_BUILD_CHECK(cudaMalloc(&splits, sizeof(Split) * max_tasks));
+    FM_BUILD_CHECK(cudaMalloc(&bins, sizeof(Bins) * max_tasks));
+
+    k_prim_bounds<<<grid_for(n, 256), 256, 0, stream>>>(src, plo, phi);
+    {
+        const uint32_t init[12] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u,
+                                   0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+        FM_BUILD_CHECK(cudaMemcpyAsync(rb, init, sizeof(init), cudaMemcpyHostToDevice, stream));
+    }
+    k_root_bounds<<<grid_for(n, 256), 256, 0, stream>>>(plo, phi, n, rb);
+    FM_BUILD_CHECK(cudaMemsetAsync(counters, 0, sizeof(int32_t) * 8, stream));
+    k_make_root<<<1, 1, 0, stream>>>(rb, n, bnodes, tasks, pos_task, small_list, counters);
+    k_fill_pos_task<<<grid_for(n, 256), 256, 0, stream>>>(pos_task, pidx, n, n <= kSmall ? -1 : 0);
+    FM_BUILD_CHECK(cudaMemcpyAsync(h_counters, counters, sizeof(int32_t) * 4, cudaMemcpyDeviceToHost, stream));
+    FM_BUILD_CHECK(cudaStreamSynchronize(stream));
+    ntasks = h_counters[1];
+    nsmall = h_counters[2];
+
+    while (ntasks > 0) {
+        k_init_bins<<<ntasks, 256, 0, stream>>>(bins, ntasks);
+        k_bin<<<(n + 1023) / 1024, 256, 0, stream>>>(plo, phi, pidx, pos_task, tasks, bins, n);
+        FM_BUILD_CHECK(cudaMemsetAsync(counters + 1, 0, sizeof(int32_t), stream));
+        FM_BUILD_CHECK(cudaMemsetAsync(counters + 3, 0, sizeof(int32_t), stream));
+        k_sah<<<(ntasks + 127) / 128, 128, 0, stream>>>(tasks, ntasks, bins, splits, bnodes, tasks2, small_list,
+                                                         counters, counters + 3);
+        k_flags<<<grid_for(n, 256), 256, 0, stream>>>(plo, phi, pidx, pos_task, tasks, splits, flags, n);
+        k_scan_tiles<<<ntiles, kScanBlock, 0, stream>>>(flags, scan, tile_sums, n);
+        k_scan_sums<<<1, kScanBlock, 0, stream>>>(tile_sums, ntiles, scan + n);
+        k_scan_add<<<ntiles, 256, 0, stream>>>(scan, tile_sums, n);
+        k_scatter<<<grid_for(n, 256), 256, 0, stream>>>(pidx, pos_task, tasks, splits, flags, scan, pidx2, pos_task2,
+                                                         n);
+        FM_BUILD_CHECK(cudaMemcpyAsync(h_counters, counters, sizeof(int32_t) * 4, cudaMemcpyDeviceToHost, stream));
+        FM_BUILD_CHECK(cudaStreamSynchronize(stream));
+        if (h_counters[3] > 0)
+            k_pending_bounds<<<ntasks, 256, 0, stream>>>(plo, phi, pidx2, tasks, splits, ntasks, bnodes, tasks2,
+                                                          small_list, 0, 0);
+        std::swap(pidx, pidx2);
+        std::swap(pos_task, pos_task2);
+        std::swap(tasks, tasks2);
+        ntasks = h_counters[1];
+        nsmall = h_counters[2];
+        if (ntasks > max_tasks) {
+            err = "bvh build: task list overflow";
+            goto fail;
+        }
+    }
+    if (nsmall > 0) k_small<<<(nsmall + 63) / 64, 64, 0, stream>>>(plo, phi, pidx, small_list, nsmall, bnodes, counters);
+    FM_BUILD_CHECK(cudaGetLastError());
+
+    // Collapse.  Wide node count <= binary internal nodes; leaf slots == n.
+    FM_BUILD_CHECK(cudaMalloc(&out.nodes, sizeof(uint4) * 5 * (size_t)(n + 1)));
+    FM_BUILD_CHECK(cudaMalloc(&leaf_prim, sizeof(int32_t) * n));
+    FM_BUILD_CHECK(cudaMalloc(&front, sizeof(int2) * (n + 1)));
+    FM_BUILD_CHECK(cudaMalloc(&front2, sizeof(int2) * (n + 1)));
+    {
+        const int2 r0 = make_int2(0, 0);
+        FM_BUILD_CHECK(cudaMemcpyAsync(front, &r0, sizeof(int2), cudaMemcpyHostToDevice, stream));
+        const int32_t c0[4] = {1, 0, 0, 0};
+        FM_BUILD_CHECK(cudaMemcpyAsync(counters, c0, sizeof(c0), cudaMemcpyHostToDevice, stream));
+    }
+    {
+        int nfront = 1;
+        while (nfront > 0) {
+            ++depth;
+            FM_BUILD_CHECK(cudaMemsetAsync(counters + 2, 0, sizeof(int32_t), stream));
+            k_collapse<<<(nfront + 127) / 128, 128, 0, stream>>>(bnodes, pidx, front, nfront, front2, counters,
+                                                                  out.nodes, leaf_prim);
+            FM_BUILD_CHECK(cudaMemcpyAsync(h_counters, counters, sizeof(int32_t) * 4, cudaMemcpyDeviceToHost, stream));
+            FM_BUILD_CHECK(cudaStreamSynchronize(stream));
+            nfront = h_counters[2];
+            std::swap(front, front2);
+        }
+        nwide = h_counters[0];
+        nleaf = h_counters[1];
+    }
+    if (nleaf != n) {
+        err = "bvh build: leaf count mismatch";
+        goto fail;
+    }
+    if (depth >= kTraversalStack) {
+        err = "bvh build: tree deeper than the traversal stack";
+        goto fail;
+    }
+    FM_BUILD_CHECK(cudaMalloc(&out.leaf, sizeof(float4) * 3 * (size_t)n));
+    k_fill_leaf<<<grid_for(n, 256), 256, 0, stream>>>(leaf_prim, n, src, out.leaf);
+    FM_BUILD_CHECK(cudaGetLastError());
+    FM_BUILD_CHECK(cudaEventRecord(ev1, stream));
+    FM_BUILD_CHECK(cudaEventSynchronize(ev1));
+    {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ev0, ev1);
+        out.build_ms = ms;
+    }
+    out.num_nodes = nwide;
+    out.num_leaf = nleaf;
+    out.depth = depth;
+    cudaFree(plo);
+    cudaFree(phi);
+    cudaFree(pidx);
+    cudaFree(pidx2);
+    cudaFree(pos_task);
+    cudaFree(pos_task2);
+    cudaFree(flags);
+    cudaFree(scan);
+    cudaFree(tile_sums);
+    cudaFree(small_list);
+    cudaFree(counters);
+    cudaFree(rb);
+    cudaFree(bnodes);
+    cudaFree(tasks);
+    cudaFree(tasks2);
+    cudaFree(splits);
+    cudaFree(bins);
+    cudaFree(front);
+    cudaFree(front2);
+    cudaFree(leaf_prim);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    return 0;
+fail:
+    cudaStreamSynchronize(stream);
+    cudaFree(plo);
+    cudaFree(phi);
+    cudaFree(pidx);
+    cudaFree(pidx2);
+    cudaFree(pos_task);
+    cudaFree(pos_task2);
+    cudaFree(flags);
+    cudaFree(scan);
+    cudaFree(tile_sums);
+    cudaFree(small_list);
+    cudaFree(counters);
+    cudaFree(rb);
+    cudaFree(bnodes);
+    cudaFree(tasks);
+    cudaFree(tasks2);
+    cudaFree(splits);
+    cudaFree(bins);
+    cudaFree(front);
+    cudaFree(front2);
+    cudaFree(leaf_prim);
+    cudaFree(out.nodes);
+    cudaFree(out.leaf);
+    out = BvhResult{};
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    return -1;
+}
+
+}  // namespace fm

@@ -1,0 +1,197 @@
+// Environment-map importance tables, built on the device.
+//
+// Follows EnvImportanceSampler's construction (light/env_importance_sampler.h:28-65)
+// and Distribution1D/2D (math/distribution_1d.cpp:5-29, distribution_2d.cpp:9-26):
+//   lum[j][i]  = luminance(tex(texel centre)) * sin(pi * (j + 0.5) / H)
+//   lumn       = lum / sum(lum) * W * H                      (mean 1)
+//   row_j      = sum_i lumn[j][i] / W                        (Distribution1D::pdf_sum)
+//   marg       = sum_j row_j / H                             (marginal pdf_sum)
+//   sampling density of texel (i, j)  = lumn[j][i] / marg
+//   density reported by EnvLight::Pdf = (lumn[j][i] / row_j) / marg
+// All sums are FP64.  Sampling uses Vose alias tables (one per row for the
+// conditional, one for the marginal) built from the same weights.
+#include "fm_internal.h"
+#include "fm_texture.cuh"
+
+namespace fm {
+
+namespace {
+
+__global__ void k_env_lum(DevTexture tex, int w, int h, float* lum)
+{
+    const int n = w * h;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const int i = q % w, j = q / w;
+        const float du = 1.0f / (float)w, dv = 1.0f / (float)h;
+        const float u0 = (float)i / (float)w, v0 = (float)j / (float)h;
+        const float sin_theta = sinf(kPi * (v0 + 0.5f * dv));
+        const f3 rad = tex_sample(tex, u0 + 0.5f * du, v0 + 0.5f * dv);
+        lum[q] = luminance(rad) * sin_theta;
+    }
+}
+
+__global__ void k_env_rowsum(const float* lum, int w, double* rowsum)
+{
+    __shared__ double s[256];
+    const int j = blockIdx.x;
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < w; i += blockDim.x) acc += (double)lum[(size_t)j * w + i];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+        if (threadIdx.x < off) s[threadIdx.x] += s[threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) rowsum[j] = s[0];
+}
+
+// totals[0] = sum of lum, totals[1] = marginal sum (of normalized row sums / H)
+__global__ void k_env_totals(const double* rowsum, int w, int h, double* totals)
+{
+    __shared__ double s[256];
+    double acc = 0.0;
+    for (int j = threadIdx.x; j < h; j += blockDim.x) acc += rowsum[j];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+        if (threadIdx.x < off) s[threadIdx.x] += s[threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double total = s[0];
+        totals[0] = total;
+        // row_j = (rowsum_j / total * W * H) / W ; marg = sum_j row_j / H
+        double m = 0.0;
+        for (int j = 0; j < h; ++j) m += (rowsum[j] / total * (double)w * (double)h) / (double)w;
+        totals[1] = m / (double)h;
+    }
+}
+
+__global__ void k_env_pdfs(const float* lum, const double* rowsum, const double* totals, int w, int h,
+                           float* pdf_sample, float* pdf_eval)
+{
+    const int n = w * h;
+    const double total = totals[0], marg = totals[1];
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const int j = q / w;
+        const double lumn = (double)lum[q] / total * (double)w * (double)h;
+        const double row = rowsum[j] / total * (double)h;   // sum_i lumn / W
+        pdf_sample[q] = (float)(lumn / marg);
+        pdf_eval[q] = (float)((lumn / row) / marg);
+    }
+}
+
+// Vose's alias method over n weights, sequential; `small`/`large` are scratch stacks.
+FM_D void vose(const float* wts_f, const double* wts_d, int n, float* prob, int32_t* alias, int32_t* small,
+               int32_t* large)
+{
+    double sum = 0.0;
+    for (int i = 0; i < n; ++i) sum += wts_f ? (double)wts_f[i] : wts_d[i];
+    if (!(sum > 0.0)) {
+        for (int i = 0; i < n; ++i) {
+            prob[i] = 1.0f;
+            alias[i] = i;
+        }
+        return;
+    }
+    // scaled weights are kept in prob as float while the stacks are processed in double
+    int ns = 0, nl = 0;
+    const double scale = (double)n / sum;
+    for (int i = 0; i < n; ++i) {
+        const double q = (wts_f ? (double)wts_f[i] : wts_d[i]) * scale;
+        prob[i] = (float)q;
+        if (q < 1.0) small[ns++] = i;
+        else large[nl++] = i;
+    }
+    // remaining mass of the current large entries is tracked in double
+    while (ns > 0 && nl > 0) {
+        const int s = small[--ns];
+        const int l = large[nl - 1];
+        alias[s] = l;
+        const double ql = ((double)prob[l] + (double)prob[s]) - 1.0;
+        prob[l] = (float)ql;
+        if (ql < 1.0) {
+            --nl;
+            small[ns++] = l;
+        }
+    }
+    while (nl > 0) {
+        const int l = large[--nl];
+        prob[l] = 1.0f;
+        alias[l] = l;
+    }
+    while (ns > 0) {
+        const int s = small[--ns];
+        prob[s] = 1.0f;
+        alias[s] = s;
+    }
+}
+
+__global__ void k_env_alias_rows(const float* lum, int w, int h, float* prob, int32_t* alias, int32_t* scratch)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= h) return;
+    int32_t* small = scratch + (size_t)j * 2 * w;
+    vose(lum + (size_t)j * w, nullptr, w, prob + (size_t)j * w, alias + (size_t)j * w, small, small + w);
+}
+
+__global__ void k_env_alias_marg(const double* rowsum, int h, float* prob, int32_t* alias, int32_t* scratch)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    vose(nullptr, rowsum, h, prob, alias, scratch, scratch + h);
+}
+
+}  // namespace
+
+fm_status env_build_tables(fm_ctx* ctx, fm_scene* scene, const DevTexture& tex, DevEnv& env)
+{
+    const int w = tex.w, h = tex.h;
+    const size_t n = (size_t)w * h;
+    float *lum = nullptr, *pdf_sample = nullptr, *pdf_eval = nullptr, *row_prob = nullptr, *marg_prob = nullptr;
+    int32_t *row_alias = nullptr, *marg_alias = nullptr, *scratch = nullptr;
+    double *rowsum = nullptr, *totals = nullptr;
+    auto track = [&](void* p) { scene->allocations.push_back(p); };
+    FM_CUDA_TRY(ctx, cudaMalloc(&pdf_sample, n * sizeof(float)), "env tables");
+    track(pdf_sample);
+    FM_CUDA_TRY(ctx, cudaMalloc(&pdf_eval, n * sizeof(float)), "env tables");
+    track(pdf_eval);
+    FM_CUDA_TRY(ctx, cudaMalloc(&row_prob, n * sizeof(float)), "env tables");
+    track(row_prob);
+    FM_CUDA_TRY(ctx, cudaMalloc(&row_alias, n * sizeof(int32_t)), "env tables");
+    track(row_alias);
+    FM_CUDA_TRY(ctx, cudaMalloc(&marg_prob, h * sizeof(float)), "env tables");
+    track(marg_prob);
+    FM_CUDA_TRY(ctx, cudaMalloc(&marg_alias, h * sizeof(int32_t)), "env tables");
+    track(marg_alias);
+    // temporaries
+    FM_CUDA_TRY(ctx, cudaMalloc(&lum, n * sizeof(float)), "env tables");
+    FM_CUDA_TRY(ctx, cudaMalloc(&scratch, 2 * n * sizeof(int32_t)), "env tables");
+    FM_CUDA_TRY(ctx, cudaMalloc(&rowsum, h * sizeof(double)), "env tables");
+    FM_CUDA_TRY(ctx, cudaMalloc(&totals, 2 * sizeof(double)), "env tables");
+    cudaStream_t st = ctx->stream;
+    k_env_lum<<<(int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096), 256, 0, st>>>(tex, w, h, lum);
+    k_env_rowsum<<<h, 256, 0, st>>>(lum, w, rowsum);
+    k_env_totals<<<1, 256, 0, st>>>(rowsum, w, h, totals);
+    k_env_pdfs<<<(int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096), 256, 0, st>>>(lum, rowsum, totals, w, h,
+                                                                                       pdf_sample, pdf_eval);
+    k_env_alias_rows<<<(h + 63) / 64, 64, 0, st>>>(lum, w, h, row_prob, row_alias, scratch);
+    k_env_alias_marg<<<1, 1, 0, st>>>(rowsum, h, marg_prob, marg_alias, scratch);
+    cudaError_t e = cudaStreamSynchronize(st);
+    cudaFree(lum);
+    cudaFree(scratch);
+    cudaFree(rowsum);
+    cudaFree(totals);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "env tables");
+    FM_CUDA_TRY(ctx, cudaGetLastError(), "env tables");
+    env.w = w;
+    env.h = h;
+    env.pdf_sample = pdf_sample;
+    env.pdf_eval = pdf_eval;
+    env.row_prob = row_prob;
+    env.row_alias = row_alias;
+    env.marg_prob = marg_prob;
+    env.marg_alias = marg_alias;
+    return FM_OK;
+}
+
+}  // namespace fm

@@ -1,0 +1,50 @@
+// Host-side definitions shared by the C-ABI translation units.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "../../include/fumeng_b200.h"
+#include "fm_bvh_build.h"
+#include "fm_scene.cuh"
+
+struct fm_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string error;
+    uint32_t* d_status = nullptr;   // device status word: bit 0 stack overflow, bit 1 queue overflow
+    int num_sms = 148;
+};
+
+struct fm_scene {
+    fm::DevScene dev{};               // device pointers filled in
+    fm::DevScene* d_dev = nullptr;    // device copy of `dev` (for batched kernels)
+    std::vector<void*> allocations;   // everything to cudaFree on destroy
+    fm::BvhResult bvh;
+    int64_t num_objects = 0;
+    // host copies kept for validation and light sampling set-up
+    std::vector<fm::DevLight> lights;
+};
+
+namespace fm {
+
+inline fm_status set_error(fm_ctx* ctx, fm_status st, const std::string& msg)
+{
+    if (ctx) ctx->error = msg;
+    return st;
+}
+
+inline fm_status cuda_error(fm_ctx* ctx, cudaError_t e, const char* where)
+{
+    return set_error(ctx, FM_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define FM_CUDA_TRY(ctx, expr, where)                                   \
+    do {                                                                \
+        cudaError_t e__ = (expr);                                       \
+        if (e__ != cudaSuccess) return ::fm::cuda_error(ctx, e__, where); \
+    } while (0)
+
+// Environment-map importance tables (fm_env.cu).
+fm_status env_build_tables(fm_ctx* ctx, fm_scene* scene, const DevTexture& tex, DevEnv& env);
+
+}  // namespace fm

@@ -1,0 +1,232 @@
+"""Seeded synthetic workloads (the reference ships no scenes; its scene submodule is empty).
+
+Generators for the benchmark configurations:
+  cornell()        Cornell box, 5 walls + 2 spheres + area light (256x256, 16 spp, depth 5)
+  icosphere_mesh() icosphere subdivided `level` times, displaced by 0.05 * fBm of
+                   Perlin's improved noise (Perlin 2002), 6 octaves
+  sky_env()        HDR sky gradient x lognormal(0, 0.3) noise + a Gaussian sun lobe
+  single_mesh()    1.31M-triangle icosphere with per-vertex Disney parameters, thin lens
+  batch_scenes()   64 scenes of 1-40 displaced icospheres / subdivided boxes
+  hit_scene()      meshes + rectangles for hit-ID parity tests, with random rays
+All randomness comes from numpy Generators seeded by the caller.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .scene import Mesh, Rect, SceneSpec, Sphere, rgbe_quantize
+
+# ---- geometry -------------------------------------------------------------------------
+
+
+def icosahedron():
+    t = (1.0 + math.sqrt(5.0)) / 2.0
+    v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+                  [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], np.float64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    f = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2],
+                  [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5],
+                  [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]], np.int64)
+    return v, f
+
+
+def subdivide(v: np.ndarray, f: np.ndarray):
+    """One loop of midpoint subdivision projected to the unit sphere (20*4^L faces)."""
+    e = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+    es = np.sort(e, axis=1)
+    uniq, inv = np.unique(es, axis=0, return_inverse=True)
+    inv = inv.reshape(-1)
+    mid = v[uniq[:, 0]] + v[uniq[:, 1]]
+    mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+    base = len(v)
+    nf = len(f)
+    m01 = base + inv[:nf]
+    m12 = base + inv[nf:2 * nf]
+    m20 = base + inv[2 * nf:]
+    a, b, c = f[:, 0], f[:, 1], f[:, 2]
+    nf_ = np.concatenate([np.stack([a, m01, m20], 1), np.stack([b, m12, m01], 1), np.stack([c, m20, m12], 1),
+                          np.stack([m01, m12, m20], 1)])
+    return np.concatenate([v, mid]), nf_
+
+
+def icosphere(level: int):
+    v, f = icosahedron()
+    for _ in range(level):
+        v, f = subdivide(v, f)
+    return v, f
+
+
+class PerlinNoise:
+    """Perlin's improved noise (K. Perlin, "Improving Noise", SIGGRAPH 2002): quintic fade,
+    12 edge gradients selected by a hashed permutation table (seeded here)."""
+
+    GRAD = np.array([[1, 1, 0], [-1, 1, 0], [1, -1, 0], [-1, -1, 0], [1, 0, 1], [-1, 0, 1], [1, 0, -1], [-1, 0, -1],
+                     [0, 1, 1], [0, -1, 1], [0, 1, -1], [0, -1, -1], [1, 1, 0], [0, -1, 1], [-1, 1, 0], [0, -1, -1]],
+                    np.float64)
+
+    def __init__(self, seed: int):
+        p = np.random.default_rng(seed).permutation(256)
+        self.p = np.concatenate([p, p]).astype(np.int64)
+
+    @staticmethod
+    def _fade(t):
+        return t * t * t * (t * (t * 6 - 15) + 10)
+
+    def __call__(self, x, y, z):
+        X, Y, Z = np.floor(x).astype(np.int64) & 255, np.floor(y).astype(np.int64) & 255, np.floor(z).astype(np.int64) & 255
+        x, y, z = x - np.floor(x), y - np.floor(y), z - np.floor(z)
+        u, v, w = self._fade(x), self._fade(y), self._fade(z)
+        p = self.p
+        A, B = p[X] + Y, p[X + 1] + Y
+        AA, AB, BA, BB = p[A] + Z, p[A + 1] + Z, p[B] + Z, p[B + 1] + Z
+
+        def g(h, dx, dy, dz):
+            G = self.GRAD[h & 15]
+            return G[..., 0] * dx + G[..., 1] * dy + G[..., 2] * dz
+
+        def lerp(t, a, b):
+            return a + t * (b - a)
+        return lerp(w, lerp(v, lerp(u, g(p[AA], x, y, z), g(p[BA], x - 1, y, z)),
+                            lerp(u, g(p[AB], x, y - 1, z), g(p[BB], x - 1, y - 1, z))),
+                    lerp(v, lerp(u, g(p[AA + 1], x, y, z - 1), g(p[BA + 1], x - 1, y, z - 1)),
+                         lerp(u, g(p[AB + 1], x, y - 1, z - 1), g(p[BB + 1], x - 1, y - 1, z - 1))))
+
+    def fbm(self, P: np.ndarray, octaves=6, lacunarity=2.0, gain=0.5, freq=2.0):
+        out = np.zeros(len(P))
+        amp = 1.0
+        for _ in range(octaves):
+            out += amp * self(P[:, 0] * freq, P[:, 1] * freq, P[:, 2] * freq)
+            freq *= lacunarity
+            amp *= gain
+        return out
+
+
+def displaced_icosphere(level: int, seed: int, amp: float = 0.05):
+    v, f = icosphere(level)
+    n = PerlinNoise(seed).fbm(v)
+    return v * (1.0 + amp * n)[:, None], f
+
+
+def subdivided_box(n: int):
+    """Unit cube [-1,1]^3 with each face split into n x n quads (12 n^2 triangles)."""
+    verts, faces = [], []
+    g = np.linspace(-1.0, 1.0, n + 1)
+    for axis in range(3):
+        for sign in (-1.0, 1.0):
+            uu, vv = np.meshgrid(g, g, indexing="ij")
+            P = np.zeros((n + 1, n + 1, 3))
+            a1, a2 = (axis + 1) % 3, (axis + 2) % 3
+            P[..., axis] = sign
+            P[..., a1] = uu
+            P[..., a2] = vv
+            base = sum(len(x) for x in verts)
+            verts.append(P.reshape(-1, 3))
+            idx = np.arange((n + 1) * (n + 1)).reshape(n + 1, n + 1) + base
+            q0, q1, q2, q3 = idx[:-1, :-1], idx[1:, :-1], idx[1:, 1:], idx[:-1, 1:]
+            if sign > 0:
+                t1 = np.stack([q0, q1, q2], -1)
+                t2 = np.stack([q0, q2, q3], -1)
+            else:
+                t1 = np.stack([q0, q2, q1], -1)
+                t2 = np.stack([q0, q3, q2], -1)
+            faces.append(np.concatenate([t1.reshape(-1, 3), t2.reshape(-1, 3)]))
+    return np.concatenate(verts), np.concatenate(faces)
+
+
+# ---- environment maps ---------------------------------------------------------------
+
+
+def sky_env(w: int, h: int, seed: int, sun_dir=(0.4, 0.3, 0.866), sun_peak=5e4, sun_sigma_deg=0.5) -> np.ndarray:
+    """z-up lat-long HDR (row 0 = zenith): sky gradient x lognormal(0, 0.3) + sun lobe."""
+    rng = np.random.default_rng(seed)
+    j = (np.arange(h) + 0.5) / h
+    i = (np.arange(w) + 0.5) / w
+    theta = j * math.pi
+    phi = i * 2 * math.pi
+    TH, PH = np.meshgrid(theta, phi, indexing="ij")
+    d = np.stack([np.sin(TH) * np.cos(PH), np.sin(TH) * np.sin(PH), np.cos(TH)], -1)
+    up = np.clip(d[..., 2], -1, 1)
+    zen = np.array([0.25, 0.45, 1.0])
+    hor = np.array([0.9, 0.85, 0.8])
+    gnd = np.array([0.25, 0.22, 0.2])
+    t = np.clip(up, 0, 1)[..., None]
+    sky = np.where(up[..., None] >= 0, hor * (1 - t) + zen * t, gnd * (0.6 + 0.4 * (1 + up[..., None])))
+    noise = rng.lognormal(0.0, 0.3, size=(h, w, 1))
+    s = np.asarray(sun_dir, np.float64)
+    s /= np.linalg.norm(s)
+    ang = np.arccos(np.clip((d * s).sum(-1), -1, 1))
+    sig = math.radians(sun_sigma_deg)
+    sun = sun_peak * np.exp(-0.5 * (ang / sig) ** 2)
+    img = sky * noise + sun[..., None] * np.array([1.0, 0.95, 0.85])
+    return rgbe_quantize(img.astype(np.float32))
+
+
+# ---- scenes -------------------------------------------------------------------------
+
+
+def cornell(res: int = 256, spp: int = 16, depth: int = 5, rr_depth: int = 3) -> SceneSpec:
+    """Cornell box in [0,1]^3, camera at (0.5,0.5,-1.4) looking at the centre."""
+    cam = {"type": "pin_hole", "pos": [0.5, 0.5, -1.4], "look_at": [0.5, 0.5, 0.5], "up": [0, 1, 0], "fov": 40.0,
+           "aspect": 1.0}
+    ren = {"width": res, "height": res, "spp": spp, "depth": depth, "rr_depth": rr_depth, "rr_coef": 0.85}
+    mats = [
+        {"name": "white", "type": "lambert_diffuse", "basecolor": [0.73, 0.73, 0.73]},
+        {"name": "red", "type": "lambert_diffuse", "basecolor": [0.65, 0.05, 0.05]},
+        {"name": "green", "type": "lambert_diffuse", "basecolor": [0.12, 0.45, 0.15]},
+        {"name": "ball", "type": "lambert_diffuse", "basecolor": [0.8, 0.8, 0.8]},
+        # aluminium-like conductor
+        {"name": "mirror", "type": "specular_reflection", "color": [1, 1, 1], "eta_i": [1, 1, 1],
+         "eta_t": [1.66, 0.88, 0.52], "k": [9.2, 6.3, 4.8]},
+        {"name": "light", "type": "lambert_diffuse", "basecolor": [0.78, 0.78, 0.78]},
+    ]
+    objs = [
+        Rect((0, 0, 0), (0, 0, 1), (1, 0, 1), (1, 0, 0), "white"),            # floor  (normal +y)
+        Rect((0, 1, 0), (1, 1, 0), (1, 1, 1), (0, 1, 1), "white"),            # ceiling (normal -y)
+        Rect((0, 0, 1), (0, 1, 1), (1, 1, 1), (1, 0, 1), "white"),            # back (normal -z)
+        Rect((0, 0, 0), (0, 1, 0), (0, 1, 1), (0, 0, 1), "red"),              # left x=0 (normal +x)
+        Rect((1, 0, 0), (1, 0, 1), (1, 1, 1), (1, 1, 0), "green"),            # right x=1 (normal -x)
+        Sphere(0.15, translation=(0.3, 0.15, 0.4), material="ball"),
+        Sphere(0.15, translation=(0.7, 0.15, 0.6), material="mirror"),
+        Rect((0.375, 0.999, 0.375), (0.625, 0.999, 0.375), (0.625, 0.999, 0.625), (0.375, 0.999, 0.625), "light",
+             emittance=(17.0, 12.0, 4.0)),                                     # normal -y
+    ]
+    return SceneSpec(cam, ren, mats, objs)
+
+
+def random_rays(rng: np.random.Generator, n: int, lo, hi, min_component: float = 1e-3) -> np.ndarray:
+    """Rays with origins uniform in the box [lo, hi] and isotropic directions whose
+    components are all at least `min_component` in magnitude.  Layout n x 8:
+    ox oy oz tmin dx dy dz tmax (tmin 0, tmax FLT_MAX)."""
+    o = rng.uniform(lo, hi, size=(n, 3))
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    small = np.abs(d) < min_component
+    d[small] = np.sign(d[small] + 1e-30) * min_component
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r = np.zeros((n, 8), np.float32)
+    r[:, 0:3] = o
+    r[:, 4:7] = d
+    r[:, 3] = 0.0
+    r[:, 7] = np.finfo(np.float32).max
+    return r
+
+
+def hit_scene(seed: int, level: int = 4, boxes: int = 3) -> SceneSpec:
+    """Displaced icosphere + subdivided boxes + a few rectangles, identity transforms."""
+    rng = np.random.default_rng(seed)
+    objs = []
+    v, f = displaced_icosphere(level, seed)
+    objs.append(Mesh((v * 0.8).astype(np.float32), f, "m0"))
+    for b in range(boxes):
+        bv, bf = subdivided_box(4 + b)
+        s = rng.uniform(0.15, 0.35)
+        c = rng.uniform(-1.2, 1.2, size=3)
+        objs.append(Mesh((bv * s + c).astype(np.float32), bf, "m0"))
+    objs.append(Rect((-2, -1.5, -2), (-2, -1.5, 2), (2, -1.5, 2), (2, -1.5, -2), "m0"))
+    objs.append(Rect((-2, -2, 1.9), (2, -2, 1.9), (2, 2, 1.9), (-2, 2, 1.9), "m0"))
+    cam = {"type": "pin_hole", "pos": [0, 0, -4], "look_at": [0, 0, 0], "up": [0, 1, 0], "fov": 45.0, "aspect": 1.0}
+    ren = {"width": 64, "height": 64, "spp": 1, "depth": 4}
+    mats = [{"name": "m0", "type": "lambert_diffuse", "basecolor": [0.5, 0.5, 0.5]}]
+    return SceneSpec(cam, ren, mats, objs)

@@ -1,0 +1,221 @@
+/*
+ * fumeng_b200 — C-ABI of the B200 path-tracing core.
+ *
+ * This library replaces the reference engine's integrator hot path
+ * (hietwll/Fumeng: Renderer::DrawFrame -> PathTracer::RenderPixel -> Scene /
+ * Aggregate / Geometry / Material / Light) with CUDA kernels for sm_100a.  Callers
+ * flatten a scene into the plain arrays below (the package's C++ SceneLoader does it
+ * from the reference's JSON schema), create it once, and render it.
+ *
+ * Conventions
+ *  - Every entry point returns an fm_status; FM_OK is 0.  On failure the message is
+ *    available from fm_last_error(ctx).  No C++ exception crosses this boundary.
+ *  - A context owns one CUDA stream and all device memory of its scenes.  A context is
+ *    not thread-safe: use one context per host thread.
+ *  - Images are row-major float32 RGB, row 0 = top row, like the reference's Image
+ *    (src/engine/src/image/image.cpp:58-61).
+ *  - Rays are 8 floats: origin xyz, t_min, direction xyz, t_max.
+ *  - Buffers are host memory unless FM_FLAG_DEVICE_PTRS is passed, in which case they
+ *    are device pointers of the context's device.
+ */
+#ifndef FUMENG_B200_H
+#define FUMENG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    FM_OK = 0,
+    FM_ERR_INVALID = 1,        /* bad argument or scene description */
+    FM_ERR_OOM = 2,            /* device allocation failed */
+    FM_ERR_CUDA = 3,           /* CUDA runtime error */
+    FM_ERR_QUEUE_OVERFLOW = 4, /* a device queue or traversal stack overflowed */
+    FM_ERR_TIMEOUT = 5,        /* a bounded device wait ran out */
+    FM_ERR_NO_DEVICE = 6       /* no CUDA device / extension not usable */
+} fm_status;
+
+typedef struct fm_ctx fm_ctx;
+typedef struct fm_scene fm_scene;
+
+enum { FM_FLAG_DEVICE_PTRS = 1 };
+
+/* ---- textures ------------------------------------------------------------------ */
+enum { FM_WRAP_REPEAT = 0, FM_WRAP_CLAMP = 1 };
+enum { FM_FILTER_LINEAR = 0, FM_FILTER_NEAREST = 1 };
+
+/* Texture::Sample / ImageTexture (core/texture.h:70-120, texture/image_texture.cpp:13-44).
+ * texels: width*height*3 linear floats, row 0 = top (as decoded by Image). */
+typedef struct {
+    int32_t width, height;
+    const float* texels;
+    int32_t wrap_u, wrap_v;
+    int32_t filter;
+} fm_texture_desc;
+
+/* A material parameter: a constant (texture < 0) or an image texture index. */
+typedef struct {
+    int32_t texture;
+    float value[3];
+} fm_tex_ref;
+
+/* ---- materials ----------------------------------------------------------------- */
+enum {
+    FM_MAT_LAMBERT = 0,     /* material/lambert_diffuse.cpp */
+    FM_MAT_SPEC_REFL = 1,   /* material/specular_reflection.cpp (conductor Fresnel) */
+    FM_MAT_SPEC_TRANS = 2,  /* material/specular_transmission.cpp (dielectric) */
+    FM_MAT_DISNEY = 3       /* material/disney.cpp */
+};
+
+/* Per-vertex Disney attributes (extension): when vattr_offset >= 0, the Disney
+ * parameters basecolor.rgb, roughness, metallic, clearcoat are interpolated with the
+ * hit's barycentrics from fm_scene_desc.tri_vattr at [offset .. offset+6) of each
+ * triangle corner; the fm_tex_ref values of those six parameters are then ignored. */
+typedef struct {
+    int32_t type;
+    int32_t thin;
+    /* Lambert uses basecolor.  Disney (disney.cpp:627-662 channel rules: metallic reads
+     * channel z, roughness channel y, the others channel x). */
+    fm_tex_ref basecolor, metallic, specular, specular_tint, roughness, anisotropic, sheen,
+        sheen_tint, clearcoat, clearcoat_gloss, spec_trans, spec_trans_roughness, diff_trans,
+        flatness, ior;
+    /* specular transmission (SpecularTransmissionConfig, core/material.h:20-34) */
+    float reflect_color[3], refract_color[3];
+    float eta_i, eta_t;
+    /* specular reflection (CreateSpecularReflection, create/material.h:11) */
+    float color[3], cond_eta_i[3], cond_eta_t[3], cond_k[3];
+    int32_t vattr_offset;
+} fm_material_desc;
+
+/* ---- lights given explicitly (area lights come from emissive objects) ---------- */
+enum { FM_LIGHT_ENV = 0, FM_LIGHT_DIRECTIONAL = 1 };
+
+typedef struct {
+    int32_t type;
+    /* env (light/env_light.cpp): texture index, rotation in degrees (Z*Y*X), factor */
+    int32_t texture;
+    float rotation[3];
+    float factor;
+    /* directional (light/directional_light.cpp): radiance and normalized direction */
+    float radiance[3];
+    float direction[3];
+} fm_light_desc;
+
+/* ---- scene ----------------------------------------------------------------------
+ * Objects are the reference's RenderObjects in load order (scene_loader.h:202-252):
+ * one per mesh triangle, rectangle or sphere.  Object index = hit ID. */
+typedef struct {
+    int64_t num_objects;
+    const int32_t* obj_material;   /* [num_objects] index into materials */
+    const float* obj_emission;     /* [num_objects*3] emittance, or NULL for none */
+
+    /* mesh triangles, world space, corner order as in the OBJ face */
+    int64_t num_triangles;
+    const float* tri_pos;          /* [n*9]  v0, v1, v2 */
+    const float* tri_normal;       /* [n*9]  or NULL */
+    const uint8_t* tri_has_normal; /* [n]    or NULL (all have normals iff tri_normal) */
+    const float* tri_uv;           /* [n*6]  (u, 1-v) per corner as triangle.cpp:152, or NULL */
+    const int32_t* tri_object;     /* [n]    object index */
+    const float* tri_vattr;        /* [n*3*vattr_dim] per-corner attributes, or NULL */
+    int32_t vattr_dim;
+
+    /* rectangles (geometry/rectangle.cpp): pa, pb, pc, pd */
+    int64_t num_rects;
+    const float* rect_pts;         /* [n*12] */
+    const int32_t* rect_object;    /* [n] */
+
+    /* spheres (geometry/sphere.cpp): object-space radius and the object-to-world
+     * transform as a row-major 4x4 */
+    int64_t num_spheres;
+    const float* sphere_radius;    /* [n] */
+    const float* sphere_xform;     /* [n*16] */
+    const int32_t* sphere_object;  /* [n] */
+
+    int32_t num_materials;
+    const fm_material_desc* materials;
+    int32_t num_textures;
+    const fm_texture_desc* textures;
+    int32_t num_lights;            /* JSON lights, appended after area lights */
+    const fm_light_desc* lights;
+} fm_scene_desc;
+
+/* ---- camera and render parameters ---------------------------------------------- */
+enum { FM_CAMERA_PINHOLE = 0, FM_CAMERA_THIN_LENS = 1 };
+
+/* PinHoleCameraConfig / ThinLensCameraConfig (core/camera.h:9-41) */
+typedef struct {
+    int32_t type;
+    float pos[3], look_at[3], up[3];
+    float fov;            /* degrees */
+    float aspect;
+    float focal_distance;
+    float lens_radius;
+} fm_camera;
+
+enum { FM_MODE_MEGAKERNEL = 0, FM_MODE_WAVEFRONT = 1 };
+
+/* PathTracerConfig (core/renderer.h:17-60) plus the seed of the counter-based RNG. */
+typedef struct {
+    int32_t width, height, spp;
+    int32_t depth, direct_loop, rr_depth;
+    float rr_coef;
+    uint64_t seed;
+    int32_t mode;
+    int32_t sample_offset;   /* first sample index (for split / decorrelated renders) */
+} fm_render_params;
+
+/* Counters of one render, read back after it completes. */
+typedef struct {
+    int64_t paths;            /* camera samples completed */
+    int64_t closest_rays;     /* closest-hit queries traced */
+    int64_t shadow_rays;      /* any-hit queries traced */
+    int64_t bounces;          /* shading events */
+    int64_t nan_samples;      /* samples whose radiance was not finite */
+    double kernel_ms;         /* device time of the render kernels */
+} fm_render_stats;
+
+/* ---- entry points ---------------------------------------------------------------- */
+
+/* Replaces: nothing in the reference (it has no device); creates the CUDA context
+ * holder used by every other call. */
+fm_status fm_ctx_create(int device, fm_ctx** out);
+void fm_ctx_destroy(fm_ctx* ctx);
+const char* fm_last_error(const fm_ctx* ctx);
+
+/* Replaces: SceneLoader::ParseScene's aggregate construction
+ * (scene_loader.h:86-146 -> CreateBVHAggregate, accelerator/bvh_aggregate.cpp:126-155)
+ * and the area-light collection of Scene::Scene (core/scene.h:21-25).  Copies the
+ * description to the device and builds the BVH there (binned SAH, 8-wide nodes). */
+fm_status fm_scene_create(fm_ctx* ctx, const fm_scene_desc* desc, fm_scene** out);
+fm_status fm_scene_destroy(fm_ctx* ctx, fm_scene* scene);
+/* BVH statistics: wide nodes, leaf primitive slots, max depth, build milliseconds. */
+fm_status fm_scene_bvh_stats(fm_ctx* ctx, const fm_scene* scene, int64_t* nodes, int64_t* prims,
+                             int32_t* depth, double* build_ms);
+
+/* Replaces: Aggregate::GetIntersect (core/aggregate.h:30, accelerator/bvh_aggregate.cpp:
+ * 167-176).  rays: n x 8 floats.  obj_id[i] = object index of the closest hit or -1;
+ * t[i] = its distance (+inf on a miss). */
+fm_status fm_trace_closest(fm_ctx* ctx, const fm_scene* scene, const float* rays, int64_t n,
+                           int32_t* obj_id, float* t, int32_t flags);
+
+/* Replaces: Aggregate::IsIntersect (core/aggregate.h:24, bvh_aggregate.cpp:157-165).
+ * occluded[i] = 1 if any object is hit with t in (t_min, t_max). */
+fm_status fm_trace_any(fm_ctx* ctx, const fm_scene* scene, const float* rays, int64_t n,
+                       uint8_t* occluded, int32_t flags);
+
+/* Replaces: Renderer::DrawFrame's sample loop and PathTracer::RenderPixel
+ * (core/renderer.h:84-117, renderer/path_tracing.cpp:34-229).  Writes width*height*3
+ * floats to each non-NULL output: mean color, mean albedo, mean normal over spp
+ * samples.  stats may be NULL. */
+fm_status fm_render(fm_ctx* ctx, const fm_scene* scene, const fm_camera* camera,
+                    const fm_render_params* params, float* rgb, float* albedo, float* normal,
+                    int32_t flags, fm_render_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FUMENG_B200_H */

@@ -1,0 +1,34 @@
+"""Closest-hit object IDs and distances of the CUDA BVH match the reference's built-in BVH
+bit for bit on seeded ray sets, excluding rays whose two nearest hits lie within 1e-6
+relative t; occlusion queries match exactly."""
+import numpy as np
+import pytest
+
+from golden.make_golden import HIT_CASES, hit_inputs
+
+GOLDEN_DIR = __import__("pathlib").Path(__file__).resolve().parent / "golden"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", HIT_CASES, ids=[c[0] for c in HIT_CASES])
+def test_closest_and_any_hit_bit_exact(ctx, case):
+    spec, rays, shadow, digest, = hit_inputs(case)
+    g = np.load(GOLDEN_DIR / f"{case[0]}.npz")
+    assert str(g["sha256"]) == digest
+    holder = spec.to_desc()
+    scene = ctx.create_scene(holder)
+    try:
+        st = scene.bvh_stats()
+        assert st["prims"] == holder.desc.num_triangles + 2 * holder.desc.num_rects
+        obj, t = scene.trace_closest(rays)
+        occ = scene.trace_any(shadow)
+    finally:
+        scene.destroy()
+    gt1, gt2 = g["t"], g["t2"]
+    tie = np.abs(gt2 - gt1) <= 1e-6 * np.abs(gt1)
+    keep = ~tie
+    mism = np.nonzero(obj[keep] != g["obj"][keep])[0]
+    assert mism.size == 0, f"{mism.size} object-ID mismatches of {keep.sum()} (first {mism[:10]})"
+    assert np.array_equal(t[keep], gt1[keep])
+    ref_occ = np.unpackbits(g["occ"])[: len(shadow)]
+    assert np.array_equal(occ, ref_occ), f"{int((occ != ref_occ).sum())} occlusion mismatches"
