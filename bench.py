@@ -1,0 +1,361 @@
+#!/usr/bin/env python
+"""Throughput benchmark: 64 independent scenes rendered in one batched wavefront.
+
+Workload (one step): 64 seeded synthetic scenes (fumeng_b200.synth.batch_scene: 1-40
+displaced icospheres / subdivided boxes per scene, 1k-200k triangles each, 2.4M in
+total; Disney / Lambert / dielectric materials; one area light and a 512x256 HDR sky;
+resolutions 128^2-512^2, 4-64 spp, depth 8) rendered once through fm_render_batch.
+Metric: camera paths per second (a path = one pixel sample, counted when complete).
+
+    python bench.py [--steps K] [--warmup W] [--impl ours|reference]
+    torchrun --nproc-per-node N bench.py --gpus N ...   (replicas: each rank renders its own batch)
+
+value  : device-resident scenes, device output images; time = device time of the K
+         timed steps (CUDA events, max over ranks).
+e2e    : the same metric through the C-ABI from host memory: every step creates the 64
+         scenes from host descriptors (upload + device BVH build + env tables), renders
+         into host images and destroys the scenes.
+The plain per-pixel megakernel is timed on the same batch for comparison.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mpaths/s batched wavefront vs plain megakernel at relMSE≤1e-3; adjoint/fwd ratio"
+WORKLOAD = "batched: 64 scenes x (1-40 displaced icosphere/box meshes, 1k-200k tris), 512x256 HDR env + 1 area light, 128^2-512^2, 4-64 spp, depth 8"
+NSCENES = 64
+# DRAM bytes the trace kernel moved per traced ray in one ncu capture of this workload
+# (profiles/k_wf_trace_batched64.md); None until captured.
+TRACE_DRAM_BYTES_PER_RAY = None
+
+
+def measured_peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(prefix="fm_clocks_", suffix=".csv")[1])
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in self.path.read_text().strip().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        finally:
+            try:
+                self.path.unlink()
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if len(r) > 5 + k and "Active" in r[5 + k]
+                          and "Not" not in r[5 + k]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def bvh_depth_estimate(nprims: int) -> int:
+    return max(1, math.ceil(math.log(max(nprims, 5) / 4.0, 8)))
+
+
+def desc_bytes(holder) -> int:
+    n = 0
+    for name in ("obj_material", "obj_emission", "tri_pos", "tri_normal", "tri_has_normal", "tri_uv", "tri_object",
+                 "tri_vattr", "rect_pts", "rect_object", "sphere_radius", "sphere_xform", "sphere_object"):
+        a = getattr(holder, name, None)
+        if a is not None:
+            n += a.nbytes
+    n += sum(a.nbytes for a in holder.tex_arrays)
+    return n
+
+
+def scene_indices(rank: int):
+    return [rank * NSCENES + s for s in range(NSCENES)]
+
+
+# ---- reference arm (CPU) ---------------------------------------------------------------
+
+def run_reference(args, specs=None, steps=None, warmup=None, sample_scenes=2, spp=1):
+    """The reference's own CPU integrator (oracle/_ref float build, RenderPixel per camera
+    sample on all host threads) on a bounded sample of the workload per step."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import fmref  # noqa: E402  (test/baseline infrastructure)
+    from fumeng_b200 import synth
+    if not fmref.available("float"):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libfmref_f.so was not built (no reference sources)"}
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
+    threads = os.cpu_count() or 1
+    tmp = Path(tempfile.mkdtemp(prefix="fm_ref_"))
+    times, paths = [], []
+    loaded = {}
+    for it in range(warmup + steps):
+        ids = [(it * sample_scenes + k) % NSCENES for k in range(sample_scenes)]
+        t_step, p_step = 0.0, 0
+        for s in ids:
+            if s not in loaded:
+                spec = synth.batch_scene(s)
+                loaded[s] = fmref.RefScene(spec.write(tmp / f"s{s}"), "float")
+            rs = loaded[s]
+            w, h, _ = rs.image_size()
+            t0 = time.perf_counter()
+            rs.render(spp, seed=it, threads=threads)
+            t_step += time.perf_counter() - t0
+            p_step += w * h * spp
+        if it >= warmup:
+            times.append(t_step)
+            paths.append(p_step)
+    value = sum(paths) / sum(times) / 1e6
+    return {"value": value, "unit": "Mpaths/s", "cores": threads, "kind": "reference",
+            "sample": f"{sample_scenes} scenes x {spp} spp per step (scenes rotate through the batch), "
+                      f"reference float build, all {threads} host threads",
+            "ms_per_step": 1e3 * sum(times) / len(times)}
+
+
+# ---- our arm (GPU) ---------------------------------------------------------------------
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--mk-steps", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        r = run_reference(args)
+        if "unavailable" in r:
+            print(json.dumps(r))
+            return
+        line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": "Mpaths/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": {"workload": WORKLOAD, "scenes": NSCENES},
+                "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": r["value"], "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    import fumeng_b200 as fb
+    from fumeng_b200 import synth
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    ctx = fb.Context(local_rank)
+    specs = [synth.batch_scene(s) for s in scene_indices(rank)]
+    holders = [s.to_desc() for s in specs]
+    cams = [s.camera_struct() for s in specs]
+    params_wf = [s.render_params(seed=1, mode=fb.FM_MODE_WAVEFRONT) for s in specs]
+    params_mk = [s.render_params(seed=1, mode=fb.FM_MODE_MEGAKERNEL) for s in specs]
+    paths_per_step = sum(p.width * p.height * p.spp for p in params_wf)
+    tris = sum(h.desc.num_triangles for h in holders)
+    scenes = [ctx.create_scene(h) for h in holders]
+    build_ms = sum(s.bvh_stats()["build_ms"] for s in scenes)
+    outs = [torch.empty((p.height, p.width, 3), device="cuda", dtype=torch.float32) for p in params_wf]
+    out_ptrs = [o.data_ptr() for o in outs]
+
+    tuning = ctx.autotune_batch(scenes, cams, params_wf)
+
+    def step_wf(profile=False):
+        return ctx.render_batch(scenes, cams, params_wf, tuning=tuning, device_outputs=out_ptrs, profile=profile)[3]
+
+    for _ in range(args.warmup):
+        step_wf()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    totals = {"paths": 0, "closest": 0, "shadow": 0, "bounces": 0, "nans": 0, "trace_ms": 0.0, "shade_ms": 0.0,
+              "launches": 0, "kernel_ms": 0.0}
+    barrier()
+    with ClockSampler(local_rank) as clk:
+        ev0.record()
+        for _ in range(args.steps):
+            st = step_wf(profile=True)
+            totals["paths"] += st.paths
+            totals["closest"] += st.closest_rays
+            totals["shadow"] += st.shadow_rays
+            totals["bounces"] += st.bounces
+            totals["nans"] += st.nan_samples
+            totals["trace_ms"] += st.trace_ms
+            totals["shade_ms"] += st.shade_ms
+            totals["launches"] += st.launches
+            totals["kernel_ms"] += st.kernel_ms
+        ev1.record()
+        barrier()
+    clocks = clk.summary()
+    elapsed_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    all_paths = sum_over_ranks(float(totals["paths"]))
+    value = all_paths / (elapsed_ms / 1e3) / 1e6
+    assert totals["paths"] == paths_per_step * args.steps, (totals["paths"], paths_per_step)
+
+    # megakernel on the same batch
+    mk = None
+    if args.mk_steps > 0:
+        ctx.render_batch(scenes, cams, params_mk, device_outputs=out_ptrs)   # warm-up
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.mk_steps):
+            ctx.render_batch(scenes, cams, params_mk, device_outputs=out_ptrs)
+        e1.record()
+        barrier()
+        mk_ms = max_over_ranks(e0.elapsed_time(e1))
+        mk = {"value": sum_over_ranks(float(paths_per_step * args.mk_steps)) / (mk_ms / 1e3) / 1e6,
+              "ms_per_step": mk_ms / args.mk_steps, "steps": args.mk_steps}
+
+    # roofline of the trace kernel (algorithmic bytes per the fixed per-ray formula)
+    depth_eff = sum(bvh_depth_estimate(h.desc.num_triangles + 2 * h.desc.num_rects) * p.width * p.height * p.spp
+                    for h, p in zip(holders, params_wf)) / paths_per_step
+    closest_b = 32 + 16 + 80 * depth_eff + 160
+    shadow_b = 32 + 4 + 80 * depth_eff + 160
+    alg_bytes = totals["closest"] * closest_b + totals["shadow"] * shadow_b
+    peak, peak_kind = measured_peak_hbm()
+    achieved = alg_bytes / (totals["trace_ms"] / 1e3) / 1e9 if totals["trace_ms"] > 0 else None
+    launches_trace = max(1, totals["launches"] // 3)
+    traffic = None
+    if TRACE_DRAM_BYTES_PER_RAY is not None:
+        traffic = TRACE_DRAM_BYTES_PER_RAY * (totals["closest"] + totals["shadow"]) / launches_trace
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "kernel": "k_wf_trace", "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+                "alg_bytes_per_closest_ray": closest_b, "alg_bytes_per_shadow_ray": shadow_b,
+                "trace_share_of_step": totals["trace_ms"] / max(totals["kernel_ms"], 1e-9)}
+
+    # end to end through the C-ABI from host memory
+    e2e = None
+    if args.e2e_steps > 0:
+        h2d = sum(desc_bytes(h) for h in holders)
+        d2h = sum(p.width * p.height * 3 * 4 for p in params_wf)
+
+        def step_e2e():
+            sc = [ctx.create_scene(h) for h in holders]
+            ctx.render_batch(sc, cams, params_wf, tuning=tuning)
+            for s in sc:
+                s.destroy()
+        step_e2e()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.e2e_steps):
+            step_e2e()
+        e1.record()
+        barrier()
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+        e2e = {"value": sum_over_ranks(float(paths_per_step * args.e2e_steps)) / (e2e_ms / 1e3) / 1e6,
+               "unit": "Mpaths/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "ms_per_step": e2e_ms / args.e2e_steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = run_reference(args, steps=2, warmup=0, sample_scenes=4, spp=1)
+        cpu = {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")} if "unavailable" not in r else r
+
+    for s in scenes:
+        s.destroy()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "scenes": NSCENES, "triangles": int(tris),
+                       "paths_per_step": int(paths_per_step), "depth": 8,
+                       "parallelism": f"replicas x{world} (each rank renders its own 64-scene batch)",
+                       "l2": "inputs larger than L2 (scene data + path state exceed 126 MB)",
+                       "bvh_build_ms_total": build_ms, "tuning": tuning.as_dict()},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(totals["launches"]),
+            "clocks": clocks, "megakernel": mk,
+            "wavefront_vs_megakernel": (value / mk["value"]) if mk else None,
+            "per_path": {"closest_rays": totals["closest"] / totals["paths"],
+                         "shadow_rays": totals["shadow"] / totals["paths"],
+                         "bounces": totals["bounces"] / totals["paths"]},
+            "nan_samples": int(totals["nans"]),
+        }
+        print(json.dumps(line))
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -18,6 +18,7 @@ LIB_PATH = _PKG / "libfumeng_b200.so"
 
 FM_OK, FM_ERR_INVALID, FM_ERR_OOM, FM_ERR_CUDA, FM_ERR_QUEUE_OVERFLOW, FM_ERR_TIMEOUT, FM_ERR_NO_DEVICE = range(7)
 FM_FLAG_DEVICE_PTRS = 1
+FM_FLAG_PROFILE = 2
 FM_WRAP_REPEAT, FM_WRAP_CLAMP = 0, 1
 FM_FILTER_LINEAR, FM_FILTER_NEAREST = 0, 1
 FM_MAT_LAMBERT, FM_MAT_SPEC_REFL, FM_MAT_SPEC_TRANS, FM_MAT_DISNEY = 0, 1, 2, 3
@@ -81,7 +82,17 @@ class RenderParams(C.Structure):
 
 class RenderStats(C.Structure):
     _fields_ = [("paths", C.c_int64), ("closest_rays", C.c_int64), ("shadow_rays", C.c_int64),
-                ("bounces", C.c_int64), ("nan_samples", C.c_int64), ("kernel_ms", C.c_double)]
+                ("bounces", C.c_int64), ("nan_samples", C.c_int64), ("kernel_ms", C.c_double),
+                ("trace_ms", C.c_double), ("shade_ms", C.c_double), ("launches", C.c_int64)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("pool", C.c_int64), ("trace_block", C.c_int32), ("shade_block", C.c_int32),
+                ("iters_per_graph", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {"pool": self.pool, "trace_block": self.trace_block, "shade_block": self.shade_block,
+                "iters_per_graph": self.iters_per_graph}
 
 
 class FumengError(RuntimeError):
@@ -115,6 +126,11 @@ def load_library() -> C.CDLL:
         "fm_trace_any": ([vp, vp, vp, C.c_int64, vp, C.c_int32], C.c_int),
         "fm_render": ([vp, vp, C.POINTER(Camera), C.POINTER(RenderParams), vp, vp, vp, C.c_int32,
                        C.POINTER(RenderStats)], C.c_int),
+        "fm_render_batch": ([vp, C.c_int32, C.POINTER(vp), C.POINTER(Camera), C.POINTER(RenderParams),
+                             C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.c_int32, C.POINTER(Tuning),
+                             C.POINTER(RenderStats)], C.c_int),
+        "fm_autotune_batch": ([vp, C.c_int32, C.POINTER(vp), C.POINTER(Camera), C.POINTER(RenderParams),
+                               C.POINTER(Tuning)], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -125,7 +141,8 @@ def load_library() -> C.CDLL:
 
 
 EXPORTED_SYMBOLS = ["fm_ctx_create", "fm_ctx_destroy", "fm_last_error", "fm_scene_create", "fm_scene_destroy",
-                    "fm_scene_bvh_stats", "fm_trace_closest", "fm_trace_any", "fm_render"]
+                    "fm_scene_bvh_stats", "fm_trace_closest", "fm_trace_any", "fm_render", "fm_render_batch",
+                    "fm_autotune_batch"]
 
 
 def _ptr(a, ctype=C.c_void_p):
@@ -165,6 +182,43 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    def _batch_args(self, scenes, cams, params):
+        n = len(scenes)
+        sc = (C.c_void_p * n)(*[s.h.value if hasattr(s.h, "value") else s.h for s in scenes])
+        ca = (Camera * n)(*cams)
+        pa = (RenderParams * n)(*params)
+        return n, sc, ca, pa
+
+    def render_batch(self, scenes, cams, params, want_aov: bool = False, tuning: Tuning | None = None,
+                     device_outputs=None, profile: bool = False):
+        """Render view i = (scenes[i], cams[i], params[i]) for all i in one call.
+
+        device_outputs: optional list of device pointers (ints) for the rgb images, which
+        makes the call skip the device-to-host copies (FM_FLAG_DEVICE_PTRS)."""
+        n, sc, ca, pa = self._batch_args(scenes, cams, params)
+        stats = RenderStats()
+        tp = C.byref(tuning) if tuning is not None else None
+        if device_outputs is not None:
+            rgb_p = (C.c_void_p * n)(*device_outputs)
+            flags = FM_FLAG_DEVICE_PTRS | (FM_FLAG_PROFILE if profile else 0)
+            self.check(self.lib.fm_render_batch(self.h, n, sc, ca, pa, rgb_p, None, None, flags, tp, C.byref(stats)))
+            return None, None, None, stats
+        rgb = [np.empty((p.height, p.width, 3), np.float32) for p in params]
+        alb = [np.empty((p.height, p.width, 3), np.float32) for p in params] if want_aov else None
+        nrm = [np.empty((p.height, p.width, 3), np.float32) for p in params] if want_aov else None
+        rgb_p = (C.c_void_p * n)(*[a.ctypes.data for a in rgb])
+        alb_p = (C.c_void_p * n)(*[a.ctypes.data for a in alb]) if want_aov else None
+        nrm_p = (C.c_void_p * n)(*[a.ctypes.data for a in nrm]) if want_aov else None
+        flags = FM_FLAG_PROFILE if profile else 0
+        self.check(self.lib.fm_render_batch(self.h, n, sc, ca, pa, rgb_p, alb_p, nrm_p, flags, tp, C.byref(stats)))
+        return rgb, alb, nrm, stats
+
+    def autotune_batch(self, scenes, cams, params) -> Tuning:
+        n, sc, ca, pa = self._batch_args(scenes, cams, params)
+        t = Tuning()
+        self.check(self.lib.fm_autotune_batch(self.h, n, sc, ca, pa, C.byref(t)))
+        return t
 
     def create_scene(self, desc_holder) -> "Scene":
         h = C.c_void_p()

@@ -1,0 +1,287 @@
+// Batched rendering (many views / scenes in one persistent wavefront) and the autotuner.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "fm_render.h"
+
+namespace fm {
+
+namespace {
+
+std::tuple<int, int, int> shape_class(int n, const fm_render_params* params, const fm_scene* const* scenes)
+{
+    double samples = 0.0;
+    int lights = 0;
+    for (int i = 0; i < n; ++i) {
+        samples += (double)params[i].width * params[i].height * params[i].spp;
+        lights = std::max(lights, scenes[i]->dev.num_lights);
+    }
+    return {n, (int)std::floor(std::log2(std::max(1.0, samples))), lights};
+}
+
+WfTuning to_wf(const fm_tuning& t)
+{
+    WfTuning w;
+    w.pool = t.pool;
+    w.trace_block = t.trace_block;
+    w.shade_block = t.shade_block;
+    w.iters_per_graph = t.iters_per_graph;
+    return w;
+}
+
+fm_status check_tuning(fm_ctx* ctx, const fm_tuning& t)
+{
+    auto okb = [](int b) { return b == 32 || b == 64 || b == 128 || b == 256; };
+    if (t.pool < 1024 || t.pool > ((int64_t)1 << 26) || !okb(t.trace_block) || !okb(t.shade_block) ||
+        t.iters_per_graph < 1 || t.iters_per_graph > 64)
+        return set_error(ctx, FM_ERR_INVALID, "tuning out of range");
+    return FM_OK;
+}
+
+// Views rendering into the given device images (spp overridden when spp_override > 0).
+std::vector<WfView> make_views(int n, const fm_scene* const* scenes, const fm_camera* cams, const fm_render_params* params,
+                               float* const* rgb, float* const* alb, float* const* nrm, int spp_override)
+{
+    std::vector<WfView> v((size_t)n);
+    for (int i = 0; i < n; ++i) {
+        WfView& w = v[i];
+        w = WfView{};
+        w.scene = scenes[i]->d_dev;
+        w.cam = make_camera(cams[i]);
+        fm_render_params p = params[i];
+        if (spp_override > 0) p.spp = std::min(p.spp, spp_override);
+        w.cfg = make_cfg(p);
+        w.rgb = rgb[i];
+        w.alb = alb ? alb[i] : nullptr;
+        w.nrm = nrm ? nrm[i] : nullptr;
+    }
+    return v;
+}
+
+fm_status validate_batch(fm_ctx* ctx, int32_t n, const fm_scene* const* scenes, const fm_camera* cams,
+                         const fm_render_params* params)
+{
+    if (n <= 0 || !scenes || !cams || !params) return set_error(ctx, FM_ERR_INVALID, "batch: bad arguments");
+    for (int i = 0; i < n; ++i) {
+        fm_status st = validate_render(ctx, scenes[i], &cams[i], &params[i]);
+        if (st != FM_OK) return st;
+        if (params[i].mode != params[0].mode) return set_error(ctx, FM_ERR_INVALID, "batch: all views must use one mode");
+    }
+    return FM_OK;
+}
+
+fm_status autotune(fm_ctx* ctx, int32_t n, const fm_scene* const* scenes, const fm_camera* cams,
+                   const fm_render_params* params, fm_tuning* out)
+{
+    // scratch images for the trial renders
+    std::vector<float*> imgs((size_t)n, nullptr);
+    size_t total = 0;
+    for (int i = 0; i < n; ++i) total += (size_t)params[i].width * params[i].height * 3;
+    float* buf = nullptr;
+    FM_CUDA_TRY(ctx, cudaMalloc(&buf, total * sizeof(float)), "autotune alloc");
+    Counters* cnt = nullptr;
+    if (cudaMalloc(&cnt, sizeof(Counters)) != cudaSuccess) {
+        cudaFree(buf);
+        return set_error(ctx, FM_ERR_OOM, "autotune alloc");
+    }
+    size_t off = 0;
+    for (int i = 0; i < n; ++i) {
+        imgs[i] = buf + off;
+        off += (size_t)params[i].width * params[i].height * 3;
+    }
+    const std::vector<WfView> views = make_views(n, scenes, cams, params, imgs.data(), nullptr, nullptr, 2);
+    double samples = 0.0;
+    for (const auto& v : views) samples += (double)v.cfg.width * v.cfg.height * v.cfg.spp;
+    fm_tuning best{(int64_t)1 << 21, 128, 128, 8};
+    double best_rate = -1.0;
+    fm_status st = FM_OK;
+    auto trial = [&](fm_tuning t) -> fm_status {
+        WfTimes tm;
+        cudaMemsetAsync(cnt, 0, sizeof(Counters), ctx->stream);
+        fm_status s = wavefront_views(ctx, views, to_wf(t), cnt, &tm);
+        if (s != FM_OK) return s;
+        const double ms = tm.total_ms;
+        const double rate = samples / std::max(ms, 1e-3);
+        if (rate > best_rate) {
+            best_rate = rate;
+            best = t;
+        }
+        return FM_OK;
+    };
+    // warm-up, then coordinate descent over pool size, trace block, shade block, graph depth
+    st = trial(best);
+    best_rate = -1.0;
+    const int64_t pools[] = {(int64_t)1 << 19, (int64_t)1 << 20, (int64_t)1 << 21, (int64_t)1 << 22};
+    for (int64_t p : pools) {
+        if (st != FM_OK) break;
+        if ((double)p > samples * 2.0 && p != pools[0]) continue;
+        fm_tuning t = best;
+        t.pool = p;
+        st = trial(t);
+    }
+    for (int b : {64, 128, 256}) {
+        if (st != FM_OK) break;
+        fm_tuning t = best;
+        t.trace_block = b;
+        st = trial(t);
+    }
+    for (int b : {64, 128, 256}) {
+        if (st != FM_OK) break;
+        fm_tuning t = best;
+        t.shade_block = b;
+        st = trial(t);
+    }
+    for (int k : {4, 8, 16}) {
+        if (st != FM_OK) break;
+        fm_tuning t = best;
+        t.iters_per_graph = k;
+        st = trial(t);
+    }
+    cudaFree(buf);
+    cudaFree(cnt);
+    if (st != FM_OK) return st;
+    *out = best;
+    return FM_OK;
+}
+
+}  // namespace
+
+}  // namespace fm
+
+using namespace fm;
+
+extern "C" fm_status fm_autotune_batch(fm_ctx* ctx, int32_t n, const fm_scene* const* scenes, const fm_camera* cameras,
+                                       const fm_render_params* params, fm_tuning* out)
+{
+    if (!ctx) return FM_ERR_INVALID;
+    if (!out) return set_error(ctx, FM_ERR_INVALID, "autotune: null output");
+    fm_status st = validate_batch(ctx, n, scenes, cameras, params);
+    if (st != FM_OK) return st;
+    FM_CUDA_TRY(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+    st = autotune(ctx, n, scenes, cameras, params, out);
+    if (st == FM_OK) ctx->tune_cache[shape_class(n, params, scenes)] = *out;
+    return st;
+}
+
+extern "C" fm_status fm_render_batch(fm_ctx* ctx, int32_t n, const fm_scene* const* scenes, const fm_camera* cameras,
+                                     const fm_render_params* params, float* const* rgb, float* const* albedo,
+                                     float* const* normal, int32_t flags, const fm_tuning* tuning,
+                                     fm_render_stats* stats)
+{
+    if (!ctx) return FM_ERR_INVALID;
+    fm_status st = validate_batch(ctx, n, scenes, cameras, params);
+    if (st != FM_OK) return st;
+    if (!rgb) return set_error(ctx, FM_ERR_INVALID, "batch: rgb is null");
+    for (int i = 0; i < n; ++i)
+        if (!rgb[i]) return set_error(ctx, FM_ERR_INVALID, "batch: rgb entry is null");
+    FM_CUDA_TRY(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+    const bool dev = (flags & FM_FLAG_DEVICE_PTRS) != 0;
+    const bool wave = params[0].mode == FM_MODE_WAVEFRONT;
+    fm_tuning tune{(int64_t)1 << 21, 128, 128, 8};
+    if (wave) {
+        if (tuning) {
+            st = check_tuning(ctx, *tuning);
+            if (st != FM_OK) return st;
+            tune = *tuning;
+        } else {
+            const auto key = shape_class(n, params, scenes);
+            auto it = ctx->tune_cache.find(key);
+            if (it == ctx->tune_cache.end()) {
+                st = autotune(ctx, n, scenes, cameras, params, &tune);
+                if (st != FM_OK) return st;
+                ctx->tune_cache[key] = tune;
+            } else {
+                tune = it->second;
+            }
+        }
+    }
+    // device images (staging when the caller passed host buffers)
+    std::vector<float*> d_rgb((size_t)n), d_alb((size_t)n, nullptr), d_nrm((size_t)n, nullptr);
+    std::vector<size_t> bytes((size_t)n);
+    char* staging = nullptr;
+    size_t total = 0;
+    for (int i = 0; i < n; ++i) {
+        bytes[i] = (size_t)params[i].width * params[i].height * 3 * sizeof(float);
+        if (!dev) total += bytes[i] * (1 + (albedo && albedo[i] ? 1 : 0) + (normal && normal[i] ? 1 : 0));
+    }
+    Counters* d_cnt = nullptr;
+    FM_CUDA_TRY(ctx, cudaMallocAsync((void**)&staging, total + 256, ctx->stream), "batch alloc");
+    d_cnt = reinterpret_cast<Counters*>(staging);
+    {
+        char* q = staging + 256;
+        for (int i = 0; i < n; ++i) {
+            if (dev) {
+                d_rgb[i] = rgb[i];
+                d_alb[i] = albedo ? albedo[i] : nullptr;
+                d_nrm[i] = normal ? normal[i] : nullptr;
+                continue;
+            }
+            d_rgb[i] = reinterpret_cast<float*>(q);
+            q += bytes[i];
+            if (albedo && albedo[i]) {
+                d_alb[i] = reinterpret_cast<float*>(q);
+                q += bytes[i];
+            }
+            if (normal && normal[i]) {
+                d_nrm[i] = reinterpret_cast<float*>(q);
+                q += bytes[i];
+            }
+        }
+    }
+    FM_CUDA_TRY(ctx, cudaMemsetAsync(d_cnt, 0, sizeof(Counters), ctx->stream), "batch");
+    FM_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), ctx->stream), "batch");
+    double ms = 0.0;
+    WfTimes tm;
+    if (wave) {
+        const std::vector<WfView> views = make_views(n, scenes, cameras, params, d_rgb.data(), d_alb.data(), d_nrm.data(), 0);
+        WfTuning wt = to_wf(tune);
+        wt.profile = (flags & FM_FLAG_PROFILE) != 0;
+        st = wavefront_views(ctx, views, wt, d_cnt, &tm);
+        ms = tm.total_ms;
+    } else {
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, ctx->stream);
+        for (int i = 0; i < n && st == FM_OK; ++i)
+            st = launch_megakernel(ctx, scenes[i], make_camera(cameras[i]), make_cfg(params[i]), d_rgb[i], d_alb[i],
+                                   d_nrm[i], d_cnt);
+        cudaEventRecord(e1, ctx->stream);
+        cudaEventSynchronize(e1);
+        float f = 0.0f;
+        cudaEventElapsedTime(&f, e0, e1);
+        ms = f;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    if (st == FM_OK && !dev) {
+        for (int i = 0; i < n; ++i) {
+            cudaMemcpyAsync(rgb[i], d_rgb[i], bytes[i], cudaMemcpyDeviceToHost, ctx->stream);
+            if (d_alb[i]) cudaMemcpyAsync(albedo[i], d_alb[i], bytes[i], cudaMemcpyDeviceToHost, ctx->stream);
+            if (d_nrm[i]) cudaMemcpyAsync(normal[i], d_nrm[i], bytes[i], cudaMemcpyDeviceToHost, ctx->stream);
+        }
+    }
+    Counters hc{};
+    uint32_t hs = 0;
+    cudaMemcpyAsync(&hc, d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream);
+    cudaMemcpyAsync(&hs, ctx->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream);
+    cudaFreeAsync(staging, ctx->stream);
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (st != FM_OK) return st;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "batch");
+    if (stats) {
+        stats->paths = (int64_t)hc.paths;
+        stats->closest_rays = (int64_t)hc.closest;
+        stats->shadow_rays = (int64_t)hc.shadow;
+        stats->bounces = (int64_t)hc.bounces;
+        stats->nan_samples = (int64_t)hc.nans;
+        stats->kernel_ms = ms;
+        stats->trace_ms = tm.trace_ms;
+        stats->shade_ms = tm.shade_ms;
+        stats->launches = wave ? tm.launches : (int64_t)n;
+    }
+    if (hs & 1u) return set_error(ctx, FM_ERR_QUEUE_OVERFLOW, "batch: traversal stack overflow");
+    if (hs & 2u) return set_error(ctx, FM_ERR_QUEUE_OVERFLOW, "batch: wavefront queue overflow");
+    return FM_OK;
+}

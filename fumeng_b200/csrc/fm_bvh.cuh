@@ -28,6 +28,16 @@ namespace fm {
 constexpr int kTraversalStack = 32;   // the builder rejects trees deeper than this
 constexpr uint32_t kSphereFlag = 0x80000000u;
 
+// The fields of a DevScene the traversal reads, kept in registers.
+struct TraceScene {
+    const uint4* nodes;
+    const float4* leaf;
+    const SphereDev* spheres;
+    int32_t num_nodes, num_tris;
+};
+
+FM_HD TraceScene trace_scene(const DevScene& S) { return TraceScene{S.nodes, S.leaf, S.spheres, S.num_nodes, S.num_tris}; }
+
 struct Hit {
     float t;
     int32_t prim;   // -1 on a miss
@@ -94,7 +104,7 @@ FM_D void intersect_node(const uint4* __restrict__ nodes, int node, f3 o, f3 idi
 // halves skip the second check (rectangle.cpp:42-56); spheres use the inclusive range
 // (sphere.cpp:116-127).
 template <bool ANY>
-FM_D bool test_prim(const DevScene& S, const RayPre& rp, f3 o, f3 d, int slot, float tmin, float& tbest,
+FM_D bool test_prim(const TraceScene& S, const RayPre& rp, f3 o, f3 d, int slot, float tmin, float& tbest,
                     Hit& hit)
 {
     const float4 a = __ldg(S.leaf + 3 * (size_t)slot);
@@ -132,7 +142,7 @@ FM_D bool test_prim(const DevScene& S, const RayPre& rp, f3 o, f3 d, int slot, f
 // *overflow is set when the traversal stack would overflow (the builder bounds the tree
 // depth so that this cannot happen for trees it accepted).
 template <bool ANY>
-FM_D bool trace_ray(const DevScene& S, f3 o, f3 d, float tmin, float tmax, Hit& hit, uint32_t* overflow)
+FM_D bool trace_ray(const TraceScene& S, f3 o, f3 d, float tmin, float tmax, Hit& hit, uint32_t* overflow)
 {
     hit.t = tmax;
     hit.prim = -1;
@@ -182,6 +192,13 @@ FM_D bool trace_ray(const DevScene& S, f3 o, f3 d, float tmin, float tmax, Hit& 
         }
     }
     return found;
+}
+
+template <bool ANY>
+FM_D bool trace_ray(const DevScene& S, f3 o, f3 d, float tmin, float tmax, Hit& hit, uint32_t* overflow)
+{
+    const TraceScene ts = trace_scene(S);
+    return trace_ray<ANY>(ts, o, d, tmin, tmax, hit, overflow);
 }
 
 }  // namespace fm

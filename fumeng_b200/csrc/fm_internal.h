@@ -1,6 +1,8 @@
 // Host-side definitions shared by the C-ABI translation units.
 #pragma once
+#include <map>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/fumeng_b200.h"
@@ -13,6 +15,8 @@ struct fm_ctx {
     std::string error;
     uint32_t* d_status = nullptr;   // device status word: bit 0 stack overflow, bit 1 queue overflow
     int num_sms = 148;
+    // autotuned wavefront settings per batch shape class (views, log2 samples, max lights)
+    std::map<std::tuple<int, int, int>, fm_tuning> tune_cache;
 };
 
 struct fm_scene {

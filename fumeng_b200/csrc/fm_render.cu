@@ -1,10 +1,228 @@
-// Rendering entry point (integrator kernels are added in this file).
+// Rendering: the plain per-pixel megakernel and the fm_render entry point.
+#include <array>
+#include <cmath>
+
 #include "fm_internal.h"
+#include "fm_path.cuh"
+#include "fm_render.h"
+
+namespace fm {
+
+namespace {
+
+FM_D void kahan_add(f3& sum, f3& c, f3 x)
+{
+    f3 y = x - c;
+    f3 t = sum + y;
+    c = (t - sum) - y;
+    sum = t;
+}
+
+FM_D void add_counters(Counters* cnt, unsigned long long paths, unsigned long long closest, unsigned long long shadow,
+                       unsigned long long bounces, unsigned long long nans)
+{
+    const unsigned mask = __activemask();
+    for (int off = 16; off > 0; off >>= 1) {
+        paths += __shfl_xor_sync(mask, paths, off);
+        closest += __shfl_xor_sync(mask, closest, off);
+        shadow += __shfl_xor_sync(mask, shadow, off);
+        bounces += __shfl_xor_sync(mask, bounces, off);
+        nans += __shfl_xor_sync(mask, nans, off);
+    }
+    if ((threadIdx.x & 31) == (__ffs(mask) - 1)) {
+        atomicAdd(&cnt->paths, paths);
+        atomicAdd(&cnt->closest, closest);
+        atomicAdd(&cnt->shadow, shadow);
+        atomicAdd(&cnt->bounces, bounces);
+        atomicAdd(&cnt->nans, nans);
+    }
+}
+
+// Plain megakernel: one thread owns one pixel and runs its samples one after another
+// (the reference's per-pixel task, renderer.h:97-116).
+__global__ void __launch_bounds__(128) k_megakernel(const __grid_constant__ DevScene S, DevCamera cam, RenderCfg cfg,
+                                                    float* rgb, float* alb, float* nrm, Counters* cnt,
+                                                    uint32_t* status)
+{
+    const int npix = cfg.width * cfg.height;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+        const int row = p / cfg.width, i = p % cfg.width;
+        const int j = cfg.height - 1 - row;
+        f3 sum = mk(0.0f), comp = mk(0.0f), asum = mk(0.0f), nsum = mk(0.0f);
+        unsigned long long nc = 0, ns = 0, nb = 0, nn = 0;
+        for (int k = 0; k < cfg.spp; ++k) {
+            Rng rng = rng_for(cfg.seed, (uint64_t)p, (uint64_t)(cfg.sample_offset + k));
+            const float fx = rng_1d(rng), fy = rng_1d(rng);
+            const float lx = rng_1d(rng), ly = rng_1d(rng);
+            const float px = ((float)i + fx) / (float)cfg.width;
+            const float py = ((float)j + fy) / (float)cfg.height;
+            f3 o, d;
+            camera_ray(cam, px, py, lx, ly, o, d);
+            const PathOut po = trace_path(S, cfg, o, d, rng, status);
+            if (!isfinite(po.color.x) || !isfinite(po.color.y) || !isfinite(po.color.z)) ++nn;
+            kahan_add(sum, comp, po.color);
+            asum += po.albedo;
+            nsum += po.normal;
+            nc += po.closest;
+            ns += po.shadow;
+            nb += po.bounces;
+        }
+        const float inv = 1.0f / (float)cfg.spp;
+        st3(rgb + 3 * (size_t)p, sum * inv);
+        if (alb) st3(alb + 3 * (size_t)p, asum * inv);
+        if (nrm) st3(nrm + 3 * (size_t)p, nsum * inv);
+        add_counters(cnt, (unsigned long long)cfg.spp, nc, ns, nb, nn);
+    }
+}
+
+}  // namespace
+
+DevCamera make_camera(const fm_camera& c)
+{
+    // camera_to_world = inverse(lookAt_LH(pos, look_at, normalize(up)))
+    // (pin_hole_camera.cpp:5-16): columns s, u, f and translation pos.
+    auto v = [](const float* a) { return std::array<double, 3>{a[0], a[1], a[2]}; };
+    auto sub = [](std::array<double, 3> a, std::array<double, 3> b) {
+        return std::array<double, 3>{a[0] - b[0], a[1] - b[1], a[2] - b[2]};
+    };
+    auto nrm = [](std::array<double, 3> a) {
+        const double l = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+        return std::array<double, 3>{a[0] / l, a[1] / l, a[2] / l};
+    };
+    auto crs = [](std::array<double, 3> a, std::array<double, 3> b) {
+        return std::array<double, 3>{a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+    };
+    const auto pos = v(c.pos), at = v(c.look_at), up = nrm(v(c.up));
+    const auto f = nrm(sub(at, pos));
+    const auto s = nrm(crs(up, f));
+    const auto u = crs(f, s);
+    DevCamera d;
+    d.pos = f3{c.pos[0], c.pos[1], c.pos[2]};
+    d.s = f3{(float)s[0], (float)s[1], (float)s[2]};
+    d.u = f3{(float)u[0], (float)u[1], (float)u[2]};
+    d.f = f3{(float)f[0], (float)f[1], (float)f[2]};
+    const float fov_rad = c.fov / 180.0f * kPi;
+    d.film_h = 2.0f * c.focal_distance * std::tan(fov_rad / 2.0f);
+    d.film_w = c.aspect * d.film_h;
+    d.focal = c.focal_distance;
+    d.lens_radius = c.lens_radius;
+    d.type = c.type;
+    return d;
+}
+
+RenderCfg make_cfg(const fm_render_params& p)
+{
+    RenderCfg r;
+    r.width = p.width;
+    r.height = p.height;
+    r.spp = p.spp;
+    r.depth = p.depth;
+    r.direct_loop = p.direct_loop;
+    r.rr_depth = p.rr_depth;
+    r.rr_coef = p.rr_coef;
+    r.seed = p.seed;
+    r.sample_offset = p.sample_offset;
+    r.rr_enabled = p.depth > p.rr_depth ? 1 : 0;
+    return r;
+}
+
+fm_status validate_render(fm_ctx* ctx, const fm_scene* scene, const fm_camera* camera, const fm_render_params* p)
+{
+    if (!scene || !camera || !p) return set_error(ctx, FM_ERR_INVALID, "render: null argument");
+    if (p->width <= 0 || p->height <= 0 || p->spp <= 0 || p->depth <= 0 || p->direct_loop <= 0)
+        return set_error(ctx, FM_ERR_INVALID, "render: width, height, spp, depth and direct_loop must be positive");
+    if ((int64_t)p->width * p->height > (int64_t)1 << 30) return set_error(ctx, FM_ERR_INVALID, "render: image too large");
+    if (camera->type != FM_CAMERA_PINHOLE && camera->type != FM_CAMERA_THIN_LENS)
+        return set_error(ctx, FM_ERR_INVALID, "render: bad camera type");
+    if (p->mode != FM_MODE_MEGAKERNEL && p->mode != FM_MODE_WAVEFRONT)
+        return set_error(ctx, FM_ERR_INVALID, "render: bad mode");
+    if (p->sample_offset < 0) return set_error(ctx, FM_ERR_INVALID, "render: negative sample_offset");
+    return FM_OK;
+}
+
+fm_status launch_megakernel(fm_ctx* ctx, const fm_scene* scene, const DevCamera& cam, const RenderCfg& cfg, float* rgb,
+                            float* alb, float* nrm, Counters* cnt)
+{
+    const int npix = cfg.width * cfg.height;
+    const int block = 128;
+    int grid = (npix + block - 1) / block;
+    k_megakernel<<<grid, block, 0, ctx->stream>>>(scene->dev, cam, cfg, rgb, alb, nrm, cnt, ctx->d_status);
+    FM_CUDA_TRY(ctx, cudaGetLastError(), "megakernel launch");
+    return FM_OK;
+}
+
+}  // namespace fm
+
+using namespace fm;
 
 extern "C" fm_status fm_render(fm_ctx* ctx, const fm_scene* scene, const fm_camera* camera,
                                const fm_render_params* params, float* rgb, float* albedo, float* normal,
                                int32_t flags, fm_render_stats* stats)
 {
-    (void)scene; (void)camera; (void)params; (void)rgb; (void)albedo; (void)normal; (void)flags; (void)stats;
-    return fm::set_error(ctx, FM_ERR_INVALID, "fm_render: integrator not built yet");
+    if (!ctx) return FM_ERR_INVALID;
+    fm_status st = validate_render(ctx, scene, camera, params);
+    if (st != FM_OK) return st;
+    if (!rgb) return set_error(ctx, FM_ERR_INVALID, "render: rgb output is null");
+    FM_CUDA_TRY(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+    const DevCamera cam = make_camera(*camera);
+    const RenderCfg cfg = make_cfg(*params);
+    const size_t npix = (size_t)cfg.width * cfg.height;
+    const size_t img_bytes = npix * 3 * sizeof(float);
+    const bool dev = (flags & FM_FLAG_DEVICE_PTRS) != 0;
+    char* tmp = nullptr;
+    float *d_rgb = rgb, *d_alb = albedo, *d_nrm = normal;
+    Counters* d_cnt = nullptr;
+    const size_t nimg = dev ? 0 : 1 + (albedo ? 1 : 0) + (normal ? 1 : 0);
+    FM_CUDA_TRY(ctx, cudaMallocAsync((void**)&tmp, nimg * img_bytes + 256, ctx->stream), "render alloc");
+    d_cnt = reinterpret_cast<Counters*>(tmp);
+    if (!dev) {
+        char* q = tmp + 256;
+        d_rgb = reinterpret_cast<float*>(q);
+        q += img_bytes;
+        d_alb = albedo ? reinterpret_cast<float*>(q) : nullptr;
+        q += albedo ? img_bytes : 0;
+        d_nrm = normal ? reinterpret_cast<float*>(q) : nullptr;
+    }
+    FM_CUDA_TRY(ctx, cudaMemsetAsync(d_cnt, 0, sizeof(Counters), ctx->stream), "render");
+    FM_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), ctx->stream), "render");
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, ctx->stream);
+    if (cfg.spp > 0 && params->mode == FM_MODE_WAVEFRONT)
+        st = launch_wavefront(ctx, scene, cam, cfg, d_rgb, d_alb, d_nrm, d_cnt);
+    else
+        st = launch_megakernel(ctx, scene, cam, cfg, d_rgb, d_alb, d_nrm, d_cnt);
+    cudaEventRecord(e1, ctx->stream);
+    if (st == FM_OK && !dev) {
+        cudaMemcpyAsync(rgb, d_rgb, img_bytes, cudaMemcpyDeviceToHost, ctx->stream);
+        if (albedo) cudaMemcpyAsync(albedo, d_alb, img_bytes, cudaMemcpyDeviceToHost, ctx->stream);
+        if (normal) cudaMemcpyAsync(normal, d_nrm, img_bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    }
+    Counters hc{};
+    uint32_t hs = 0;
+    cudaMemcpyAsync(&hc, d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream);
+    cudaMemcpyAsync(&hs, ctx->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream);
+    cudaFreeAsync(tmp, ctx->stream);
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != FM_OK) return st;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "render");
+    if (stats) {
+        stats->paths = (int64_t)hc.paths;
+        stats->closest_rays = (int64_t)hc.closest;
+        stats->shadow_rays = (int64_t)hc.shadow;
+        stats->bounces = (int64_t)hc.bounces;
+        stats->nan_samples = (int64_t)hc.nans;
+        stats->kernel_ms = ms;
+        stats->trace_ms = 0.0;
+        stats->shade_ms = 0.0;
+        stats->launches = params->mode == FM_MODE_WAVEFRONT ? -1 : 1;
+    }
+    if (hs & 1u) return set_error(ctx, FM_ERR_QUEUE_OVERFLOW, "render: traversal stack overflow");
+    if (hs & 2u) return set_error(ctx, FM_ERR_QUEUE_OVERFLOW, "render: wavefront queue overflow");
+    return FM_OK;
 }

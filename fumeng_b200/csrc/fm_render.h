@@ -1,0 +1,48 @@
+// Rendering internals shared by fm_render.cu, fm_wavefront.cu and fm_batch.cu.
+#pragma once
+#include "fm_integrator.cuh"
+#include "fm_internal.h"
+
+namespace fm {
+
+DevCamera make_camera(const fm_camera& c);
+RenderCfg make_cfg(const fm_render_params& p);
+fm_status validate_render(fm_ctx* ctx, const fm_scene* scene, const fm_camera* camera, const fm_render_params* p);
+
+// Device-side description of one view in a wavefront launch.
+struct WfView {
+    const DevScene* scene;   // device pointer
+    DevCamera cam;
+    RenderCfg cfg;
+    int64_t item_base;       // first work item of this view
+    int32_t chunk;           // samples per work item
+    int32_t nchunks;         // work items per pixel
+    float4* partial;         // [nchunks * npix * 3] (color Kahan sum, albedo sum, normal sum)
+    float* rgb;              // outputs (device)
+    float* alb;
+    float* nrm;
+};
+
+// Wavefront tuning knobs (pool size, block sizes, graph depth).
+struct WfTuning {
+    int64_t pool = 1 << 21;   // path slots
+    int trace_block = 128;
+    int shade_block = 128;
+    int iters_per_graph = 8;
+    bool profile = false;     // record CUDA events around each trace / shade launch
+};
+
+struct WfTimes {
+    double total_ms = 0.0, trace_ms = 0.0, shade_ms = 0.0;
+    int64_t launches = 0;
+};
+
+fm_status launch_wavefront(fm_ctx* ctx, const fm_scene* scene, const DevCamera& cam, const RenderCfg& cfg, float* rgb,
+                           float* alb, float* nrm, Counters* cnt);
+fm_status launch_megakernel(fm_ctx* ctx, const fm_scene* scene, const DevCamera& cam, const RenderCfg& cfg, float* rgb,
+                            float* alb, float* nrm, Counters* cnt);
+// Renders several views (possibly of different scenes) in one wavefront.
+fm_status wavefront_views(fm_ctx* ctx, const std::vector<WfView>& views, const WfTuning& tune, Counters* cnt,
+                          WfTimes* times);
+
+}  // namespace fm

@@ -230,3 +230,98 @@ def hit_scene(seed: int, level: int = 4, boxes: int = 3) -> SceneSpec:
     ren = {"width": 64, "height": 64, "spp": 1, "depth": 4}
     mats = [{"name": "m0", "type": "lambert_diffuse", "basecolor": [0.5, 0.5, 0.5]}]
     return SceneSpec(cam, ren, mats, objs)
+
+
+def material_scene(seed: int, res: int = 64, env_w: int = 128, env_h: int = 64, spp: int = 16, depth: int = 6) -> SceneSpec:
+    """Small scene exercising every BSDF and light kind: Disney icosphere (specTrans 0),
+    Disney clearcoat sphere, dielectric sphere, conductor sphere, Lambert floor, a
+    rectangle area light, a directional light and an HDR environment (z-up)."""
+    rng = np.random.default_rng(seed)
+    v, f = displaced_icosphere(3, seed)
+    objs = [Mesh((v * 0.45 + np.array([-0.5, 0.0, 0.45])).astype(np.float32), f, "disney_a"),
+            Sphere(0.3, translation=(0.45, -0.35, 0.3), material="glass"),
+            Sphere(0.25, translation=(0.55, 0.45, 0.25), material="coat"),
+            Sphere(0.2, translation=(-0.1, -0.75, 0.2), material="metal"),
+            Rect((-2, -2, 0), (2, -2, 0), (2, 2, 0), (-2, 2, 0), "floor"),
+            Rect((-0.4, -0.4, 1.8), (-0.4, 0.4, 1.8), (0.4, 0.4, 1.8), (0.4, -0.4, 1.8), "floor", emittance=(6.0, 6.0, 5.0))]
+    mats = [
+        {"name": "disney_a", "type": "disney", "basecolor": [0.8, 0.3, 0.2], "metallic": 0.0, "roughness": 0.4,
+         "specular": 0.5, "clearcoat": 0.3, "clearcoatGloss": 0.7, "sheen": 0.2, "anisotropic": 0.3},
+        {"name": "coat", "type": "disney", "basecolor": [0.2, 0.5, 0.8], "metallic": 1.0, "roughness": 0.25,
+         "clearcoat": 1.0, "clearcoatGloss": 0.9},
+        {"name": "glass", "type": "specular_transmission", "reflect_color": [1, 1, 1], "refract_color": [1, 1, 1],
+         "eta_i": 1.0, "eta_t": float(rng.uniform(1.3, 1.7))},
+        {"name": "metal", "type": "specular_reflection", "color": [0.95, 0.9, 0.8], "eta_i": [1, 1, 1],
+         "eta_t": [0.2, 0.92, 1.1], "k": [3.9, 2.45, 2.14]},
+        {"name": "floor", "type": "lambert_diffuse", "basecolor": [0.6, 0.6, 0.55]},
+    ]
+    env = sky_env(env_w, env_h, seed + 1, sun_peak=200.0, sun_sigma_deg=4.0)
+    cam = {"type": "pin_hole", "pos": [0.0, -3.2, 1.4], "look_at": [0.0, 0.0, 0.35], "up": [0, 0, 1], "fov": 45.0,
+           "aspect": 1.0}
+    ren = {"width": res, "height": res, "spp": spp, "depth": depth, "rr_depth": 3, "rr_coef": 0.85}
+    lights = [{"type": "env", "texture": "sky", "rotation": [0, 0, 30], "factor": 1.0},
+              {"type": "directional", "radiance": [1.5, 1.4, 1.2], "direction": [0.3, 0.5, -0.8]}]
+    return SceneSpec(cam, ren, mats, objs, lights, {"sky": env})
+
+
+def _random_disney(rng):
+    return {"type": "disney", "basecolor": list(rng.uniform(0.1, 0.9, 3)), "roughness": float(rng.uniform(0.05, 1.0)),
+            "metallic": float(rng.random() < 0.3), "specular": 0.5, "clearcoat": float(rng.uniform(0, 1)),
+            "clearcoatGloss": float(rng.uniform(0, 1)), "specTrans": 0.0}
+
+
+def batch_scene(s: int, env_w: int = 512, env_h: int = 256, res: int | None = None, spp: int | None = None,
+                depth: int = 8) -> SceneSpec:
+    """Scene `s` of the batched workload (seed 100 + s): 1-40 meshes (displaced
+    icospheres or subdivided boxes) totalling a log-uniform 1k-200k triangles, materials
+    drawn from {Disney (specTrans 0), Lambert, dielectric IOR U[1.3, 1.7]}, a ground
+    plane, one rectangle area light and a 512x256 sky; resolution in {128, 256, 384, 512}^2,
+    spp in {4, 16, 64}, depth 8."""
+    rng = np.random.default_rng(100 + s)
+    k = int(rng.integers(1, 41))
+    total = float(np.exp(rng.uniform(np.log(1e3), np.log(2e5))))
+    w = rng.dirichlet(np.ones(k))
+    objs, mats = [], []
+    for m in range(k):
+        budget = max(20.0, total * w[m])
+        name = f"m{m}"
+        kind = rng.random()
+        if kind < 0.45:
+            mats.append({"name": name, **_random_disney(rng)})
+        elif kind < 0.8:
+            mats.append({"name": name, "type": "lambert_diffuse", "basecolor": list(rng.uniform(0.1, 0.9, 3))})
+        else:
+            mats.append({"name": name, "type": "specular_transmission", "reflect_color": [1, 1, 1],
+                         "refract_color": list(rng.uniform(0.7, 1.0, 3)), "eta_i": 1.0,
+                         "eta_t": float(rng.uniform(1.3, 1.7))})
+        r = float(rng.uniform(0.12, 0.45))
+        c = np.array([rng.uniform(-1.6, 1.6), rng.uniform(-1.6, 1.6), 0.0])
+        if rng.random() < 0.6:
+            level = int(np.clip(np.round(np.log(budget / 20.0) / np.log(4.0)), 0, 7))
+            v, f = displaced_icosphere(level, 1000 * s + m)
+            c[2] = r
+        else:
+            n = max(1, int(round(np.sqrt(budget / 12.0))))
+            v, f = subdivided_box(n)
+            v = v * np.array([1.0, rng.uniform(0.5, 1.5), rng.uniform(0.5, 1.5)])
+            c[2] = r * abs(v[:, 2]).max()
+        objs.append(Mesh((v * r + c).astype(np.float32), f, name))
+    mats.append({"name": "ground", "type": "lambert_diffuse", "basecolor": [0.5, 0.5, 0.5]})
+    objs.append(Rect((-4, -4, 0), (4, -4, 0), (4, 4, 0), (-4, 4, 0), "ground"))
+    objs.append(Rect((-0.6, -0.6, 3.5), (-0.6, 0.6, 3.5), (0.6, 0.6, 3.5), (0.6, -0.6, 3.5), "ground",
+                     emittance=(10.0, 10.0, 9.0)))
+    if res is None:
+        res = int(rng.choice([128, 256, 384, 512]))
+    if spp is None:
+        spp = int(rng.choice([4, 16, 64]))
+    az = rng.uniform(0, 2 * np.pi)
+    cam = {"type": "pin_hole", "pos": [4.5 * np.cos(az), 4.5 * np.sin(az), 2.2], "look_at": [0.0, 0.0, 0.4],
+           "up": [0, 0, 1], "fov": 45.0, "aspect": 1.0}
+    ren = {"width": res, "height": res, "spp": spp, "depth": depth, "rr_depth": 3, "rr_coef": 0.85}
+    env = sky_env(env_w, env_h, 100 + s, sun_peak=5e4, sun_sigma_deg=0.5)
+    lights = [{"type": "env", "texture": "sky", "rotation": [0, 0, float(rng.uniform(0, 360))], "factor": 1.0}]
+    return SceneSpec(cam, ren, mats, objs, lights, {"sky": env})
+
+
+def batch_scenes(n: int = 64, **kw) -> list:
+    return [batch_scene(s, **kw) for s in range(n)]

@@ -41,7 +41,10 @@ typedef enum {
 typedef struct fm_ctx fm_ctx;
 typedef struct fm_scene fm_scene;
 
-enum { FM_FLAG_DEVICE_PTRS = 1 };
+enum {
+    FM_FLAG_DEVICE_PTRS = 1, /* buffers are device pointers */
+    FM_FLAG_PROFILE = 2      /* time the wavefront's trace and shade kernels (CUDA events) */
+};
 
 /* ---- textures ------------------------------------------------------------------ */
 enum { FM_WRAP_REPEAT = 0, FM_WRAP_CLAMP = 1 };
@@ -175,6 +178,9 @@ typedef struct {
     int64_t bounces;          /* shading events */
     int64_t nan_samples;      /* samples whose radiance was not finite */
     double kernel_ms;         /* device time of the render kernels */
+    double trace_ms;          /* wavefront trace kernels (with FM_FLAG_PROFILE), else 0 */
+    double shade_ms;          /* wavefront shade kernels (with FM_FLAG_PROFILE), else 0 */
+    int64_t launches;         /* kernels launched (graph nodes included) */
 } fm_render_stats;
 
 /* ---- entry points ---------------------------------------------------------------- */
@@ -213,6 +219,31 @@ fm_status fm_trace_any(fm_ctx* ctx, const fm_scene* scene, const float* rays, in
 fm_status fm_render(fm_ctx* ctx, const fm_scene* scene, const fm_camera* camera,
                     const fm_render_params* params, float* rgb, float* albedo, float* normal,
                     int32_t flags, fm_render_stats* stats);
+
+/* Wavefront tuning: path-slot pool size (queue capacities scale with it), block sizes of
+ * the trace and shade kernels, and iterations per captured CUDA graph. */
+typedef struct {
+    int64_t pool;
+    int32_t trace_block, shade_block, iters_per_graph;
+} fm_tuning;
+
+/* Replaces: running the reference once per scene (main.cpp:5-11, one SceneLoader and one
+ * Renderer::DrawFrame per process).  Renders n views -- view i is scenes[i] seen by
+ * cameras[i] with params[i] -- in one persistent wavefront whose kernel sequence is
+ * captured as a CUDA graph.  rgb[i] / albedo[i] / normal[i] receive view i's images
+ * (albedo and normal arrays, or their entries, may be NULL).  All params must use
+ * FM_MODE_WAVEFRONT, or all FM_MODE_MEGAKERNEL (then the views are rendered one after
+ * another by the plain megakernel, the baseline).  tuning == NULL selects the tuning
+ * cached for this batch's shape class, running the autotuner on first use. */
+fm_status fm_render_batch(fm_ctx* ctx, int32_t n, const fm_scene* const* scenes, const fm_camera* cameras,
+                          const fm_render_params* params, float* const* rgb, float* const* albedo,
+                          float* const* normal, int32_t flags, const fm_tuning* tuning, fm_render_stats* stats);
+
+/* Replaces: nothing in the reference (its thread pool has no knobs beyond thread_count).
+ * Times candidate tunings on a reduced copy of the batch (spp 1) and returns the fastest;
+ * the result is cached in the context for the batch's shape class. */
+fm_status fm_autotune_batch(fm_ctx* ctx, int32_t n, const fm_scene* const* scenes, const fm_camera* cameras,
+                            const fm_render_params* params, fm_tuning* out);
 
 #ifdef __cplusplus
 }

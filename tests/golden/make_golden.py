@@ -66,10 +66,38 @@ def make_hit(case):
     print(case[0], "hits", int((obj >= 0).sum()), "occluded", int(occ.sum()))
 
 
+# name, builder, oracle spp, seed; images are stored at every `stride`-th pixel
+IMAGE_CASES = [
+    ("img_cornell", lambda: synth.cornell(), 4096, 7, 2),
+    ("img_materials", lambda: synth.material_scene(3), 4096, 8, 1),
+]
+
+
+def make_image(case):
+    name, builder, spp, seed, stride = case
+    spec = builder()
+    with tempfile.TemporaryDirectory() as d:
+        rs = fmref.RefScene(spec.write(Path(d)), "double")
+        t0 = time.time()
+        r = rs.render(spp, seed=seed, aov=True)
+        dt = time.time() - t0
+        rs.close()
+    mean = r["sum"] / spp
+    var = np.maximum(r["sumsq"] / spp - mean * mean, 0.0) * spp / (spp - 1)
+    sl = (slice(None, None, stride), slice(None, None, stride))
+    np.savez_compressed(GOLDEN / f"{name}.npz", mean=mean[sl].astype(np.float32), var=var[sl].astype(np.float32),
+                        albedo=(r["albedo"] / spp)[sl].astype(np.float32), normal=(r["normal"] / spp)[sl].astype(np.float32),
+                        spp=spp, stride=stride)
+    print(name, "spp", spp, "%.1fs" % dt, "mean", mean.mean(axis=(0, 1)))
+
+
 if __name__ == "__main__":
     what = set(sys.argv[1:]) or {"hit"}
     t0 = time.time()
     if "hit" in what:
         for c in HIT_CASES:
             make_hit(c)
+    if "images" in what:
+        for c in IMAGE_CASES:
+            make_image(c)
     print("done in %.1fs" % (time.time() - t0))

@@ -1,0 +1,102 @@
+"""Converged images of the CUDA renderers against the reference's double build.
+
+For each golden scene the GPU renders 16 independent batches of 256 samples (4096 spp;
+batch b uses sample indices [256 b, 256 b + 256)), which gives per-pixel means and the
+variance of those means.  The golden fixture holds the reference's per-pixel mean and
+single-sample variance at 4096 spp (tests/golden/make_golden.py).  Checks:
+  * per-pixel 3-sigma agreement: |mu_gpu - mu_ref| <= 3 sqrt(var_gpu/N + var_ref/N);
+    about 0.27% of pixel channels fail under pure noise, the bound is 1%;
+  * relMSE = mean((mu_gpu - mu_ref)^2 / (mu_ref^2 + 1e-2)); with both estimators at 4096
+    spp it contains their noise, so the test bounds relMSE minus its expected noise part
+    (the squared bias) by 1e-3 and reports both;
+  * albedo and normal AOVs (first-hit averages) agree to 2e-2 mean absolute difference.
+"""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import fumeng_b200 as fb
+from golden.make_golden import IMAGE_CASES
+
+GOLDEN_DIR = Path(__file__).resolve().parent / "golden"
+BATCHES, BATCH_SPP = 16, 256
+RESULTS = Path(__file__).resolve().parents[1] / "gpurun_out"
+
+
+def render_batches(ctx, spec, mode, seed=1234, batches=BATCHES, spp=BATCH_SPP):
+    scene = ctx.create_scene(spec.to_desc())
+    try:
+        cam = spec.camera_struct()
+        rgb, alb, nrm = [], [], []
+        for b in range(batches):
+            p = spec.render_params(spp=spp, seed=seed, mode=mode, sample_offset=b * spp)
+            c, a, n, st = scene.render(cam, p)
+            assert st.paths == p.width * p.height * spp
+            rgb.append(c)
+            alb.append(a)
+            nrm.append(n)
+    finally:
+        scene.destroy()
+    return np.stack(rgb).astype(np.float64), np.mean(alb, 0), np.mean(nrm, 0)
+
+
+def compare(rgb_batches, g):
+    K = rgb_batches.shape[0]
+    s = int(g["stride"])
+    mu = rgb_batches.mean(0)[::s, ::s]
+    var_mu = rgb_batches.var(0, ddof=1)[::s, ::s] / K
+    r = g["mean"].astype(np.float64)
+    var_r = g["var"].astype(np.float64) / float(g["spp"])
+    den = r * r + 1e-2
+    relmse = float(np.mean((mu - r) ** 2 / den))
+    noise = float(np.mean((var_mu + var_r) / den))
+    z = np.abs(mu - r) / np.sqrt(var_mu + var_r + 1e-12)
+    return {"relmse": relmse, "relmse_noise": noise, "relmse_bias": relmse - noise,
+            "frac_3sigma": float(np.mean(z > 3.0)), "pixels": int(np.prod(r.shape[:2]))}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", [fb.FM_MODE_MEGAKERNEL, fb.FM_MODE_WAVEFRONT], ids=["megakernel", "wavefront"])
+@pytest.mark.parametrize("case", IMAGE_CASES, ids=[c[0] for c in IMAGE_CASES])
+def test_converged_image_matches_reference(ctx, case, mode):
+    name = case[0]
+    g = np.load(GOLDEN_DIR / f"{name}.npz")
+    spec = case[1]()
+    rgb, alb, nrm = render_batches(ctx, spec, mode)
+    res = compare(rgb, g)
+    s = int(g["stride"])
+    res["albedo_mad"] = float(np.mean(np.abs(alb[::s, ::s] - g["albedo"])))
+    res["normal_mad"] = float(np.mean(np.abs(nrm[::s, ::s] - g["normal"])))
+    res.update(case=name, mode="megakernel" if mode == fb.FM_MODE_MEGAKERNEL else "wavefront")
+    print(json.dumps(res))
+    if RESULTS.is_dir():
+        with open(RESULTS / "image_parity.jsonl", "a") as f:
+            f.write(json.dumps(res) + "\n")
+    assert np.all(np.isfinite(rgb))
+    assert res["frac_3sigma"] < 0.01, res
+    assert res["relmse_bias"] < 1e-3, res
+    assert res["albedo_mad"] < 2e-2 and res["normal_mad"] < 2e-2, res
+
+
+@pytest.mark.gpu
+def test_megakernel_is_deterministic(ctx):
+    from fumeng_b200 import synth
+    spec = synth.material_scene(3, res=32)
+    a = render_batches(ctx, spec, fb.FM_MODE_MEGAKERNEL, batches=1, spp=8)[0]
+    b = render_batches(ctx, spec, fb.FM_MODE_MEGAKERNEL, batches=1, spp=8)[0]
+    assert np.array_equal(a, b, equal_nan=True)
+
+
+@pytest.mark.gpu
+def test_wavefront_matches_megakernel_on_same_random_streams(ctx):
+    # Both renderers draw the same random numbers in the same order for every sample, so
+    # their images agree up to float summation order (and the rare path that a rounding
+    # difference sends another way).
+    from fumeng_b200 import synth
+    spec = synth.material_scene(3, res=48)
+    a = render_batches(ctx, spec, fb.FM_MODE_MEGAKERNEL, batches=1, spp=64)[0][0]
+    b = render_batches(ctx, spec, fb.FM_MODE_WAVEFRONT, batches=1, spp=64)[0][0]
+    rel = np.abs(a - b) / (np.abs(a) + 1e-3)
+    assert np.mean(rel < 1e-3) > 0.97, float(np.mean(rel < 1e-3))
