@@ -118,8 +118,8 @@ def desc_bytes(holder) -> int:
     return n
 
 
-def scene_indices(rank: int):
-    return [rank * NSCENES + s for s in range(NSCENES)]
+def scene_indices(rank: int, n: int = NSCENES):
+    return [rank * NSCENES + s for s in range(n)]
 
 
 # ---- reference arm (CPU) ---------------------------------------------------------------
@@ -172,6 +172,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--mk-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scenes", type=int, default=NSCENES, help="batch size (profiling runs use fewer)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -225,7 +226,7 @@ def main():
         return float(t.item())
 
     ctx = fb.Context(local_rank)
-    specs = [synth.batch_scene(s) for s in scene_indices(rank)]
+    specs = [synth.batch_scene(s) for s in scene_indices(rank, args.scenes)]
     holders = [s.to_desc() for s in specs]
     cams = [s.camera_struct() for s in specs]
     params_wf = [s.render_params(seed=1, mode=fb.FM_MODE_WAVEFRONT) for s in specs]
@@ -338,7 +339,7 @@ def main():
             "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "scenes": NSCENES, "triangles": int(tris),
+            "config": {"workload": WORKLOAD, "scenes": len(specs), "triangles": int(tris),
                        "paths_per_step": int(paths_per_step), "depth": 8,
                        "parallelism": f"replicas x{world} (each rank renders its own 64-scene batch)",
                        "l2": "inputs larger than L2 (scene data + path state exceed 126 MB)",

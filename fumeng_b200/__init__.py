@@ -131,6 +131,8 @@ def load_library() -> C.CDLL:
                              C.POINTER(RenderStats)], C.c_int),
         "fm_autotune_batch": ([vp, C.c_int32, C.POINTER(vp), C.POINTER(Camera), C.POINTER(RenderParams),
                                C.POINTER(Tuning)], C.c_int),
+        "fm_scene_load": ([vp, C.c_char_p, C.POINTER(vp), C.POINTER(Camera), C.POINTER(RenderParams)], C.c_int),
+        "fm_draw_frame": ([vp, C.c_char_p], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -142,7 +144,7 @@ def load_library() -> C.CDLL:
 
 EXPORTED_SYMBOLS = ["fm_ctx_create", "fm_ctx_destroy", "fm_last_error", "fm_scene_create", "fm_scene_destroy",
                     "fm_scene_bvh_stats", "fm_trace_closest", "fm_trace_any", "fm_render", "fm_render_batch",
-                    "fm_autotune_batch"]
+                    "fm_autotune_batch", "fm_scene_load", "fm_draw_frame"]
 
 
 def _ptr(a, ctype=C.c_void_p):
@@ -220,6 +222,18 @@ class Context:
         self.check(self.lib.fm_autotune_batch(self.h, n, sc, ca, pa, C.byref(t)))
         return t
 
+    def load_scene(self, json_path):
+        """SceneLoader::Load through the C++ loader: returns (Scene, Camera, RenderParams)."""
+        h = C.c_void_p()
+        cam = Camera()
+        params = RenderParams()
+        self.check(self.lib.fm_scene_load(self.h, str(json_path).encode(), C.byref(h), C.byref(cam), C.byref(params)))
+        return Scene(self, h, None), cam, params
+
+    def draw_frame(self, json_path) -> None:
+        """SceneLoader::DrawFrame: render the scene file and write its PNG outputs."""
+        self.check(self.lib.fm_draw_frame(self.h, str(json_path).encode()))
+
     def create_scene(self, desc_holder) -> "Scene":
         h = C.c_void_p()
         self.check(self.lib.fm_scene_create(self.h, C.byref(desc_holder.desc), C.byref(h)))
@@ -266,3 +280,12 @@ class Scene:
         self.ctx.check(self.ctx.lib.fm_render(self.ctx.h, self.h, C.byref(camera), C.byref(params), _ptr(rgb),
                                               _ptr(alb), _ptr(nrm), 0, C.byref(stats)))
         return rgb, alb, nrm, stats
+
+
+def parse_scene_file(json_path):
+    """Parse-only SceneLoader::Load (no device): returns (status, Camera, RenderParams)."""
+    lib = load_library()
+    cam = Camera()
+    params = RenderParams()
+    st = lib.fm_scene_load(None, str(json_path).encode(), None, C.byref(cam), C.byref(params))
+    return st, cam, params

@@ -216,6 +216,12 @@ void fm_ctx_destroy(fm_ctx* ctx)
 
 const char* fm_last_error(const fm_ctx* ctx) { return ctx ? ctx->error.c_str() : "null context"; }
 
+// Used by the host-side scene loader (compiled by the C++ compiler) to report errors.
+void fm_internal_set_error(fm_ctx* ctx, const char* msg)
+{
+    if (ctx) ctx->error = msg ? msg : "";
+}
+
 fm_status fm_scene_create(fm_ctx* ctx, const fm_scene_desc* d, fm_scene** out)
 {
     if (!ctx) return FM_ERR_INVALID;

@@ -18,18 +18,18 @@ FM_D void kahan_add(f3& sum, f3& c, f3 x)
     sum = t;
 }
 
+// Called once per thread after its loop, by all 32 lanes of the warp.
 FM_D void add_counters(Counters* cnt, unsigned long long paths, unsigned long long closest, unsigned long long shadow,
                        unsigned long long bounces, unsigned long long nans)
 {
-    const unsigned mask = __activemask();
     for (int off = 16; off > 0; off >>= 1) {
-        paths += __shfl_xor_sync(mask, paths, off);
-        closest += __shfl_xor_sync(mask, closest, off);
-        shadow += __shfl_xor_sync(mask, shadow, off);
-        bounces += __shfl_xor_sync(mask, bounces, off);
-        nans += __shfl_xor_sync(mask, nans, off);
+        paths += __shfl_xor_sync(0xffffffffu, paths, off);
+        closest += __shfl_xor_sync(0xffffffffu, closest, off);
+        shadow += __shfl_xor_sync(0xffffffffu, shadow, off);
+        bounces += __shfl_xor_sync(0xffffffffu, bounces, off);
+        nans += __shfl_xor_sync(0xffffffffu, nans, off);
     }
-    if ((threadIdx.x & 31) == (__ffs(mask) - 1)) {
+    if ((threadIdx.x & 31) == 0) {
         atomicAdd(&cnt->paths, paths);
         atomicAdd(&cnt->closest, closest);
         atomicAdd(&cnt->shadow, shadow);
@@ -45,11 +45,11 @@ __global__ void __launch_bounds__(128) k_megakernel(const __grid_constant__ DevS
                                                     uint32_t* status)
 {
     const int npix = cfg.width * cfg.height;
+    unsigned long long np = 0, nc = 0, ns = 0, nb = 0, nn = 0;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
         const int row = p / cfg.width, i = p % cfg.width;
         const int j = cfg.height - 1 - row;
         f3 sum = mk(0.0f), comp = mk(0.0f), asum = mk(0.0f), nsum = mk(0.0f);
-        unsigned long long nc = 0, ns = 0, nb = 0, nn = 0;
         for (int k = 0; k < cfg.spp; ++k) {
             Rng rng = rng_for(cfg.seed, (uint64_t)p, (uint64_t)(cfg.sample_offset + k));
             const float fx = rng_1d(rng), fy = rng_1d(rng);
@@ -71,8 +71,9 @@ __global__ void __launch_bounds__(128) k_megakernel(const __grid_constant__ DevS
         st3(rgb + 3 * (size_t)p, sum * inv);
         if (alb) st3(alb + 3 * (size_t)p, asum * inv);
         if (nrm) st3(nrm + 3 * (size_t)p, nsum * inv);
-        add_counters(cnt, (unsigned long long)cfg.spp, nc, ns, nb, nn);
+        np += (unsigned long long)cfg.spp;
     }
+    add_counters(cnt, np, nc, ns, nb, nn);
 }
 
 }  // namespace

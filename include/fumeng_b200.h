@@ -245,6 +245,21 @@ fm_status fm_render_batch(fm_ctx* ctx, int32_t n, const fm_scene* const* scenes,
 fm_status fm_autotune_batch(fm_ctx* ctx, int32_t n, const fm_scene* const* scenes, const fm_camera* cameras,
                             const fm_render_params* params, fm_tuning* out);
 
+/* Replaces: SceneLoader::Load (create/scene_loader.h:293-302).  Reads a scene file in
+ * the reference's JSON schema (plus the extensions documented in
+ * fumeng_b200/host/fm_scene_loader.h), loads its OBJ meshes and .hdr / PNG textures,
+ * creates the device scene and returns the camera and renderer settings it names.
+ * With out == NULL the file is only parsed and checked (no device is needed and ctx
+ * may be NULL). */
+fm_status fm_scene_load(fm_ctx* ctx, const char* json_path, fm_scene** out, fm_camera* camera,
+                        fm_render_params* params);
+
+/* Replaces: SceneLoader::DrawFrame -> Renderer::DrawFrame (scene_loader.h:304-307,
+ * core/renderer.h:84-144), as called by the command line (src/cmd/src/main.cpp:5-11):
+ * renders the scene file, applies its post-process chain and writes <output>.png,
+ * <output>_albedo.png and <output>_normal.png. */
+fm_status fm_draw_frame(fm_ctx* ctx, const char* json_path);
+
 #ifdef __cplusplus
 }
 #endif
