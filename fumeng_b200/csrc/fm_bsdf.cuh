@@ -338,7 +338,11 @@ FM_D f3 ds_spec_eval(const Disney& d, f3 wo, f3 wi)
     const f3 f = lerp3(d.specular * f_diel, f_cond, d.metallic);
     const float D = gtr2_aniso(wh, d.ax, d.ay);
     const float G = smith_ggx_aniso(wo, wi, d.ax, d.ay);
-    return f * D * G / fabsf(4.0f * cos_i * cos_o);
+    // Exactly grazing directions give 0/0 here; the value is set to zero (a set of
+    // measure zero) so that float does not emit NaN where the double build does not.
+    const float den = fabsf(4.0f * cos_i * cos_o);
+    if (den == 0.0f) return mk(0.0f);
+    return f * D * G / den;
 }
 
 FM_D f3 ds_spec_sample(const Disney& d, f3 wo, float u0, float u1)
@@ -398,7 +402,9 @@ FM_D f3 ds_cc_eval(const Disney& d, f3 wo, f3 wi)
     const float f = 0.04f + (1.0f - 0.04f) * p5(clampf(1.0f - cos_d, 0.0f, 1.0f));
     const float D = gtr1(wh, d.cc_rough);
     const float G = smith_ggx_sep(wi, 0.25f) * smith_ggx_sep(wo, 0.25f);
-    return mk(d.clearcoat * f * D * G / fabsf(4.0f * cos_i * cos_o));
+    const float den = fabsf(4.0f * cos_i * cos_o);
+    if (den == 0.0f) return mk(0.0f);
+    return mk(d.clearcoat * f * D * G / den);
 }
 
 FM_D f3 ds_cc_sample(const Disney& d, f3 wo, float u0, float u1)
@@ -432,7 +438,9 @@ FM_D f3 ds_trans_eval(const Disney& d, f3 wo, f3 wi, float ax, float ay, f3 c)
     const float D = gtr2_aniso(wh, ax, ay);
     const float G = smith_ggx_aniso(wo, wi, ax, ay);
     const float den = eta * cdi + cdo;
-    const float ft = (1.0f - f) * D * G * cdo * cdi / (cos_i * cos_o * den * den);
+    const float q = cos_i * cos_o * den * den;
+    if (q == 0.0f) return mk(0.0f);
+    const float ft = (1.0f - f) * D * G * cdo * cdi / q;
     return d.spec_trans * (1.0f - d.metallic) * c * fabsf(ft);
 }
 
@@ -580,9 +588,18 @@ FM_D BsdfSample bsdf_sample(const Bsdf& b, f3 wo_w, f3 u)
         s.delta = false;
         return s;
     }
+    // Delta samples at an exactly grazing angle (cos = 0) give 0/0 or x/0; they are
+    // returned as failed samples (a set of measure zero) instead of NaN.
     if (b.type == 1) {
         const f3 wi = f3{-wo.x, -wo.y, wo.z};
         const float ci = cos_dir(wi);
+        if (ci == 0.0f) {
+            s.f = mk(0.0f);
+            s.wi = mk(0.0f);
+            s.pdf = 0.0f;
+            s.delta = true;
+            return s;
+        }
         const f3 fr = f3{fresnel_conductor1(ci, b.eta2.x, b.etak2.x), fresnel_conductor1(ci, b.eta2.y, b.etak2.y),
                          fresnel_conductor1(ci, b.eta2.z, b.etak2.z)};
         s.f = fr * b.color / fabsf(ci);
@@ -594,6 +611,12 @@ FM_D BsdfSample bsdf_sample(const Bsdf& b, f3 wo_w, f3 u)
     if (b.type == 2) {
         const float fr = fresnel_dielectric(cos_dir(wo), b.eta_i, b.eta_t);
         s.delta = true;
+        if (cos_dir(wo) == 0.0f) {
+            s.f = mk(0.0f);
+            s.wi = mk(0.0f);
+            s.pdf = 0.0f;
+            return s;
+        }
         if (u.x < fr) {
             const f3 wi = f3{-wo.x, -wo.y, wo.z};
             const float ci = cos_dir(wi);
@@ -620,6 +643,12 @@ FM_D BsdfSample bsdf_sample(const Bsdf& b, f3 wo_w, f3 u)
         }
         s.pdf = 1.0f - fr;
         const float ct = cos_dir(wt);
+        if (ct == 0.0f) {
+            s.f = mk(0.0f);
+            s.wi = mk(0.0f);
+            s.pdf = 0.0f;
+            return s;
+        }
         s.f = eta * eta * b.color2 * (1.0f - fr) / fabsf(ct);
         s.wi = to_world(b, wt);
         return s;

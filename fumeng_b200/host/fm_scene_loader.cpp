@@ -184,6 +184,7 @@ ObjData load_obj(const std::string& path)
 
 fm_scene_desc FlatScene::desc() const
 {
+    for (size_t i = 0; i < textures.size(); ++i) textures[i].texels = texels[i].data();
     fm_scene_desc d{};
     d.num_objects = (int64_t)obj_material.size();
     d.obj_material = obj_material.data();

@@ -35,7 +35,7 @@ struct FlatScene {
     std::vector<int32_t> sphere_object;
     std::vector<fm_material_desc> materials;
     std::vector<std::vector<float>> texels;
-    std::vector<fm_texture_desc> textures;
+    mutable std::vector<fm_texture_desc> textures;   // texel pointers are set by desc()
     std::vector<fm_light_desc> lights;
 
     fm_scene_desc desc() const;
