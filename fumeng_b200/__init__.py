@@ -133,6 +133,7 @@ def load_library() -> C.CDLL:
                                C.POINTER(Tuning)], C.c_int),
         "fm_scene_load": ([vp, C.c_char_p, C.POINTER(vp), C.POINTER(Camera), C.POINTER(RenderParams)], C.c_int),
         "fm_draw_frame": ([vp, C.c_char_p], C.c_int),
+        "fm_trace_closest_noalloc": ([vp, vp, vp, C.c_int64, vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -144,7 +145,7 @@ def load_library() -> C.CDLL:
 
 EXPORTED_SYMBOLS = ["fm_ctx_create", "fm_ctx_destroy", "fm_last_error", "fm_scene_create", "fm_scene_destroy",
                     "fm_scene_bvh_stats", "fm_trace_closest", "fm_trace_any", "fm_render", "fm_render_batch",
-                    "fm_autotune_batch", "fm_scene_load", "fm_draw_frame"]
+                    "fm_autotune_batch", "fm_scene_load", "fm_draw_frame", "fm_trace_closest_noalloc"]
 
 
 def _ptr(a, ctype=C.c_void_p):
@@ -261,6 +262,15 @@ class Scene:
         obj = np.empty(n, np.int32)
         t = np.empty(n, np.float32)
         self.ctx.check(self.ctx.lib.fm_trace_closest(self.ctx.h, self.h, _ptr(rays), n, _ptr(obj), _ptr(t), 0))
+        return obj, t
+
+    def trace_closest_noalloc(self, rays: np.ndarray):
+        """fm_trace_closest through the library's fixed staging area (no device allocation)."""
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        obj = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        self.ctx.check(self.ctx.lib.fm_trace_closest_noalloc(self.ctx.h, self.h, _ptr(rays), n, _ptr(obj), _ptr(t)))
         return obj, t
 
     def trace_any(self, rays: np.ndarray) -> np.ndarray:

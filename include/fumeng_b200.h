@@ -260,6 +260,21 @@ fm_status fm_scene_load(fm_ctx* ctx, const char* json_path, fm_scene** out, fm_c
  * <output>_albedo.png and <output>_normal.png. */
 fm_status fm_draw_frame(fm_ctx* ctx, const char* json_path);
 
+/* No counterpart in the reference (its queries never leave host memory).  Same query and
+ * results as fm_trace_closest with host buffers, for callers that cannot have the
+ * library allocate device memory while they run -- a real-time loop with a fixed
+ * device-memory budget and a frame deadline, or an application whose own pool owns the
+ * device memory.  Instead of per-call allocations it stages rays and results in a fixed
+ * 10 MiB array that is part of the library image; every GPU that loads the library holds
+ * that array until the process exits.
+ *   - n may be at most 262144 rays; larger batches are rejected with FM_ERR_INVALID.
+ *   - The first call on a device looks up the array's device address (with that device
+ *     current); make that first call before any stream capture.
+ *   - All calls on a device share the array: calls that run at the same time on that
+ *     device (from different contexts or threads) race with each other. */
+fm_status fm_trace_closest_noalloc(fm_ctx* ctx, const fm_scene* scene, const float* rays, int64_t n,
+                                   int32_t* obj_id, float* t);
+
 #ifdef __cplusplus
 }
 #endif
