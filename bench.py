@@ -15,7 +15,10 @@ value  : device-resident scenes, device output images; time = device time of the
 e2e    : the same metric through the C-ABI from host memory: every step creates the 64
          scenes from host descriptors (upload + device BVH build + env tables), renders
          into host images and destroys the scenes.
-The plain per-pixel megakernel is timed on the same batch for comparison.
+The plain per-pixel megakernel is timed on the same batch for comparison, and the
+path-replay adjoint against its own forward pass on the inverse-rendering workload
+(fumeng_b200.synth.inverse_scene: 120k triangles, 512^2 basecolor and roughness /
+metallic textures, 16 views of 256^2, 32 spp forward and 32 spp adjoint, depth 6).
 """
 from __future__ import annotations
 
@@ -163,6 +166,50 @@ def run_reference(args, specs=None, steps=None, warmup=None, sample_scenes=2, sp
 
 # ---- our arm (GPU) ---------------------------------------------------------------------
 
+ADJ_WORKLOAD = ("inverse rendering: 120k-tri UV-mapped displaced plane + sphere, Disney with 512^2 basecolor and "
+                "roughness(G)/metallic(B) textures, 16 views 256^2, 32 spp forward + 32 spp adjoint, depth 6")
+
+
+def measure_adjoint(ctx, args, barrier, max_over_ranks):
+    """Device time of the path-replay adjoint (gradients w.r.t. both 512^2 textures and
+    the env texels) against the forward wavefront render of the same 16 views."""
+    import fumeng_b200 as fb
+    from fumeng_b200 import synth
+    from fumeng_b200.scene import camera_struct
+    spec = synth.inverse_scene(target=True)
+    holder = spec.to_desc()
+    ti = holder.texture_index
+    sc = ctx.create_scene(holder)
+    cams = [camera_struct(c) for c in synth.inverse_views(16)]
+    fwd = [spec.render_params(spp=32, seed=100 + v) for v in range(16)]
+    adj = [spec.render_params(spp=32, seed=5000 + v) for v in range(16)]
+    tune = fb.Tuning(1 << 21, 128, 128, 8)
+    d_rgb = [np.random.default_rng(v).standard_normal((p.height, p.width, 3)).astype(np.float32) * 1e-3
+             for v, p in enumerate(adj)]
+    shapes = {ti["basecolor"]: spec.textures["basecolor"].shape[:2], ti["rm"]: spec.textures["rm"].shape[:2],
+              ti["sky"]: spec.textures["sky"].shape[:2]}
+    ctx.render_batch([sc] * 16, cams, fwd, tuning=tune)
+    sc.render_adjoint(cams, adj, d_rgb, shapes)
+    f_ms, a_ms, a_wall, nans = [], [], [], 0
+    for _ in range(args.adjoint_steps):
+        barrier()
+        st = ctx.render_batch([sc] * 16, cams, fwd, tuning=tune)[3]
+        f_ms.append(st.kernel_ms)
+        t0 = time.perf_counter()
+        _, _, _, sa = sc.render_adjoint(cams, adj, d_rgb, shapes)
+        a_wall.append(1e3 * (time.perf_counter() - t0))
+        a_ms.append(sa.kernel_ms)
+        nans += sa.nan_samples
+    sc.destroy()
+    f, a = max_over_ranks(float(np.mean(f_ms))), max_over_ranks(float(np.mean(a_ms)))
+    paths = sum(p.width * p.height * p.spp for p in fwd)
+    return {"workload": ADJ_WORKLOAD, "forward_ms": f, "adjoint_ms": a, "adjoint_over_forward": a / f,
+            "adjoint_wall_ms_host_buffers": float(np.mean(a_wall)), "forward_mpaths_s": paths / f / 1e3,
+            "adjoint_mpaths_s": paths / a / 1e3, "grad_texels": int(sum(h * w for h, w in shapes.values())),
+            "nan_samples": int(nans), "steps": args.adjoint_steps,
+            "timing": "device time of the wavefront loop (CUDA events), same default tuning for both passes"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -173,6 +220,7 @@ def main():
     ap.add_argument("--mk-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scenes", type=int, default=NSCENES, help="batch size (profiling runs use fewer)")
+    ap.add_argument("--adjoint-steps", type=int, default=2, help="timed adjoint/forward pairs (0 skips)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -293,7 +341,9 @@ def main():
     alg_bytes = totals["closest"] * closest_b + totals["shadow"] * shadow_b
     peak, peak_kind = measured_peak_hbm()
     achieved = alg_bytes / (totals["trace_ms"] / 1e3) / 1e9 if totals["trace_ms"] > 0 else None
-    launches_trace = max(1, totals["launches"] // 3)
+    # five launches per wavefront iteration (prep, trace, two shade kernels, logic) plus
+    # one init and one reduce per view per step
+    launches_trace = max(1, (totals["launches"] - args.steps * (1 + len(specs))) // 5)
     traffic = None
     if TRACE_DRAM_BYTES_PER_RAY is not None:
         traffic = TRACE_DRAM_BYTES_PER_RAY * (totals["closest"] + totals["shadow"]) / launches_trace
@@ -327,6 +377,8 @@ def main():
                "unit": "Mpaths/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": e2e_ms / args.e2e_steps}
 
+    adj = measure_adjoint(ctx, args, barrier, max_over_ranks) if args.adjoint_steps > 0 else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = run_reference(args, steps=2, warmup=0, sample_scenes=4, spp=1)
@@ -351,6 +403,7 @@ def main():
                          "shadow_rays": totals["shadow"] / totals["paths"],
                          "bounces": totals["bounces"] / totals["paths"]},
             "nan_samples": int(totals["nans"]),
+            "adjoint": adj,
         }
         print(json.dumps(line))
     ctx.close()

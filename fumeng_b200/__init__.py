@@ -101,6 +101,13 @@ class FumengError(RuntimeError):
         self.status = status
 
 
+class GradDesc(C.Structure):
+    """fm_grad_desc: gradient outputs of fm_render_adjoint (added to)."""
+    _fields_ = [("texture_grads", C.POINTER(C.c_void_p)), ("material_grads", C.c_void_p)]
+
+
+GRAD_PARAMS = 5   # basecolor r, g, b, metallic, roughness
+
 _lib = None
 
 
@@ -134,6 +141,11 @@ def load_library() -> C.CDLL:
         "fm_scene_load": ([vp, C.c_char_p, C.POINTER(vp), C.POINTER(Camera), C.POINTER(RenderParams)], C.c_int),
         "fm_draw_frame": ([vp, C.c_char_p], C.c_int),
         "fm_trace_closest_noalloc": ([vp, vp, vp, C.c_int64, vp, vp], C.c_int),
+        "fm_scene_update_texture": ([vp, vp, C.c_int32, vp, C.c_int32], C.c_int),
+        "fm_scene_info": ([vp, vp, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                           C.POINTER(C.c_int32)], C.c_int),
+        "fm_render_adjoint": ([vp, vp, C.c_int32, C.POINTER(Camera), C.POINTER(RenderParams), C.POINTER(vp),
+                               C.POINTER(vp), C.POINTER(GradDesc), C.c_int32, C.POINTER(RenderStats)], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -145,7 +157,8 @@ def load_library() -> C.CDLL:
 
 EXPORTED_SYMBOLS = ["fm_ctx_create", "fm_ctx_destroy", "fm_last_error", "fm_scene_create", "fm_scene_destroy",
                     "fm_scene_bvh_stats", "fm_trace_closest", "fm_trace_any", "fm_render", "fm_render_batch",
-                    "fm_autotune_batch", "fm_scene_load", "fm_draw_frame", "fm_trace_closest_noalloc"]
+                    "fm_autotune_batch", "fm_scene_load", "fm_draw_frame", "fm_trace_closest_noalloc",
+                    "fm_scene_update_texture", "fm_render_adjoint", "fm_scene_info"]
 
 
 def _ptr(a, ctype=C.c_void_p):
@@ -279,6 +292,45 @@ class Scene:
         occ = np.empty(n, np.uint8)
         self.ctx.check(self.ctx.lib.fm_trace_any(self.ctx.h, self.h, _ptr(rays), n, _ptr(occ), 0))
         return occ
+
+    def info(self) -> dict:
+        o, m, t, l = C.c_int64(), C.c_int32(), C.c_int32(), C.c_int32()
+        self.ctx.check(self.ctx.lib.fm_scene_info(self.ctx.h, self.h, C.byref(o), C.byref(m), C.byref(t), C.byref(l)))
+        return {"objects": o.value, "materials": m.value, "textures": t.value, "lights": l.value}
+
+    def update_texture(self, index: int, texels: np.ndarray) -> None:
+        """Replace texture `index`'s texels (HxWx3 float32, row 0 = top) in place."""
+        texels = np.ascontiguousarray(texels, dtype=np.float32)
+        self.ctx.check(self.ctx.lib.fm_scene_update_texture(self.ctx.h, self.h, int(index), _ptr(texels), 0))
+
+    def render_adjoint(self, cams, params, d_rgb, texture_shapes: dict, material_grads: bool = False,
+                       want_image: bool = False):
+        """Path-replay adjoint over views (cams[i], params[i]) with dLoss/dI images d_rgb[i].
+
+        texture_shapes: {texture index: (height, width)} of the textures whose texel
+        gradients are wanted.  Returns (texture grads {index: HxWx3 float64},
+        material grads (num_materials x 5 float64) or None, images or None, stats)."""
+        n = len(cams)
+        ca = (Camera * n)(*cams)
+        pa = (RenderParams * n)(*params)
+        d_rgb = [np.ascontiguousarray(d, dtype=np.float32) for d in d_rgb]
+        dp = (C.c_void_p * n)(*[d.ctypes.data for d in d_rgb])
+        imgs = [np.empty((p.height, p.width, 3), np.float32) for p in params] if want_image else None
+        ip = (C.c_void_p * n)(*[a.ctypes.data for a in imgs]) if want_image else None
+        info = self.info()
+        nt = info["textures"]
+        if any(k < 0 or k >= nt for k in texture_shapes):
+            raise ValueError("texture index out of range")
+        tg = {k: np.zeros((h, w, 3), np.float64) for k, (h, w) in texture_shapes.items()}
+        tarr = (C.c_void_p * max(nt, 1))(*[tg[k].ctypes.data if k in tg else None for k in range(nt)])
+        mg = None
+        if material_grads:
+            mg = np.zeros((info["materials"], GRAD_PARAMS), np.float64)
+        gd = GradDesc(tarr if nt else None, mg.ctypes.data if mg is not None else None)
+        stats = RenderStats()
+        self.ctx.check(self.ctx.lib.fm_render_adjoint(self.ctx.h, self.h, n, ca, pa, dp, ip, C.byref(gd), 0,
+                                                      C.byref(stats)))
+        return tg, mg, imgs, stats
 
     def render(self, camera: Camera, params: RenderParams, want_aov: bool = True):
         """Returns (rgb, albedo, normal, stats) as HxWx3 float32 arrays (row 0 = top)."""

@@ -11,6 +11,7 @@
 //   material/material_common.cpp       GTR1/GTR2, Smith, refraction
 #pragma once
 #include "fm_common.cuh"
+#include "fm_dual.cuh"
 #include "fm_scene.cuh"
 #include "fm_texture.cuh"
 
@@ -85,27 +86,31 @@ FM_D bool refract_dir(f3 wi, f3 n, float eta, f3& out)
     return true;
 }
 
-FM_D float sph_phi(f3 w)
-{
-    const float p = atan2f(w.y, w.x);
-    return p < 0 ? p + 2.0f * kPi : p;
-}
-FM_D float sph_theta(f3 w) { return acosf(clampf(w.z, -1.0f, 1.0f)); }
+// The microfacet helpers below evaluate the reference's formulas
+// (material_common.cpp:7-103), which are written with the spherical angles of a unit
+// vector w (phi = atan2(y, x), theta = acos(z)), with those angles eliminated:
+// sin(theta)cos(phi) = x, sin(theta)sin(phi) = y, cos(theta) = z,
+// tan^2(theta) = (1 - z^2) / z^2.  The functions are the same; only rounding differs,
+// and the code avoids acos/atan2/tan and their large inline expansions.
 
-FM_D float gtr2_aniso(f3 wh, float ax, float ay)
+// GTR2Anisotropic: 1 / (pi ax ay (sin^2(th)(cos^2(ph)/ax^2 + sin^2(ph)/ay^2) + cos^2(th))^2)
+// (T is float, or a dual number when the adjoint differentiates with respect to the
+// roughness that the alphas come from.)
+template <class T>
+FM_D T gtr2_aniso(f3 wh, T ax, T ay)
 {
-    const float phi = sph_phi(wh), theta = sph_theta(wh);
-    const float a = cosf(phi) / ax;
-    const float b = sinf(phi) / ay;
-    const float st = sinf(theta), ct = cosf(theta);
-    const float den = st * st * (a * a + b * b) + ct * ct;
+    const float z = clampf(wh.z, -1.0f, 1.0f);
+    const T a = wh.x / ax, b = wh.y / ay;
+    const T den = a * a + b * b + z * z;
     return 1.0f / (kPi * ax * ay * den * den);
 }
 
 FM_D f3 sample_gtr2(float ax, float ay, float u0, float u1)
 {
-    float sin_phi = ay * sinf(2.0f * kPi * u0);
-    float cos_phi = ax * cosf(2.0f * kPi * u0);
+    float s2, c2;
+    sincosf(2.0f * kPi * u0, &s2, &c2);
+    float sin_phi = ay * s2;
+    float cos_phi = ax * c2;
     const float norm = 1.0f / sqrtf(sin_phi * sin_phi + cos_phi * cos_phi);
     sin_phi *= norm;
     cos_phi *= norm;
@@ -117,12 +122,13 @@ FM_D f3 sample_gtr2(float ax, float ay, float u0, float u1)
     return normalize(f3{st * cos_phi, st * sin_phi, ct});
 }
 
+// GTR1GGX: (a^2 - 1) / (2 pi log(a) (a^2 cos^2(th) + sin^2(th)))
 FM_D float gtr1(f3 wh, float alpha)
 {
-    const float theta = sph_theta(wh);
-    const float st = sinf(theta), ct = cosf(theta);
+    const float z = clampf(wh.z, -1.0f, 1.0f);
+    const float c2 = z * z;
     const float a2 = alpha * alpha;
-    const float den = 2.0f * kPi * logf(alpha) * (a2 * ct * ct + st * st);
+    const float den = 2.0f * kPi * logf(alpha) * (a2 * c2 + (1.0f - c2));
     return (a2 - 1.0f) / den;
 }
 
@@ -131,30 +137,37 @@ FM_D f3 sample_gtr1(float alpha, float u0, float u1)
     const float phi = 2.0f * kPi * u0;
     const float ct = sqrtf((powf(alpha, 2.0f - 2.0f * u1) - 1.0f) / (alpha * alpha - 1.0f));
     const float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
-    return normalize(f3{st * cosf(phi), st * sinf(phi), ct});
+    float sp, cp;
+    sincosf(phi, &sp, &cp);
+    return normalize(f3{st * cp, st * sp, ct});
 }
 
-FM_D float smith_lambda(f3 w, float ax, float ay)
+// SmithLambda: -1/2 + 1/2 sqrt(1 + (cos^2(ph) ax^2 + sin^2(ph) ay^2) tan^2(th))
+template <class T>
+FM_D T smith_lambda(f3 w, T ax, T ay)
 {
-    const float phi = sph_phi(w), theta = sph_theta(w);
-    const float a = cosf(phi) * ax;
-    const float b = sinf(phi) * ay;
-    const float tt = tanf(theta);
-    return -0.5f + 0.5f * sqrtf(1.0f + (a * a + b * b) * tt * tt);
+    const float z = clampf(w.z, -1.0f, 1.0f);
+    const T a = w.x * ax, b = w.y * ay;
+    const T t = (a * a + b * b) / (z * z);
+    return -0.5f + 0.5f * dsqrt(1.0f + t);
 }
 
 // SmithGGXAnisotropic uses alpha_y for both axes (material_common.cpp:85-90).
-FM_D float smith_ggx_aniso(f3 wo, f3 wi, float ax, float ay)
+template <class T>
+FM_D T smith_ggx_aniso(f3 wo, f3 wi, T ax, T ay)
 {
     (void)ax;
-    const float li = smith_lambda(wi, ay, ay) + 1.0f;
-    const float lo = smith_lambda(wo, ay, ay) + 1.0f;
+    const T li = smith_lambda(wi, ay, ay) + 1.0f;
+    const T lo = smith_lambda(wo, ay, ay) + 1.0f;
     return 1.0f / li / lo;
 }
 
+// SmithGGXSeprate: 2 / (1 + sqrt(1 + (alpha tan(th))^2)), 1 when tan(th) < eps_pdf
 FM_D float smith_ggx_sep(f3 w, float alpha)
 {
-    const float tt = fabsf(tanf(sph_theta(w)));
+    const float z = clampf(w.z, -1.0f, 1.0f);
+    const float s2 = fmaxf(0.0f, 1.0f - z * z);
+    const float tt = sqrtf(s2) / fabsf(z);
     if (tt < kEpsPdf) return 1.0f;
     const float den = tt * alpha;
     return 2.0f / (1.0f + sqrtf(1.0f + den * den));
@@ -264,16 +277,25 @@ FM_D void disney_setup(Disney& d, float wo_z)
     }
 }
 
+// Material classes for specialised shading kernels: kClsDisney holds only Disney,
+// kClsSimple holds Lambert / conductor / dielectric, kClsAny holds every type.  A kernel
+// instantiated for one class contains only that class's code.
+constexpr int kClsAny = -1, kClsDisney = 0, kClsSimple = 1;
+FM_HD int material_class(int type) { return type == 3 ? kClsDisney : kClsSimple; }
+
+template <int CLS = kClsAny>
 FM_D Bsdf make_bsdf(const DevScene& S, const HitInfo& h)
 {
     Bsdf b;
     const DevMaterial& M = S.materials[h.mat];
-    b.type = M.type;
+    b.type = CLS == kClsDisney ? 3 : M.type;
     b.ng = h.ng;
     b.zs = h.ns;
     b.xs = normalize(h.ss);
     b.ys = cross(b.zs, b.xs);
-    if (M.type == 0) {
+    if (CLS == kClsDisney) {
+        // fall through to the Disney branch below
+    } else if (M.type == 0) {
         b.color = fetch(S, M.p[MP_BASECOLOR], h);
     } else if (M.type == 1) {
         b.color = ld3(M.color);
@@ -284,7 +306,8 @@ FM_D Bsdf make_bsdf(const DevScene& S, const HitInfo& h)
         b.color2 = ld3(M.refract_color);
         b.eta_i = M.eta_i;
         b.eta_t = M.eta_t;
-    } else {
+    }
+    if (CLS != kClsSimple && b.type == 3) {
         Disney& d = b.d;
         d.basecolor = fetch(S, M.p[MP_BASECOLOR], h);
         d.metallic = fetch(S, M.p[MP_METALLIC], h).z;
@@ -426,9 +449,10 @@ FM_D float ds_cc_pdf(const Disney& d, f3 wo, f3 wi)
 
 // DisneyMicrofacetTransmission with lobe alphas (ax, ay) and colour `c`.  Sampling and
 // pdf use the BSDF's trans_alpha (disney.cpp:238-273) whatever the lobe's own alphas.
-FM_D f3 ds_trans_eval(const Disney& d, f3 wo, f3 wi, float ax, float ay, f3 c)
+// |ft| of the transmission lobe: everything but spec_trans (1 - metallic) c; wo, wi in
+// opposite hemispheres.
+FM_D float ds_trans_ft(const Disney& d, f3 wo, f3 wi, float ax, float ay)
 {
-    if (!opposite_hemi(wo, wi)) return mk(0.0f);
     const float eta = wo.z > 0 ? d.ior : d.ior_r;
     f3 wh = normalize(wo + eta * wi);
     if (wh.z < 0) wh = -wh;
@@ -439,9 +463,14 @@ FM_D f3 ds_trans_eval(const Disney& d, f3 wo, f3 wi, float ax, float ay, f3 c)
     const float G = smith_ggx_aniso(wo, wi, ax, ay);
     const float den = eta * cdi + cdo;
     const float q = cos_i * cos_o * den * den;
-    if (q == 0.0f) return mk(0.0f);
-    const float ft = (1.0f - f) * D * G * cdo * cdi / q;
-    return d.spec_trans * (1.0f - d.metallic) * c * fabsf(ft);
+    if (q == 0.0f) return 0.0f;
+    return fabsf((1.0f - f) * D * G * cdo * cdi / q);
+}
+
+FM_D f3 ds_trans_eval(const Disney& d, f3 wo, f3 wi, float ax, float ay, f3 c)
+{
+    if (!opposite_hemi(wo, wi)) return mk(0.0f);
+    return d.spec_trans * (1.0f - d.metallic) * c * ds_trans_ft(d, wo, wi, ax, ay);
 }
 
 FM_D f3 ds_trans_sample(const Disney& d, f3 wo, float u0, float u1)
@@ -556,29 +585,37 @@ FM_D f3 disney_sample_dir(const Disney& d, f3 wo, f3 u)
 // ---- BSDF interface (bsdf.h:136-182 and the overrides) ------------------------------
 
 // CalFunc(wo_w, wi_w)
+template <int CLS = kClsAny>
 FM_D f3 bsdf_f(const Bsdf& b, f3 wo_w, f3 wi_w)
 {
-    if (b.type == 0) return b.color * kInvPi;
-    if (b.type == 1 || b.type == 2) return mk(0.0f);
+    if (CLS != kClsDisney) {
+        if (b.type == 0) return b.color * kInvPi;
+        if (b.type == 1 || b.type == 2 || CLS == kClsSimple) return mk(0.0f);
+    }
     return disney_f(b.d, to_local(b, wo_w), to_local(b, wi_w));
 }
 
 // Pdf(wo_w, wi_w)
+template <int CLS = kClsAny>
 FM_D float bsdf_pdf(const Bsdf& b, f3 wo_w, f3 wi_w)
 {
-    if (b.type == 1 || b.type == 2) return 0.0f;
+    if (CLS != kClsDisney && (b.type == 1 || b.type == 2)) return 0.0f;
     const f3 wo = to_local(b, wo_w), wi = to_local(b, wi_w);
-    if (b.type == 0) {
-        if (wo.z * wi.z < 0.0f) return 0.0f;
-        return fabsf(wi.z) * kInvPi;
+    if (CLS != kClsDisney) {
+        if (b.type == 0 || CLS == kClsSimple) {
+            if (wo.z * wi.z < 0.0f) return 0.0f;
+            return fabsf(wi.z) * kInvPi;
+        }
     }
     return disney_pdf(b.d, wo, wi);
 }
 
+template <int CLS = kClsAny>
 FM_D BsdfSample bsdf_sample(const Bsdf& b, f3 wo_w, f3 u)
 {
     BsdfSample s;
     const f3 wo = to_local(b, wo_w);
+    if (CLS == kClsDisney) goto disney;
     if (b.type == 0) {
         f3 wi = cosine_hemisphere(u.x, u.y);
         if (wo.z * wi.z < 0.0f) wi.z *= -1.0f;
@@ -653,6 +690,14 @@ FM_D BsdfSample bsdf_sample(const Bsdf& b, f3 wo_w, f3 u)
         s.wi = to_world(b, wt);
         return s;
     }
+    if (CLS == kClsSimple) {
+        s.f = mk(0.0f);
+        s.wi = mk(0.0f);
+        s.pdf = 0.0f;
+        s.delta = false;
+        return s;
+    }
+disney:
     // Disney: SampleBSDF -> SampleInfoFromWoWi (disney.cpp:481-548)
     const f3 wi = disney_sample_dir(b.d, wo, u);
     s.delta = false;

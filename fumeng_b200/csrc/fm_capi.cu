@@ -398,6 +398,7 @@ fm_status fm_scene_create(fm_ctx* ctx, const fm_scene_desc* d, fm_scene** out)
         }
         FM_TRY(upload(ctx, sc, texs.data(), texs.size(), &S.textures));
         S.num_textures = d->num_textures;
+        sc->textures = texs;
         // lights: area lights in object order (Scene::Scene via
         // Aggregate::ConstructAreaLight, core/scene.h:21-25), then the given lights
         std::vector<DevLight> lights;

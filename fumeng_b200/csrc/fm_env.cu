@@ -141,7 +141,48 @@ __global__ void k_env_alias_marg(const double* rowsum, int h, float* prob, int32
     vose(nullptr, rowsum, h, prob, alias, scratch, scratch + h);
 }
 
+// grad[k][l][c] -= total_score * d log(sum lum)/d texel + row_score[k] * d log(rowsum_k)/d texel,
+// with d lum[k][l] / d texel[k][l][c] = L_c * sin_k (lum as in k_env_lum).
+__global__ void k_env_grad_spread(const float* lum, const double* rowsum, const double* totals, const double* row_score,
+                                  const double* total_score, int w, int h, double* grad)
+{
+    const int n = w * h;
+    const double total = totals[0], ts = total_score[0];
+    const double Lc[3] = {0.2126, 0.7152, 0.0722};
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const int j = q / w;
+        const double sin_theta = (double)sinf(kPi * (((float)j + 0.5f) / (float)h));
+        const double k_tot = total > 0.0 ? ts * sin_theta / total : 0.0;
+        const double k_row = rowsum[j] > 0.0 ? row_score[j] * sin_theta / rowsum[j] : 0.0;
+        for (int c = 0; c < 3; ++c) grad[3 * (size_t)q + c] -= (k_tot + k_row) * Lc[c];
+    }
+}
+
 }  // namespace
+
+fm_status env_grad_finalize(fm_ctx* ctx, const DevTexture& tex, const double* env_row, const double* env_total,
+                            double* grad)
+{
+    const int w = tex.w, h = tex.h;
+    const size_t n = (size_t)w * h;
+    cudaStream_t st = ctx->stream;
+    float* lum = nullptr;
+    double *rowsum = nullptr, *totals = nullptr;
+    FM_CUDA_TRY(ctx, cudaMallocAsync(&lum, n * sizeof(float), st), "env grad");
+    FM_CUDA_TRY(ctx, cudaMallocAsync(&rowsum, h * sizeof(double), st), "env grad");
+    FM_CUDA_TRY(ctx, cudaMallocAsync(&totals, 2 * sizeof(double), st), "env grad");
+    const int grid = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
+    k_env_lum<<<grid, 256, 0, st>>>(tex, w, h, lum);
+    k_env_rowsum<<<h, 256, 0, st>>>(lum, w, rowsum);
+    k_env_totals<<<1, 256, 0, st>>>(rowsum, w, h, totals);
+    k_env_grad_spread<<<grid, 256, 0, st>>>(lum, rowsum, totals, env_row, env_total, w, h, grad);
+    const cudaError_t e = cudaGetLastError();
+    cudaFreeAsync(lum, st);
+    cudaFreeAsync(rowsum, st);
+    cudaFreeAsync(totals, st);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "env grad");
+    return FM_OK;
+}
 
 fm_status env_build_tables(fm_ctx* ctx, fm_scene* scene, const DevTexture& tex, DevEnv& env)
 {
@@ -151,18 +192,28 @@ fm_status env_build_tables(fm_ctx* ctx, fm_scene* scene, const DevTexture& tex, 
     int32_t *row_alias = nullptr, *marg_alias = nullptr, *scratch = nullptr;
     double *rowsum = nullptr, *totals = nullptr;
     auto track = [&](void* p) { scene->allocations.push_back(p); };
-    FM_CUDA_TRY(ctx, cudaMalloc(&pdf_sample, n * sizeof(float)), "env tables");
-    track(pdf_sample);
-    FM_CUDA_TRY(ctx, cudaMalloc(&pdf_eval, n * sizeof(float)), "env tables");
-    track(pdf_eval);
-    FM_CUDA_TRY(ctx, cudaMalloc(&row_prob, n * sizeof(float)), "env tables");
-    track(row_prob);
-    FM_CUDA_TRY(ctx, cudaMalloc(&row_alias, n * sizeof(int32_t)), "env tables");
-    track(row_alias);
-    FM_CUDA_TRY(ctx, cudaMalloc(&marg_prob, h * sizeof(float)), "env tables");
-    track(marg_prob);
-    FM_CUDA_TRY(ctx, cudaMalloc(&marg_alias, h * sizeof(int32_t)), "env tables");
-    track(marg_alias);
+    if (env.pdf_sample && env.w == w && env.h == h) {
+        // rebuilding for new texel values: reuse the tables
+        pdf_sample = const_cast<float*>(env.pdf_sample);
+        pdf_eval = const_cast<float*>(env.pdf_eval);
+        row_prob = const_cast<float*>(env.row_prob);
+        row_alias = const_cast<int32_t*>(env.row_alias);
+        marg_prob = const_cast<float*>(env.marg_prob);
+        marg_alias = const_cast<int32_t*>(env.marg_alias);
+    } else {
+        FM_CUDA_TRY(ctx, cudaMalloc(&pdf_sample, n * sizeof(float)), "env tables");
+        track(pdf_sample);
+        FM_CUDA_TRY(ctx, cudaMalloc(&pdf_eval, n * sizeof(float)), "env tables");
+        track(pdf_eval);
+        FM_CUDA_TRY(ctx, cudaMalloc(&row_prob, n * sizeof(float)), "env tables");
+        track(row_prob);
+        FM_CUDA_TRY(ctx, cudaMalloc(&row_alias, n * sizeof(int32_t)), "env tables");
+        track(row_alias);
+        FM_CUDA_TRY(ctx, cudaMalloc(&marg_prob, h * sizeof(float)), "env tables");
+        track(marg_prob);
+        FM_CUDA_TRY(ctx, cudaMalloc(&marg_alias, h * sizeof(int32_t)), "env tables");
+        track(marg_alias);
+    }
     // temporaries
     FM_CUDA_TRY(ctx, cudaMalloc(&lum, n * sizeof(float)), "env tables");
     FM_CUDA_TRY(ctx, cudaMalloc(&scratch, 2 * n * sizeof(int32_t)), "env tables");

@@ -27,6 +27,7 @@ struct fm_scene {
     int64_t num_objects = 0;
     // host copies kept for validation and light sampling set-up
     std::vector<fm::DevLight> lights;
+    std::vector<fm::DevTexture> textures;   // device texel pointers, for in-place updates
 };
 
 namespace fm {

@@ -21,7 +21,21 @@ struct WfView {
     float* rgb;              // outputs (device)
     float* alb;
     float* nrm;
+    const float* drgb;       // adjoint renders: dLoss/dI per pixel (device, w*h*3)
 };
+
+// Gradient outputs of an adjoint render (device buffers, added to).
+struct WfAdjoint {
+    double* const* tex_grad;   // device array over the scene's textures: NULL or w*h*3
+    double* mat_grad;          // num_materials * 5 (basecolor rgb, metallic, roughness) or NULL
+    double* env_row;           // env map height doubles, zeroed (score sums per row)
+    double* env_total;         // one double, zeroed
+};
+
+// Spreads the env importance-table normalisation terms collected during an adjoint
+// render (row and total score sums) over the env texels' gradient.
+fm_status env_grad_finalize(fm_ctx* ctx, const DevTexture& tex, const double* env_row, const double* env_total,
+                            double* grad);
 
 // Wavefront tuning knobs (pool size, block sizes, graph depth).
 struct WfTuning {
@@ -44,5 +58,10 @@ fm_status launch_megakernel(fm_ctx* ctx, const fm_scene* scene, const DevCamera&
 // Renders several views (possibly of different scenes) in one wavefront.
 fm_status wavefront_views(fm_ctx* ctx, const std::vector<WfView>& views, const WfTuning& tune, Counters* cnt,
                           WfTimes* times);
+// Path-replay adjoint over views of one scene: gradients of sum(drgb * image) with
+// respect to texture texels and material constants.  rgb (if set) receives the primal
+// image of the same samples.
+fm_status wavefront_adjoint(fm_ctx* ctx, const std::vector<WfView>& views, const WfTuning& tune, const WfAdjoint& adj,
+                            Counters* cnt, WfTimes* times);
 
 }  // namespace fm

@@ -43,6 +43,43 @@ FM_D f3 tex_sample(const DevTexture& t, float uu, float vv)
     return (a * (1.0f - pu) + b * pu) * (1.0f - pv) + (c * (1.0f - pu) + d * pu) * pv;
 }
 
+// The texels tex_sample reads at (uu, vv) and their weights (the same taps; the
+// weights are the bilinear products), for scattering derivatives back onto texels.
+struct TexTaps {
+    int x[4], y[4];
+    float w[4];
+    int n;
+};
+
+FM_D TexTaps tex_taps(const DevTexture& t, float uu, float vv)
+{
+    TexTaps r;
+    const float u = wrap_coord(uu, t.wrap_u);
+    const float v = wrap_coord(vv, t.wrap_v);
+    const float ru = u * (float)t.w;
+    const float rv = v * (float)t.h;
+    if (t.filter == 1) {
+        int x = (int)ru, y = (int)rv;
+        r.x[0] = x < 0 ? 0 : (x > t.w - 1 ? t.w - 1 : x);
+        r.y[0] = y < 0 ? 0 : (y > t.h - 1 ? t.h - 1 : y);
+        r.w[0] = 1.0f;
+        r.n = 1;
+        return r;
+    }
+    const int u0 = (int)clampf(ru - 0.5f, 0.0f, (float)(t.w - 1));
+    const int u1 = min(u0 + 1, t.w - 1);
+    const float pu = clampf(ru - 0.5f - (float)u0, 0.0f, 1.0f);
+    const int v0 = (int)clampf(rv - 0.5f, 0.0f, (float)(t.h - 1));
+    const int v1 = min(v0 + 1, t.h - 1);
+    const float pv = clampf(rv - 0.5f - (float)v0, 0.0f, 1.0f);
+    r.x[0] = u0, r.y[0] = v0, r.w[0] = (1.0f - pu) * (1.0f - pv);
+    r.x[1] = u1, r.y[1] = v0, r.w[1] = pu * (1.0f - pv);
+    r.x[2] = u0, r.y[2] = v1, r.w[2] = (1.0f - pu) * pv;
+    r.x[3] = u1, r.y[3] = v1, r.w[3] = pu * pv;
+    r.n = 4;
+    return r;
+}
+
 // GetSphericalUV (core/utils.h:149-173): z-up, u = phi / 2pi, v = theta / pi.
 FM_D void spherical_uv(f3 d, float& u, float& v, float& theta)
 {

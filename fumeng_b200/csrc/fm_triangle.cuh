@@ -40,6 +40,16 @@ FM_D RayPre ray_pre(f3 o, f3 d)
         az = 0;
     else
         az = a1 > a2 ? 1 : 2;
+    // A main-axis component of zero (or so small that 1/dz overflows) makes the shear
+    // infinite and every edge function NaN; the reference then reports NaN hits.  Its
+    // double build practically never draws such a ray, but float sampling does (a
+    // cosine-hemisphere sample at an axis-aligned wall has d.z == 0 exactly about once
+    // in 2^24 draws), so those rays use the axis of largest magnitude instead.  Rays
+    // with |dz| >= 1e-30 keep the reference's choice and its results bit for bit.
+    if (!(fabsf(comp(d, az)) >= 1e-30f)) {
+        const float m0 = fabsf(d.x), m1 = fabsf(d.y), m2 = fabsf(d.z);
+        az = (m0 >= m1 && m0 >= m2) ? 0 : (m1 >= m2 ? 1 : 2);
+    }
     const int ax = (az + 1) % 3;
     const int ay = (ax + 1) % 3;
     p.kx = ax;
@@ -58,9 +68,10 @@ FM_D float edge_double(float ax, float ay, float bx, float by)
     return __double2float_rn(__dsub_rn(__dmul_rn((double)ax, (double)by), __dmul_rn((double)ay, (double)bx)));
 }
 
-// triangle_func::IntersectTriangle.  Returns true on a hit with t in (tmin, tmax)
-// (the comparisons are written as the reference's rejection test, so a NaN t is
-// accepted exactly as on the CPU).
+// triangle_func::IntersectTriangle.  Returns true on a hit with t in (tmin, tmax).  The
+// reference's rejection test (t <= tmin || t >= tmax) lets a NaN t through; here a NaN
+// t is rejected as well (it arises only from degenerate input, never on a ray the
+// reference handles with finite arithmetic).
 FM_D bool intersect_triangle(const RayPre& r, f3 v0, f3 v1, f3 v2, float tmin, float tmax, float& t_out,
                              float& b0, float& b1, float& b2)
 {
@@ -96,7 +107,7 @@ FM_D bool intersect_triangle(const RayPre& r, f3 v0, f3 v1, f3 v2, float tmin, f
     p2z = __fmul_rn(p2z, r.sz);
     const float inv_det = __fdiv_rn(1.0f, det);
     const float t = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(e0, p0z), __fmul_rn(e1, p1z)), __fmul_rn(e2, p2z)), inv_det);
-    if (t <= tmin || t >= tmax) return false;
+    if (t <= tmin || t >= tmax || t != t) return false;
     t_out = t;
     b0 = __fmul_rn(e0, inv_det);
     b1 = __fmul_rn(e1, inv_det);

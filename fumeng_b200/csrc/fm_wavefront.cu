@@ -3,14 +3,19 @@
 // is done.  Works on any number of views (one view = one camera over one scene), which
 // is how a batch of scenes renders in one launch.
 //
-// Queues (rebuilt every iteration by the shade kernel, consumed by the trace kernel):
+// One iteration is five launches: prep (swap queue counters), trace, shade for Disney
+// surfaces, shade for the other materials, logic (finish samples, start new ones).
+// Ray queues (filled by the shade and logic kernels, consumed by the next trace):
 //   cont    slot ids whose continuation ray is in the slot's ray registers
 //   mis     MIS-BSDF rays (origin|slot, direction|pdf, weight|view)
 //   shadow  NEE shadow rays (origin|t_max, direction|slot, contribution|view)
+// Shading queues (filled by the trace kernel, consumed by the shade kernels):
+//   disney / simple   slot ids whose continuation ray hit a surface of that class
 // Entries are appended with warp-aggregated atomics (one atomic per warp and queue:
 // ballot, popcount, prefix), so each queue is dense and its float4 records are read
-// coalesced.  The trace kernel resolves MIS and shadow rays itself and adds their
-// contribution to the slot's accumulator; the next shade folds it into the path.
+// coalesced.  The trace kernel resolves MIS and shadow rays itself, and the emission a
+// continuation ray sees at the first bounce, by adding their contribution to the
+// slot's accumulator; the logic kernel folds it into the path.
 //
 // Work items are (view, pixel, chunk of `chunk` consecutive samples).  A slot runs its
 // item's samples one after another with Kahan-compensated sums and writes the item's
@@ -19,6 +24,7 @@
 #include <cmath>
 #include <vector>
 
+#include "fm_bsdf_grad.cuh"
 #include "fm_path.cuh"
 #include "fm_render.h"
 
@@ -28,7 +34,18 @@ namespace {
 
 constexpr int kNeedItem = -2;
 constexpr int kDone = -1;
-constexpr int kHasCont = 1;
+// slot flags (depth in bits 8..): a continuation ray was queued / shadow or MIS rays of
+// this slot are queued, both set by the shading kernels and read by the logic kernel
+constexpr int kNextCont = 1;
+constexpr int kPending = 2;
+// adjoint renders: the slot is replaying its sample's path (second pass)
+constexpr int kReplay = 4;
+// queue counters: the three ray queues being filled for the next trace, the same three
+// being traced, slots still holding work, and the two shading queues
+constexpr int kQcCont = 0, kQcMis = 1, kQcShadow = 2;
+constexpr int kQcTraceCont = 3, kQcTraceMis = 4, kQcTraceShadow = 5;
+constexpr int kQcActive = 6, kQcDisney = 7, kQcSimple = 8;
+constexpr int kQcCount = 16;
 
 struct WfState {
     int64_t pool;
@@ -40,20 +57,22 @@ struct WfState {
     int64_t* item;        // global work item, or kNeedItem / kDone
     int32_t* k;           // sample within the item
     int32_t* view;
-    int32_t* flags;       // bit 0: continuation ray pending; bits 8..: depth
+    int32_t* flags;       // kNextCont | kPending | depth << 8
     uint64_t* rng;
     float4* beta;
     float4* col;
     float4* ro;
     float4* rd;
     float4* hit;
-    float4* acc;          // MIS + shadow contributions (atomic adds from the trace kernel)
+    float4* acc;          // MIS, shadow and emission contributions (atomic adds from the trace kernel)
     float4* isum;
     float4* icomp;
     float4* asum;
     float4* nsum;
     // queues
     int32_t* cont_q;
+    int32_t* disney_q;    // slots whose continuation ray hit a Disney surface
+    int32_t* simple_q;    // ... a Lambert, conductor or dielectric surface
     float4* mis_o;
     float4* mis_d;
     float4* mis_a;
@@ -61,10 +80,18 @@ struct WfState {
     float4* sh_d;
     float4* sh_c;
     int64_t cap_cont, cap_mis, cap_sh;
-    // counters: [0..2] queue sizes being written, [3..5] sizes being traced, [6] active slots
-    unsigned* qc;
+    unsigned* qc;         // kQc* counters
     Counters* cnt;
     uint32_t* status;
+    // adjoint renders only (null otherwise)
+    float4* lp;           // primal radiance of the slot's current sample
+    float4* dfr;          // [5 per slot] deferred continuation gradient: dlw[15] (c*5+i), material, u, v
+    float4* sh_g;         // [3 per shadow ray] g[5], u, v, material, env weight e[3], env score s
+    float4* mis_g;        // [8 per MIS ray] B[15] (c*5+i), material, u, v, e[3], a[5], b[5]
+    double* const* tex_grad;   // per scene texture: NULL or w*h*3
+    double* mat_grad;          // num_materials * 5, or NULL
+    double* env_row;           // env importance: per-row and global score sums (see scatter_env_score)
+    double* env_total;
 };
 
 FM_D unsigned lanemask_lt() { return (1u << (threadIdx.x & 31)) - 1u; }
@@ -102,31 +129,198 @@ FM_D int find_view(const WfState& st, int64_t item)
     return lo;
 }
 
-__global__ void k_wf_prep(WfState st)
+// ---- adjoint helpers -------------------------------------------------------------
+//
+// The adjoint renders each sample twice in the same slot: a primal pass that records
+// the path's radiance L, then a replay with the same random numbers.  Each term V of a
+// sample's radiance is a product of factors along the path, and the derivative of the
+// expected image is E[dV/dp + V d log q/dp] summed over the sampled directions, q the
+// density they were drawn with (sampled directions held fixed).  At a replayed vertex
+// k with throughput beta_k and BSDF f_k (parameters p = basecolor, metallic,
+// roughness of that vertex):
+//   NEE term c (if unshadowed): dc/dp = beta Le cos w_l / pdf_l df/dp
+//                                       + c (-2 (1 - w_l) dlog pdf_b/dp)     (MIS weight)
+//   MIS term c (if it hits an emitter): beta Le cos w_b / pdf_b df/dp
+//                                       + c (dlog q/dp - dlog pdf_b/dp + 2 (1 - w_b) dlog pdf_b/dp)
+//   continuation: (L - C_<=k) (df/dp / f + dlog q/dp - dlog pdf_b/dp)
+// pdf_b is the BSDF density the reference reports and q the sampler's true density
+// (they differ for the Disney reflection lobes; see fm_bsdf_grad.cuh); C_<=k is the
+// radiance collected up to and including vertex k.  The first two are scattered by the
+// trace kernel once visibility and the emitter are known; the third is deferred to the
+// next shaded vertex, where L - C_<=k is known.  Environment texels enter through Le
+// (bilinear taps) and through the light's sampling and reported densities (importance
+// tables normalised per row and over the whole map), handled by scatter_env and
+// scatter_env_score.  Every part is contracted with the pixel's dLoss/dI / spp before it
+// is scattered, so a payload holds one float per parameter (or per parameter and
+// channel while Le is still unknown).
+
+// dLoss/dI of the slot's pixel divided by spp (the image is a mean over samples).
+FM_D f3 pixel_delta(const WfState& st, int slot, const WfView& V)
 {
-    st.qc[3] = st.qc[0];
-    st.qc[4] = st.qc[1];
-    st.qc[5] = st.qc[2];
-    st.qc[0] = 0;
-    st.qc[1] = 0;
-    st.qc[2] = 0;
-    st.qc[6] = 0;
+    const int64_t local = st.item[slot] - V.item_base;
+    const int npix = V.cfg.width * V.cfg.height;
+    const int p = (int)(local % npix);
+    const float inv = 1.0f / (float)V.cfg.spp;
+    const float* d = V.drgb + 3 * (size_t)p;
+    return f3{__ldg(d) * inv, __ldg(d + 1) * inv, __ldg(d + 2) * inv};
 }
 
+// Adds g[c] * (weight of each tap) to channel c0 + c of the taps tex_sample reads.
+FM_D void tex_scatter(const DevTexture& t, double* grad, float u, float v, int c0, int nc, const float* g)
+{
+    const TexTaps tp = tex_taps(t, u, v);
+    for (int k = 0; k < tp.n; ++k) {
+        if (tp.w[k] == 0.0f) continue;
+        double* at = grad + 3 * ((size_t)tp.y[k] * t.w + tp.x[k]) + c0;
+        for (int c = 0; c < nc; ++c)
+            if (g[c] != 0.0f) atomicAdd(at + c, (double)(tp.w[k] * g[c]));
+    }
+}
+
+// Material whose parameters a vertex's gradient goes to, or -1 (no differentiable
+// parameters: conductor, dielectric, per-vertex attributes).
+FM_D int grad_target(const DevScene& S, const HitInfo& h)
+{
+    const DevMaterial& M = S.materials[h.mat];
+    if (M.vattr_offset >= 0) return -1;
+    return (M.type == 0 || M.type == 3) ? h.mat : -1;
+}
+
+// Scatters d/d{basecolor rgb, metallic, roughness} at (u, v) of material `mat` to the
+// textures those parameters read (basecolor: rgb; metallic: the third channel;
+// roughness: the second), or to the material's constants.
+FM_D void scatter_params(const WfState& st, const DevScene& S, int mat, float u, float v, const float* g)
+{
+    if (mat < 0) return;
+    const DevMaterial& M = S.materials[mat];
+    const int which[3] = {MP_BASECOLOR, MP_METALLIC, MP_ROUGHNESS};
+    const int first[3] = {0, 3, 4}, count[3] = {3, 1, 1}, chan[3] = {0, 2, 1};
+    for (int k = 0; k < 3; ++k) {
+        const float* gg = g + first[k];
+        bool any = false;
+        for (int c = 0; c < count[k]; ++c) any = any || gg[c] != 0.0f;
+        if (!any) continue;
+        const TexRef& r = M.p[which[k]];
+        if (r.tex >= 0) {
+            double* tg = st.tex_grad ? st.tex_grad[r.tex] : nullptr;
+            if (tg) tex_scatter(S.textures[r.tex], tg, u, v, chan[k], count[k], gg);
+        } else if (st.mat_grad) {
+            for (int c = 0; c < count[k]; ++c)
+                if (gg[c] != 0.0f) atomicAdd(st.mat_grad + (size_t)mat * kGradParams + first[k] + c, (double)gg[c]);
+        }
+    }
+}
+
+// Scatters e (per channel, before the env factor) to the env texels seen along `dir`.
+FM_D void scatter_env(const WfState& st, const DevScene& S, f3 dir, f3 e)
+{
+    if (!st.tex_grad || S.env_light < 0) return;
+    const DevEnv& E = S.env;
+    double* tg = st.tex_grad[E.tex];
+    if (!tg) return;
+    float u, v, th;
+    spherical_uv(xf_vec(E.w2l, dir), u, v, th);
+    const float g[3] = {e.x * E.factor, e.y * E.factor, e.z * E.factor};
+    tex_scatter(S.textures[E.tex], tg, u, v, 0, 3, g);
+}
+
+// Texel (i, j) of the env map that holds direction `dir` and its luminance (the cell
+// EnvLight::Pdf reads).
+FM_D bool env_texel(const DevScene& S, f3 dir, int& i, int& j, float& lumt)
+{
+    const DevEnv& E = S.env;
+    float u, v, th;
+    spherical_uv(xf_vec(E.w2l, dir), u, v, th);
+    i = (int)(u * (float)E.w);
+    j = (int)(v * (float)E.h);
+    i = i < 0 ? 0 : (i > E.w - 1 ? E.w - 1 : i);
+    j = j < 0 ? 0 : (j > E.h - 1 ? E.h - 1 : j);
+    const float4 t = __ldg(S.textures[E.tex].texels + (size_t)j * E.w + i);
+    lumt = luminance(f3{t.x, t.y, t.z});
+    return lumt > 0.0f;
+}
+
+// s * d log(density)/d texels for the env light's densities at `dir`: the sampled
+// texel's own term (d log lum = L_c / lum) here; the normalisation terms are summed
+// into env_row[j] (reported density: divided by the row sum) or env_total (sampling
+// density: divided by the map's sum) and spread over the texels after the render.
+FM_D void scatter_env_score(const WfState& st, const DevScene& S, f3 dir, float s, bool per_row)
+{
+    if (s == 0.0f || !st.tex_grad || S.env_light < 0) return;
+    double* tg = st.tex_grad[S.env.tex];
+    if (!tg) return;
+    int i, j;
+    float lumt;
+    if (!env_texel(S, dir, i, j, lumt)) return;
+    double* at = tg + 3 * ((size_t)j * S.env.w + i);
+    const float k = s / lumt;
+    atomicAdd(at, (double)(0.2126f * k));
+    atomicAdd(at + 1, (double)(0.7152f * k));
+    atomicAdd(at + 2, (double)(0.0722f * k));
+    atomicAdd(per_row ? st.env_row + j : st.env_total, (double)s);
+}
+
+__global__ void k_wf_prep(WfState st)
+{
+    st.qc[kQcTraceCont] = st.qc[kQcCont];
+    st.qc[kQcTraceMis] = st.qc[kQcMis];
+    st.qc[kQcTraceShadow] = st.qc[kQcShadow];
+    st.qc[kQcCont] = 0;
+    st.qc[kQcMis] = 0;
+    st.qc[kQcShadow] = 0;
+    st.qc[kQcActive] = 0;
+    st.qc[kQcDisney] = 0;
+    st.qc[kQcSimple] = 0;
+}
+
+template <bool ADJ>
 __global__ void __launch_bounds__(256) k_wf_trace(WfState st)
 {
-    const int64_t nc = st.qc[3], nm = st.qc[4], ns = st.qc[5];
+    const int64_t nc = st.qc[kQcTraceCont], nm = st.qc[kQcTraceMis], ns = st.qc[kQcTraceShadow];
     const int64_t total = nc + nm + ns;
     unsigned long long n_closest = 0, n_shadow = 0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < total; i0 += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = i0 + threadIdx.x;
+        // continuation rays: trace, then route the slot to the shading queue of the hit's
+        // material class; a miss or a first-bounce emitter hit ends the path here
+        int cls = -1;
+        int cslot = 0;
         if (i < nc) {
-            const int slot = st.cont_q[i];
-            const DevScene& S = *st.views[st.view[slot]].scene;
-            const float4 o = st.ro[slot], d = st.rd[slot];
+            cslot = st.cont_q[i];
+            const WfView& V = st.views[st.view[cslot]];
+            const DevScene& S = *V.scene;
+            const float4 o4 = st.ro[cslot], d4 = st.rd[cslot];
+            const f3 o = f3{o4.x, o4.y, o4.z}, d = f3{d4.x, d4.y, d4.z};
+            const int cflags = st.flags[cslot];
+            const int depth = cflags >> 8;
             Hit h;
-            trace_ray<false>(S, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, 0.0f, kRealMax, h, st.status);
-            st.hit[slot] = make_float4(h.t, __int_as_float(h.prim), h.b1, h.b2);
+            const bool hit = trace_ray<false>(S, o, d, 0.0f, kRealMax, h, st.status);
             ++n_closest;
+            if (!hit) {
+                // the camera ray's beta is 1
+                if (depth == 1 && S.env_light >= 0) {
+                    acc_add(&st.acc[cslot], env_radiance(S, d));
+                    if (ADJ && (cflags & kReplay)) scatter_env(st, S, d, pixel_delta(st, cslot, V));
+                }
+            } else {
+                const int obj = __ldg(S.prim_obj + h.prim);
+                const int li = depth == 1 ? __ldg(S.obj_light + obj) : -1;
+                if (li >= 0) {
+                    const HitInfo lh = make_hit(S, o, d, h);
+                    if (dot(lh.ng, lh.wo) > 0) acc_add(&st.acc[cslot], ld3(S.lights[li].radiance));
+                } else {
+                    st.hit[cslot] = make_float4(h.t, __int_as_float(h.prim), h.b1, h.b2);
+                    cls = material_class(S.materials[__ldg(S.obj_material + obj)].type);
+                }
+            }
+        }
+        {
+            const int64_t qd = wagg_append(&st.qc[kQcDisney], cls == kClsDisney);
+            if (cls == kClsDisney) st.disney_q[qd] = cslot;
+            const int64_t qs = wagg_append(&st.qc[kQcSimple], cls == kClsSimple);
+            if (cls == kClsSimple) st.simple_q[qs] = cslot;
+        }
+        if (i >= total || i < nc) {
         } else if (i < nc + nm) {
             const int64_t q = i - nc;
             const float4 o4 = st.mis_o[q], d4 = st.mis_d[q], a4 = st.mis_a[q];
@@ -136,11 +330,18 @@ __global__ void __launch_bounds__(256) k_wf_trace(WfState st)
             const float pdf = d4.w;   // < 0: delta BSDF sample (no MIS weight)
             Hit h;
             ++n_closest;
-            f3 c = mk(0.0f);
+            f3 c = mk(0.0f), Le = mk(0.0f);
+            float w = 1.0f;
+            bool env_hit = false;
             if (!trace_ray<false>(S, o, d, 0.0f, kRealMax, h, st.status)) {
                 if (S.env_light >= 0) {
-                    c = A * env_radiance(S, d);
-                    if (pdf >= 0.0f) c *= power_heuristic(pdf, env_pdf(S, d));
+                    Le = env_radiance(S, d);
+                    c = A * Le;
+                    if (pdf >= 0.0f) {
+                        w = power_heuristic(pdf, env_pdf(S, d));
+                        c *= w;
+                    }
+                    env_hit = true;
                 }
             } else {
                 const int obj = __ldg(S.prim_obj + h.prim);
@@ -151,12 +352,45 @@ __global__ void __launch_bounds__(256) k_wf_trace(WfState st)
                     const DevLight& L = S.lights[li];
                     const f3 rad = dot(lh.ng, l2s) > 0 ? ld3(L.radiance) : mk(0.0f);
                     if (length(rad) >= kEpsPdf) {
+                        Le = rad;
                         c = A * rad;
-                        if (pdf >= 0.0f) c *= power_heuristic(pdf, area_light_pdf(S, L, o, lh.pos, lh.ng, l2s));
+                        if (pdf >= 0.0f) {
+                            w = power_heuristic(pdf, area_light_pdf(S, L, o, lh.pos, lh.ng, l2s));
+                            c *= w;
+                        }
                     }
                 }
             }
-            if (c.x != 0.0f || c.y != 0.0f || c.z != 0.0f) acc_add(&st.acc[slot], c);
+            if (c.x != 0.0f || c.y != 0.0f || c.z != 0.0f) {
+                acc_add(&st.acc[slot], c);
+                if (ADJ) {
+                    const float4* P = st.mis_g + 8 * q;
+                    const float4 p3 = P[3], p4 = P[4], p5 = P[5];
+                    const int mat = __float_as_int(p3.w);
+                    const f3 e = f3{p4.z, p4.w, p5.x};
+                    // sum_c dLoss/dc_c * c_c (e = dLoss/dI * A, c = A Le w)
+                    const float ec = e.x * Le.x * w + e.y * Le.y * w + e.z * Le.z * w;
+                    if (mat >= 0) {
+                        const float4 p0 = P[0], p1 = P[1], p2 = P[2], p6 = P[6], p7 = P[7];
+                        const float B[15] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w,
+                                             p2.x, p2.y, p2.z, p2.w, p3.x, p3.y, p3.z};
+                        const float a[kGradParams] = {p5.y, p5.z, p5.w, p6.x, p6.y};
+                        const float b[kGradParams] = {p6.z, p6.w, p7.x, p7.y, p7.z};
+                        const f3 u3 = Le * w;
+                        const float wl = pdf >= 0.0f ? 1.0f - w : 0.0f;
+                        float g[kGradParams];
+                        for (int i = 0; i < kGradParams; ++i)
+                            g[i] = u3.x * B[i] + u3.y * B[5 + i] + u3.z * B[10 + i] + ec * (a[i] + wl * b[i]);
+                        scatter_params(st, S, mat, p4.x, p4.y, g);
+                    }
+                    if (env_hit && (e.x != 0.0f || e.y != 0.0f || e.z != 0.0f)) {
+                        scatter_env(st, S, d, e * w);
+                        // MIS weight w_b = pdf_b^2 / (pdf_b^2 + pdf_env^2), pdf_env the
+                        // reported (per-row normalised) density
+                        if (pdf >= 0.0f) scatter_env_score(st, S, d, -2.0f * (1.0f - w) * ec, true);
+                    }
+                }
+            }
         } else {
             const int64_t q = i - nc - nm;
             const float4 o4 = st.sh_o[q], d4 = st.sh_d[q], c4 = st.sh_c[q];
@@ -164,8 +398,26 @@ __global__ void __launch_bounds__(256) k_wf_trace(WfState st)
             const DevScene& S = *st.views[__float_as_int(c4.w)].scene;
             Hit h;
             ++n_shadow;
-            if (!trace_ray<true>(S, f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, kEps, o4.w, h, st.status))
+            if (!trace_ray<true>(S, f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, kEps, o4.w, h, st.status)) {
                 acc_add(&st.acc[slot], f3{c4.x, c4.y, c4.z});
+                if (ADJ) {
+                    const float4* P = st.sh_g + 3 * q;
+                    const float4 p1 = P[1], p2 = P[2];
+                    const int mat = __float_as_int(p1.w);
+                    if (mat >= 0) {
+                        const float4 p0 = P[0];
+                        const float g[kGradParams] = {p0.x, p0.y, p0.z, p0.w, p1.x};
+                        scatter_params(st, S, mat, p1.y, p1.z, g);
+                    }
+                    if (p2.x != 0.0f || p2.y != 0.0f || p2.z != 0.0f) {
+                        const f3 dir = f3{d4.x, d4.y, d4.z};
+                        scatter_env(st, S, dir, f3{p2.x, p2.y, p2.z});
+                        // env NEE: 1 / pdf_sample, its MIS weight and the score of the
+                        // sampling density leave 2 (1 - w_l) d log pdf_sample
+                        scatter_env_score(st, S, dir, p2.w, false);
+                    }
+                }
+            }
         }
     }
     // per-warp counter aggregation
@@ -198,7 +450,7 @@ FM_D int item_samples(const WfView& V, int chunk_index)
 }
 
 // Start sample `k` of the slot's item: camera ray into the slot registers, enqueue it.
-FM_D void start_sample(const WfState& st, int slot, const WfView& V, int64_t item_local, int k)
+FM_D void start_sample(const WfState& st, int slot, const WfView& V, int64_t item_local, int k, int extra_flags = 0)
 {
     const int npix = V.cfg.width * V.cfg.height;
     const int c = (int)(item_local / npix);
@@ -218,12 +470,258 @@ FM_D void start_sample(const WfState& st, int slot, const WfView& V, int64_t ite
     st.rng[slot] = rng.state;
     st.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     st.col[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    st.flags[slot] = kHasCont | (1 << 8);
+    st.flags[slot] = (1 << 8) | extra_flags;
+    // a replay starts with no deferred continuation gradient
+    if (extra_flags & kReplay) st.dfr[5 * (size_t)slot + 3] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
 }
 
+// Shading of the slots whose continuation ray hit a surface of material class CLS (the
+// trace kernel queued them): AOVs at the first bounce, next-event estimation (shadow
+// rays), the MIS BSDF samples (MIS rays) and the continuation sample with Russian
+// roulette.  Sets kNextCont / kPending so that the logic kernel keeps the slot's
+// sample open.  Each class runs its own kernel, so a warp holds one kind of BSDF and
+// the kernel's code holds only that kind's lobes.
+template <int CLS, bool ADJ>
 __global__ void __launch_bounds__(256) k_wf_shade(WfState st)
 {
-    unsigned long long n_paths = 0, n_bounces = 0, n_nans = 0;
+    const int64_t n = st.qc[CLS == kClsDisney ? kQcDisney : kQcSimple];
+    const int32_t* queue = CLS == kClsDisney ? st.disney_q : st.simple_q;
+    unsigned long long n_bounces = 0;
+    for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = i0 + threadIdx.x;
+        const bool valid = i < n;
+        const int slot = valid ? queue[i] : 0;
+        bool enqueue_cont = false;
+        if (valid) {
+            ++n_bounces;
+            const int vid = st.view[slot];
+            const WfView& V = st.views[vid];
+            const DevScene& S = *V.scene;
+            const int flags0 = st.flags[slot];
+            const int depth = flags0 >> 8;
+            const bool replay = ADJ && (flags0 & kReplay);
+            int flags = (depth << 8) | (flags0 & kReplay);
+            const float4 h4 = st.hit[slot];
+            const float4 o4 = st.ro[slot], d4 = st.rd[slot];
+            const f3 o = f3{o4.x, o4.y, o4.z}, d = f3{d4.x, d4.y, d4.z};
+            const float4 b4 = st.beta[slot];
+            f3 beta = f3{b4.x, b4.y, b4.z};
+            Hit hit;
+            hit.t = h4.x;
+            hit.prim = __float_as_int(h4.y);
+            hit.b1 = h4.z;
+            hit.b2 = h4.w;
+            const HitInfo h = make_hit(S, o, d, hit);
+            Rng rng;
+            rng.state = st.rng[slot];
+            const Bsdf b = make_bsdf<CLS>(S, h);
+            f3 delta = mk(0.0f);
+            int tgt = -1;
+            if (ADJ && replay) {
+                delta = pixel_delta(st, slot, V);
+                tgt = grad_target(S, h);
+                // the previous vertex's continuation gradient: L - C_<=k-1 is known now
+                const float4* D = st.dfr + 5 * (size_t)slot;
+                const float4 d3 = D[3];
+                const int dmat = __float_as_int(d3.w);
+                if (dmat >= 0) {
+                    const float4 a4 = st.acc[slot], c4 = st.col[slot], l4 = st.lp[slot];
+                    const f3 R = f3{l4.x - (c4.x + a4.x), l4.y - (c4.y + a4.y), l4.z - (c4.z + a4.z)};
+                    const f3 wr = delta * R;
+                    const float4 d0 = D[0], d1 = D[1], d2 = D[2], d4 = D[4];
+                    const float dl[15] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w,
+                                          d2.x, d2.y, d2.z, d2.w, d3.x, d3.y, d3.z};
+                    float g[kGradParams];
+                    for (int i = 0; i < kGradParams; ++i) g[i] = wr.x * dl[i] + wr.y * dl[5 + i] + wr.z * dl[10 + i];
+                    scatter_params(st, S, dmat, d4.x, d4.y, g);
+                }
+            }
+            if (depth == 1 && !replay) {
+                const f3 al = bsdf_albedo(b);
+                float4 as = st.asum[slot], ns = st.nsum[slot];
+                as.x += al.x; as.y += al.y; as.z += al.z;
+                ns.x += h.ng.x; ns.y += h.ng.y; ns.z += h.ng.z;
+                st.asum[slot] = as;
+                st.nsum[slot] = ns;
+            }
+            const float inv_dl = 1.0f / (float)V.cfg.direct_loop;
+            for (int kk = 0; kk < V.cfg.direct_loop; ++kk) {
+                for (int l = 0; l < S.num_lights; ++l) {
+                    const DevLight& L = S.lights[l];
+                    LightSample ls;
+                    bool ok = light_sample(S, L, h.pos, rng_3d(rng), ls);
+                    ok = ok && ls.pdf >= kEpsPdf && length(ls.radiance) >= kEpsPdf;
+                    f3 f = mk(0.0f);
+                    float pb = 0.0f;
+                    if (ok) {
+                        f = bsdf_f<CLS>(b, h.wo, ls.wi);
+                        ok = length(f) >= kEpsPdf;
+                    }
+                    if (ok) {
+                        pb = bsdf_pdf<CLS>(b, h.wo, ls.wi);
+                        ok = pb >= kEpsPdf;
+                    }
+                    const int64_t q = wagg_append(&st.qc[kQcShadow], ok);
+                    if (ok) {
+                        f3 c = beta * (f * ls.radiance * absdot(ls.wi, h.ng)) / ls.pdf;
+                        if (!ls.delta) c *= power_heuristic(ls.pdf, pb);
+                        c *= inv_dl;
+                        if (q < st.cap_sh) {
+                            st.sh_o[q] = make_float4(h.pos.x, h.pos.y, h.pos.z, ls.dist - kEps);
+                            st.sh_d[q] = make_float4(ls.wi.x, ls.wi.y, ls.wi.z, __int_as_float(slot));
+                            st.sh_c[q] = make_float4(c.x, c.y, c.z, __int_as_float(vid));
+                            if (ADJ) {
+                                float4* P = st.sh_g + 3 * q;
+                                if (replay) {
+                                    const float mis = ls.delta ? 1.0f : power_heuristic(ls.pdf, pb);
+                                    const f3 base = beta * (absdot(ls.wi, h.ng) / ls.pdf * mis * inv_dl);
+                                    const float dc = dot(delta, c);   // sum_c dLoss/dc_c * c_c
+                                    float g[kGradParams] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+                                    if (tgt >= 0) {
+                                        contract(bsdf_f_grad<CLS>(b, h.wo, ls.wi), delta * base * ls.radiance, g);
+                                        if (!ls.delta) {
+                                            float dlogp[kGradParams], dscore[kGradParams];
+                                            pdf_log_derivs<CLS>(b, h.wo, ls.wi, dlogp, dscore);
+                                            for (int i = 0; i < kGradParams; ++i) g[i] -= 2.0f * (1.0f - mis) * dc * dlogp[i];
+                                        }
+                                    }
+                                    const bool env = L.kind == LK_ENV;
+                                    const f3 e = env ? delta * base * f : mk(0.0f);
+                                    const float senv = env ? 2.0f * (1.0f - mis) * dc : 0.0f;
+                                    P[0] = make_float4(g[0], g[1], g[2], g[3]);
+                                    P[1] = make_float4(g[4], h.u, h.v, __int_as_float(tgt));
+                                    P[2] = make_float4(e.x, e.y, e.z, senv);
+                                } else {
+                                    P[1] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+                                    P[2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                                }
+                            }
+                            flags |= kPending;
+                        } else {
+                            atomicOr(st.status, 2u);
+                        }
+                    }
+                }
+                const BsdfSample ms = bsdf_sample<CLS>(b, h.wo, rng_3d(rng));
+                const bool ok = length(ms.f) >= kEpsPdf && ms.pdf >= kEpsPdf;
+                const int64_t q = wagg_append(&st.qc[kQcMis], ok);
+                if (ok) {
+                    const f3 wi = normalize(ms.wi);
+                    const f3 ro = spawn_origin(h, wi);
+                    const f3 A = beta * ms.f * absdot(h.ng, wi) / ms.pdf * inv_dl;
+                    if (q < st.cap_mis) {
+                        st.mis_o[q] = make_float4(ro.x, ro.y, ro.z, __int_as_float(slot));
+                        st.mis_d[q] = make_float4(wi.x, wi.y, wi.z, ms.delta ? -1.0f : ms.pdf);
+                        st.mis_a[q] = make_float4(A.x, A.y, A.z, __int_as_float(vid));
+                        if (ADJ) {
+                            float4* P = st.mis_g + 8 * q;
+                            if (replay) {
+                                float B[15], a[kGradParams], bb[kGradParams];
+                                for (int k = 0; k < 15; ++k) B[k] = 0.0f;
+                                for (int k = 0; k < kGradParams; ++k) a[k] = bb[k] = 0.0f;
+                                if (tgt >= 0) {
+                                    const DV3 fd = bsdf_f_grad<CLS>(b, h.wo, ms.wi);
+                                    const f3 base = delta * beta * (absdot(h.ng, wi) / ms.pdf * inv_dl);
+                                    for (int i = 0; i < kGradParams; ++i) {
+                                        B[i] = base.x * fd.x.d[i];
+                                        B[5 + i] = base.y * fd.y.d[i];
+                                        B[10 + i] = base.z * fd.z.d[i];
+                                    }
+                                    if (!ms.delta) {
+                                        float dlogp[kGradParams];
+                                        pdf_log_derivs<CLS>(b, h.wo, ms.wi, dlogp, a);
+                                        for (int i = 0; i < kGradParams; ++i) bb[i] = 2.0f * dlogp[i];
+                                    }
+                                }
+                                const f3 e = delta * A;
+                                P[0] = make_float4(B[0], B[1], B[2], B[3]);
+                                P[1] = make_float4(B[4], B[5], B[6], B[7]);
+                                P[2] = make_float4(B[8], B[9], B[10], B[11]);
+                                P[3] = make_float4(B[12], B[13], B[14], __int_as_float(tgt));
+                                P[4] = make_float4(h.u, h.v, e.x, e.y);
+                                P[5] = make_float4(e.z, a[0], a[1], a[2]);
+                                P[6] = make_float4(a[3], a[4], bb[0], bb[1]);
+                                P[7] = make_float4(bb[2], bb[3], bb[4], 0.0f);
+                            } else {
+                                P[3] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+                                P[4] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                                P[5] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                            }
+                        }
+                        flags |= kPending;
+                    } else {
+                        atomicOr(st.status, 2u);
+                    }
+                }
+            }
+            const BsdfSample sc = bsdf_sample<CLS>(b, h.wo, rng_3d(rng));
+            if (length(sc.f) >= kEpsPdf && sc.pdf >= kEpsPdf) {
+                beta *= sc.f * absdot(h.ng, sc.wi) / sc.pdf;
+                if (depth < V.cfg.depth) {
+                    bool go = true;
+                    if (V.cfg.rr_enabled) {
+                        if (rng_1d(rng) > V.cfg.rr_coef)
+                            go = false;
+                        else
+                            beta /= V.cfg.rr_coef;
+                    }
+                    if (go) {
+                        const f3 no = spawn_origin(h, sc.wi);
+                        st.ro[slot] = make_float4(no.x, no.y, no.z, 0.0f);
+                        st.rd[slot] = make_float4(sc.wi.x, sc.wi.y, sc.wi.z, 0.0f);
+                        st.beta[slot] = make_float4(beta.x, beta.y, beta.z, 0.0f);
+                        flags = kNextCont | (flags & (kPending | kReplay)) | ((depth + 1) << 8);
+                        enqueue_cont = true;
+                        if (ADJ && replay) {
+                            // d log f / dp at the continuation direction, consumed at the
+                            // next shaded vertex
+                            float4* D = st.dfr + 5 * (size_t)slot;
+                            if (tgt >= 0) {
+                                const DV3 fd = bsdf_f_grad<CLS>(b, h.wo, sc.wi);
+                                float dlogp[kGradParams], dscore[kGradParams];
+                                pdf_log_derivs<CLS>(b, h.wo, sc.wi, dlogp, dscore);
+                                float dl[15];
+                                for (int i = 0; i < kGradParams; ++i) {
+                                    dl[i] = fd.x.v > 0.0f ? fd.x.d[i] / fd.x.v + dscore[i] : 0.0f;
+                                    dl[5 + i] = fd.y.v > 0.0f ? fd.y.d[i] / fd.y.v + dscore[i] : 0.0f;
+                                    dl[10 + i] = fd.z.v > 0.0f ? fd.z.d[i] / fd.z.v + dscore[i] : 0.0f;
+                                }
+                                D[0] = make_float4(dl[0], dl[1], dl[2], dl[3]);
+                                D[1] = make_float4(dl[4], dl[5], dl[6], dl[7]);
+                                D[2] = make_float4(dl[8], dl[9], dl[10], dl[11]);
+                                D[3] = make_float4(dl[12], dl[13], dl[14], __int_as_float(tgt));
+                                D[4] = make_float4(h.u, h.v, 0.0f, 0.0f);
+                            } else {
+                                D[3] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+                            }
+                        }
+                    }
+                }
+            }
+            st.rng[slot] = rng.state;
+            st.flags[slot] = flags;
+        }
+        const int64_t q = wagg_append(&st.qc[kQcCont], enqueue_cont);
+        if (enqueue_cont) {
+            if (q < st.cap_cont)
+                st.cont_q[q] = slot;
+            else
+                atomicOr(st.status, 2u);
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) n_bounces += __shfl_xor_sync(0xffffffffu, n_bounces, off);
+    if ((threadIdx.x & 31) == 0 && n_bounces) atomicAdd(&st.cnt->bounces, n_bounces);
+}
+
+// Per slot, after the shading kernels: fold the contributions the trace kernel added
+// (shadow and MIS rays of the previous bounce, emission seen by the continuation ray)
+// into the sample's color; a sample with neither a continuation ray nor rays in flight
+// is finished: it goes into the item's Kahan sum and the slot starts its next sample,
+// or takes a new work item.
+template <bool ADJ>
+__global__ void __launch_bounds__(256) k_wf_logic(WfState st)
+{
+    unsigned long long n_paths = 0, n_nans = 0;
     unsigned n_active = 0;
     for (int64_t s0 = blockIdx.x * (int64_t)blockDim.x; s0 < st.pool; s0 += (int64_t)gridDim.x * blockDim.x) {
         const int64_t s64 = s0 + threadIdx.x;
@@ -232,130 +730,35 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfState st)
         int64_t item = in_range ? st.item[slot] : (int64_t)kDone;
         bool need_new = item == kNeedItem;
         bool enqueue_cont = false;
+        bool alive = false;
         if (item >= 0) {
-            const int vid = st.view[slot];
-            const WfView& V = st.views[vid];
-            const DevScene& S = *V.scene;
             const float4 a4 = st.acc[slot];
             const float4 c4 = st.col[slot];
-            f3 col = f3{c4.x + a4.x, c4.y + a4.y, c4.z + a4.z};
-            st.acc[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            int flags = st.flags[slot];
-            bool pending = false;
-            if (flags & kHasCont) {
-                const int depth = flags >> 8;
-                flags = 0;
-                const float4 h4 = st.hit[slot];
-                const float4 o4 = st.ro[slot], d4 = st.rd[slot];
-                const f3 o = f3{o4.x, o4.y, o4.z}, d = f3{d4.x, d4.y, d4.z};
-                const float4 b4 = st.beta[slot];
-                f3 beta = f3{b4.x, b4.y, b4.z};
-                Hit hit;
-                hit.t = h4.x;
-                hit.prim = __float_as_int(h4.y);
-                hit.b1 = h4.z;
-                hit.b2 = h4.w;
-                if (hit.prim < 0) {
-                    if (depth == 1 && S.env_light >= 0) col = env_radiance(S, d);
-                } else {
-                    const HitInfo h = make_hit(S, o, d, hit);
-                    const int li = depth == 1 ? __ldg(S.obj_light + h.obj) : -1;
-                    if (li >= 0) {
-                        const f3 rad = dot(h.ng, h.wo) > 0 ? ld3(S.lights[li].radiance) : mk(0.0f);
-                        col += beta * rad;
-                    } else {
-                        ++n_bounces;
-                        Rng rng;
-                        rng.state = st.rng[slot];
-                        const Bsdf b = make_bsdf(S, h);
-                        if (depth == 1) {
-                            const f3 al = bsdf_albedo(b);
-                            float4 as = st.asum[slot], ns = st.nsum[slot];
-                            as.x += al.x; as.y += al.y; as.z += al.z;
-                            ns.x += h.ng.x; ns.y += h.ng.y; ns.z += h.ng.z;
-                            st.asum[slot] = as;
-                            st.nsum[slot] = ns;
-                        }
-                        const float inv_dl = 1.0f / (float)V.cfg.direct_loop;
-                        for (int kk = 0; kk < V.cfg.direct_loop; ++kk) {
-                            for (int l = 0; l < S.num_lights; ++l) {
-                                const DevLight& L = S.lights[l];
-                                LightSample ls;
-                                bool ok = light_sample(S, L, h.pos, rng_3d(rng), ls);
-                                ok = ok && ls.pdf >= kEpsPdf && length(ls.radiance) >= kEpsPdf;
-                                f3 f = mk(0.0f);
-                                float pb = 0.0f;
-                                if (ok) {
-                                    f = bsdf_f(b, h.wo, ls.wi);
-                                    ok = length(f) >= kEpsPdf;
-                                }
-                                if (ok) {
-                                    pb = bsdf_pdf(b, h.wo, ls.wi);
-                                    ok = pb >= kEpsPdf;
-                                }
-                                const int64_t q = wagg_append(&st.qc[2], ok);
-                                if (ok) {
-                                    f3 c = beta * (f * ls.radiance * absdot(ls.wi, h.ng)) / ls.pdf;
-                                    if (!ls.delta) c *= power_heuristic(ls.pdf, pb);
-                                    c *= inv_dl;
-                                    if (q < st.cap_sh) {
-                                        st.sh_o[q] = make_float4(h.pos.x, h.pos.y, h.pos.z, ls.dist - kEps);
-                                        st.sh_d[q] = make_float4(ls.wi.x, ls.wi.y, ls.wi.z, __int_as_float(slot));
-                                        st.sh_c[q] = make_float4(c.x, c.y, c.z, __int_as_float(vid));
-                                        pending = true;
-                                    } else {
-                                        atomicOr(st.status, 2u);
-                                    }
-                                }
-                            }
-                            const BsdfSample ms = bsdf_sample(b, h.wo, rng_3d(rng));
-                            const bool ok = length(ms.f) >= kEpsPdf && ms.pdf >= kEpsPdf;
-                            const int64_t q = wagg_append(&st.qc[1], ok);
-                            if (ok) {
-                                const f3 wi = normalize(ms.wi);
-                                const f3 ro = spawn_origin(h, wi);
-                                const f3 A = beta * ms.f * absdot(h.ng, wi) / ms.pdf * inv_dl;
-                                if (q < st.cap_mis) {
-                                    st.mis_o[q] = make_float4(ro.x, ro.y, ro.z, __int_as_float(slot));
-                                    st.mis_d[q] = make_float4(wi.x, wi.y, wi.z, ms.delta ? -1.0f : ms.pdf);
-                                    st.mis_a[q] = make_float4(A.x, A.y, A.z, __int_as_float(vid));
-                                    pending = true;
-                                } else {
-                                    atomicOr(st.status, 2u);
-                                }
-                            }
-                        }
-                        const BsdfSample sc = bsdf_sample(b, h.wo, rng_3d(rng));
-                        if (length(sc.f) >= kEpsPdf && sc.pdf >= kEpsPdf) {
-                            beta *= sc.f * absdot(h.ng, sc.wi) / sc.pdf;
-                            if (depth < V.cfg.depth) {
-                                bool go = true;
-                                if (V.cfg.rr_enabled) {
-                                    if (rng_1d(rng) > V.cfg.rr_coef)
-                                        go = false;
-                                    else
-                                        beta /= V.cfg.rr_coef;
-                                }
-                                if (go) {
-                                    const f3 no = spawn_origin(h, sc.wi);
-                                    st.ro[slot] = make_float4(no.x, no.y, no.z, 0.0f);
-                                    st.rd[slot] = make_float4(sc.wi.x, sc.wi.y, sc.wi.z, 0.0f);
-                                    st.beta[slot] = make_float4(beta.x, beta.y, beta.z, 0.0f);
-                                    flags = kHasCont | ((depth + 1) << 8);
-                                    enqueue_cont = true;
-                                }
-                            }
-                        }
-                        st.rng[slot] = rng.state;
-                    }
-                }
-            }
-            if (!enqueue_cont && !pending) {
-                // sample finished
+            const f3 col = f3{c4.x + a4.x, c4.y + a4.y, c4.z + a4.z};
+            if (a4.x != 0.0f || a4.y != 0.0f || a4.z != 0.0f) st.acc[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            const int flags = st.flags[slot];
+            if (flags & (kNextCont | kPending)) {
+                st.col[slot] = make_float4(col.x, col.y, col.z, 0.0f);
+                st.flags[slot] = flags & ~(kNextCont | kPending);
+                alive = true;
+            } else if (ADJ && !(flags & kReplay)) {
+                // primal pass of this sample done: keep L, add it to the image, replay
+                const int vid = st.view[slot];
+                const WfView& V = st.views[vid];
+                st.lp[slot] = make_float4(col.x, col.y, col.z, 0.0f);
+                float4 sum = st.isum[slot], cmp = st.icomp[slot];
+                kahan_add4(sum, cmp, col);
+                st.isum[slot] = sum;
+                st.icomp[slot] = cmp;
+                start_sample(st, slot, V, item - V.item_base, st.k[slot], kReplay);
+                enqueue_cont = true;
+            } else {
+                const int vid = st.view[slot];
+                const WfView& V = st.views[vid];
                 ++n_paths;
                 if (!isfinite(col.x) || !isfinite(col.y) || !isfinite(col.z)) ++n_nans;
                 float4 sum = st.isum[slot], cmp = st.icomp[slot];
-                kahan_add4(sum, cmp, col);
+                if (!ADJ) kahan_add4(sum, cmp, col);
                 const int kdone = st.k[slot] + 1;
                 const int64_t local = item - V.item_base;
                 const int npix = V.cfg.width * V.cfg.height;
@@ -373,9 +776,6 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfState st)
                     start_sample(st, slot, V, local, kdone);
                     enqueue_cont = true;
                 }
-            } else {
-                st.col[slot] = make_float4(col.x, col.y, col.z, 0.0f);
-                st.flags[slot] = flags;
             }
         }
         // new work items for slots that finished theirs (one atomic per warp)
@@ -401,35 +801,31 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfState st)
                     st.icomp[slot] = z;
                     st.asum[slot] = z;
                     st.nsum[slot] = z;
-                    st.acc[slot] = z;
                     start_sample(st, slot, V, it - V.item_base, 0);
                     enqueue_cont = true;
                 }
             }
         }
-        const int64_t q = wagg_append(&st.qc[0], enqueue_cont);
+        const int64_t q = wagg_append(&st.qc[kQcCont], enqueue_cont);
         if (enqueue_cont) {
             if (q < st.cap_cont)
                 st.cont_q[q] = slot;
             else
                 atomicOr(st.status, 2u);
-            ++n_active;
         }
-        if (in_range && !enqueue_cont && st.item[slot] >= 0) ++n_active;
+        if (enqueue_cont || alive) ++n_active;
     }
     for (int off = 16; off > 0; off >>= 1) {
         n_paths += __shfl_xor_sync(0xffffffffu, n_paths, off);
-        n_bounces += __shfl_xor_sync(0xffffffffu, n_bounces, off);
         n_nans += __shfl_xor_sync(0xffffffffu, n_nans, off);
         n_active += __shfl_xor_sync(0xffffffffu, n_active, off);
     }
     if ((threadIdx.x & 31) == 0) {
-        if (n_paths | n_bounces | n_nans) {
+        if (n_paths | n_nans) {
             atomicAdd(&st.cnt->paths, n_paths);
-            atomicAdd(&st.cnt->bounces, n_bounces);
             atomicAdd(&st.cnt->nans, n_nans);
         }
-        if (n_active) atomicAdd(&st.qc[6], n_active);
+        if (n_active) atomicAdd(&st.qc[kQcActive], n_active);
     }
 }
 
@@ -439,6 +835,7 @@ __global__ void k_wf_init(WfState st)
         st.item[s] = kNeedItem;
         st.flags[s] = 0;
         st.acc[s] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        st.col[s] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
 }
 
@@ -465,8 +862,11 @@ __global__ void k_wf_reduce(WfView V)
 
 }  // namespace
 
-fm_status wavefront_views(fm_ctx* ctx, const std::vector<WfView>& views_in, const WfTuning& tune, Counters* cnt,
-                          WfTimes* times)
+namespace {
+
+template <bool ADJ>
+fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const WfTuning& tune, const WfAdjoint* adj,
+                        Counters* cnt, WfTimes* times)
 {
     cudaStream_t s = ctx->stream;
     std::vector<WfView> views = views_in;
@@ -541,13 +941,25 @@ fm_status wavefront_views(fm_ctx* ctx, const std::vector<WfView>& views_in, cons
     A(st.asum, pool);
     A(st.nsum, pool);
     A(st.cont_q, st.cap_cont);
+    A(st.disney_q, pool);
+    A(st.simple_q, pool);
     A(st.mis_o, st.cap_mis);
     A(st.mis_d, st.cap_mis);
     A(st.mis_a, st.cap_mis);
     A(st.sh_o, st.cap_sh);
     A(st.sh_d, st.cap_sh);
     A(st.sh_c, st.cap_sh);
-    A(st.qc, 8);
+    A(st.qc, kQcCount);
+    if (ADJ) {
+        A(st.lp, pool);
+        A(st.dfr, 5 * (size_t)pool);
+        A(st.sh_g, 3 * (size_t)st.cap_sh);
+        A(st.mis_g, 8 * (size_t)st.cap_mis);
+        st.tex_grad = adj->tex_grad;
+        st.mat_grad = adj->mat_grad;
+        st.env_row = adj->env_row;
+        st.env_total = adj->env_total;
+    }
     if (!ok) {
         free_all();
         return set_error(ctx, FM_ERR_OOM, "wavefront: state allocation failed");
@@ -558,16 +970,18 @@ fm_status wavefront_views(fm_ctx* ctx, const std::vector<WfView>& views_in, cons
     FM_CUDA_TRY(ctx, cudaMemcpyAsync(d_views, views.data(), sizeof(WfView) * views.size(), cudaMemcpyHostToDevice, s),
                 "wavefront views");
     FM_CUDA_TRY(ctx, cudaMemsetAsync(st.next_item, 0, sizeof(unsigned long long), s), "wavefront");
-    FM_CUDA_TRY(ctx, cudaMemsetAsync(st.qc, 0, sizeof(unsigned) * 8, s), "wavefront");
+    FM_CUDA_TRY(ctx, cudaMemsetAsync(st.qc, 0, sizeof(unsigned) * kQcCount, s), "wavefront");
     const int sms = ctx->num_sms;
     k_wf_init<<<sms * 8, 256, 0, s>>>(st);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, s);
-    // one graph = `iters_per_graph` iterations of prep -> trace -> shade
+    // one graph = `iters_per_graph` iterations of prep -> trace -> shade (Disney) ->
+    // shade (other materials) -> logic
     const int trace_grid = sms * 16;
     const int shade_grid = (int)std::min<int64_t>((pool + tune.shade_block - 1) / tune.shade_block, (int64_t)sms * 32);
+    const int logic_grid = (int)std::min<int64_t>((pool + 255) / 256, (int64_t)sms * 32);
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     fm_status result = FM_OK;
@@ -583,9 +997,11 @@ fm_status wavefront_views(fm_ctx* ctx, const std::vector<WfView>& views_in, cons
         for (int it = 0; it < tune.iters_per_graph; ++it) {
             k_wf_prep<<<1, 1, 0, s>>>(st);
             if (tune.profile) cudaEventRecordWithFlags(pev[3 * it], s, cudaEventRecordExternal);
-            k_wf_trace<<<trace_grid, tune.trace_block, 0, s>>>(st);
+            k_wf_trace<ADJ><<<trace_grid, tune.trace_block, 0, s>>>(st);
             if (tune.profile) cudaEventRecordWithFlags(pev[3 * it + 1], s, cudaEventRecordExternal);
-            k_wf_shade<<<shade_grid, tune.shade_block, 0, s>>>(st);
+            k_wf_shade<kClsDisney, ADJ><<<shade_grid, tune.shade_block, 0, s>>>(st);
+            k_wf_shade<kClsSimple, ADJ><<<shade_grid, tune.shade_block, 0, s>>>(st);
+            k_wf_logic<ADJ><<<logic_grid, 256, 0, s>>>(st);
             if (tune.profile) cudaEventRecordWithFlags(pev[3 * it + 2], s, cudaEventRecordExternal);
         }
         e = cudaStreamEndCapture(s, &graph);
@@ -598,7 +1014,7 @@ fm_status wavefront_views(fm_ctx* ctx, const std::vector<WfView>& views_in, cons
         return cuda_error(ctx, e, "wavefront graph");
     }
     unsigned* h_qc = nullptr;
-    cudaMallocHost(&h_qc, sizeof(unsigned) * 8);
+    cudaMallocHost(&h_qc, sizeof(unsigned) * kQcCount);
     // Bound on graph launches: every sample takes at most depth + 1 iterations and a slot
     // runs its samples one after another.
     int max_depth = 1, max_chunk = 1;
@@ -606,14 +1022,15 @@ fm_status wavefront_views(fm_ctx* ctx, const std::vector<WfView>& views_in, cons
         max_depth = std::max(max_depth, v.cfg.depth);
         max_chunk = std::max(max_chunk, v.chunk);
     }
-    const double iter_bound = (total_samples / (double)pool + 4.0 * max_chunk + 8.0) * (max_depth + 2) * 4.0 + 1000.0;
+    const double iter_bound =
+        (total_samples / (double)pool + 4.0 * max_chunk + 8.0) * (max_depth + 2) * 4.0 * (ADJ ? 2.0 : 1.0) + 1000.0;
     const int64_t max_launches = (int64_t)(iter_bound / tune.iters_per_graph) + 16;
     int64_t guard = 0, graph_launches = 0;
     for (;;) {
         e = cudaGraphLaunch(exec, s);
         if (e != cudaSuccess) break;
         ++graph_launches;
-        e = cudaMemcpyAsync(h_qc, st.qc, sizeof(unsigned) * 8, cudaMemcpyDeviceToHost, s);
+        e = cudaMemcpyAsync(h_qc, st.qc, sizeof(unsigned) * kQcCount, cudaMemcpyDeviceToHost, s);
         if (e != cudaSuccess) break;
         e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) break;
@@ -625,7 +1042,7 @@ fm_status wavefront_views(fm_ctx* ctx, const std::vector<WfView>& views_in, cons
             shade_ms += b;
         }
         // done when no slot holds work after the last shade
-        if (h_qc[6] == 0u) break;
+        if (h_qc[kQcActive] == 0u) break;
         if (++guard > max_launches) {
             result = set_error(ctx, FM_ERR_TIMEOUT, "wavefront: iteration limit reached");
             break;
@@ -645,7 +1062,7 @@ fm_status wavefront_views(fm_ctx* ctx, const std::vector<WfView>& views_in, cons
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, e0, e1);
     if (times) {
-        times->launches = 1 + graph_launches * 3 * tune.iters_per_graph + (int64_t)views.size();
+        times->launches = 1 + graph_launches * 5 * tune.iters_per_graph + (int64_t)views.size();
         times->total_ms = ms;
         times->trace_ms = trace_ms;
         times->shade_ms = shade_ms;
@@ -659,6 +1076,20 @@ fm_status wavefront_views(fm_ctx* ctx, const std::vector<WfView>& views_in, cons
     free_all();
     cudaStreamSynchronize(s);
     return result;
+}
+
+}  // namespace
+
+fm_status wavefront_views(fm_ctx* ctx, const std::vector<WfView>& views, const WfTuning& tune, Counters* cnt,
+                          WfTimes* times)
+{
+    return run_wavefront<false>(ctx, views, tune, nullptr, cnt, times);
+}
+
+fm_status wavefront_adjoint(fm_ctx* ctx, const std::vector<WfView>& views, const WfTuning& tune, const WfAdjoint& adj,
+                            Counters* cnt, WfTimes* times)
+{
+    return run_wavefront<true>(ctx, views, tune, &adj, cnt, times);
 }
 
 fm_status launch_wavefront(fm_ctx* ctx, const fm_scene* scene, const DevCamera& cam, const RenderCfg& cfg, float* rgb,

@@ -66,12 +66,16 @@ def rgbe_quantize(rgb: np.ndarray) -> np.ndarray:
 
 
 def write_hdr(path: Path, rgb: np.ndarray) -> None:
-    """Radiance file with new-style run-length scanlines made of literal runs only."""
+    """Radiance file with new-style run-length scanlines made of literal runs only (flat
+    RGBE pixels when the width is outside [8, 32768), where run-length coding is not
+    defined)."""
     h, w, _ = rgb.shape
-    if not (8 <= w < 32768):
-        raise ValueError("hdr width must be in [8, 32768)")
     enc = rgbe_encode(rgb)
     parts = [b"#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n", f"-Y {h} +X {w}\n".encode()]
+    if not (8 <= w < 32768):
+        parts.append(np.ascontiguousarray(enc, np.uint8).tobytes())
+        Path(path).write_bytes(b"".join(parts))
+        return
     for y in range(h):
         row = [bytes([2, 2, w >> 8, w & 255])]
         for c in range(4):
@@ -143,6 +147,20 @@ class Sphere:
     scale: tuple = (1.0, 1.0, 1.0)
     material: str = "default_material"
     emittance: tuple | None = None
+
+
+def camera_struct(c: dict) -> Camera:
+    """fm_camera from a camera dict in the reference's JSON schema."""
+    cam = Camera()
+    cam.type = FM_CAMERA_THIN_LENS if c.get("type", "pin_hole") == "thin_lens" else FM_CAMERA_PINHOLE
+    cam.pos = _f3(c.get("pos", [0, 0, 0]))
+    cam.look_at = _f3(c.get("look_at", [0, 0, 0]))
+    cam.up = _f3(c.get("up", [0, 0, 1]))
+    cam.fov = f32(c.get("fov", 60.0))
+    cam.aspect = f32(c.get("aspect", 1.0))
+    cam.focal_distance = f32(c.get("focal_distance", 1.0))
+    cam.lens_radius = f32(c.get("lens_radius", 0.0))
+    return cam
 
 
 @dataclass
@@ -257,17 +275,7 @@ class SceneSpec:
         return DescHolder(self)
 
     def camera_struct(self) -> Camera:
-        c = self.camera
-        cam = Camera()
-        cam.type = FM_CAMERA_THIN_LENS if c.get("type", "pin_hole") == "thin_lens" else FM_CAMERA_PINHOLE
-        cam.pos = _f3(c.get("pos", [0, 0, 0]))
-        cam.look_at = _f3(c.get("look_at", [0, 0, 0]))
-        cam.up = _f3(c.get("up", [0, 0, 1]))
-        cam.fov = f32(c.get("fov", 60.0))
-        cam.aspect = f32(c.get("aspect", 1.0))
-        cam.focal_distance = f32(c.get("focal_distance", 1.0))
-        cam.lens_radius = f32(c.get("lens_radius", 0.0))
-        return cam
+        return camera_struct(self.camera)
 
     def render_params(self, spp: int | None = None, seed: int = 0, mode: int = FM_MODE_WAVEFRONT,
                       sample_offset: int = 0) -> RenderParams:
@@ -310,6 +318,9 @@ class DescHolder:
             mat_idx["default_material"] = len(mat_idx)
         tex_names = list(spec.textures)
         tex_idx = {n: i for i, n in enumerate(tex_names)}
+        self.texture_index = tex_idx            # texture name -> scene texture index
+        self.material_index = mat_idx           # material name -> scene material index
+        self.num_materials = len(mat_idx)
         keep = []
         # objects
         obj_mat, obj_em = [], []

@@ -325,3 +325,137 @@ def batch_scene(s: int, env_w: int = 512, env_h: int = 256, res: int | None = No
 
 def batch_scenes(n: int = 64, **kw) -> list:
     return [batch_scene(s, **kw) for s in range(n)]
+
+
+# ---- inverse rendering workload ------------------------------------------------------
+
+
+def uv_plane(n: int, size: float, seed: int, amp: float):
+    """n x n quads over [-size, size]^2 in z = 0, displaced along z by amp * fBm, with
+    uv in [0, 1]^2 (2 n^2 triangles)."""
+    g = np.linspace(-size, size, n + 1)
+    X, Y = np.meshgrid(g, g, indexing="xy")
+    P = np.stack([X, Y, np.zeros_like(X)], -1).reshape(-1, 3)
+    P[:, 2] = amp * PerlinNoise(seed).fbm(P * (1.5 / size))
+    t = np.linspace(0.0, 1.0, n + 1)
+    U, V = np.meshgrid(t, t, indexing="xy")
+    uv = np.stack([U, V], -1).reshape(-1, 2)
+    idx = np.arange((n + 1) * (n + 1)).reshape(n + 1, n + 1)
+    q0, q1, q2, q3 = idx[:-1, :-1], idx[:-1, 1:], idx[1:, 1:], idx[1:, :-1]
+    f = np.concatenate([np.stack([q0, q1, q2], -1).reshape(-1, 3), np.stack([q0, q2, q3], -1).reshape(-1, 3)])
+    return P.astype(np.float32), f, uv.astype(np.float32)
+
+
+def uv_sphere(nu: int, nv: int, radius: float, center):
+    """Latitude-longitude sphere (z-up) with u = phi / 2pi, v = theta / pi; a fan of
+    nu triangles at each pole (2 nu (nv - 1) triangles)."""
+    verts, uvs = [], []
+    for j in range(nv + 1):
+        th = math.pi * j / nv
+        for i in range(nu + 1):
+            ph = 2 * math.pi * i / nu
+            verts.append([math.sin(th) * math.cos(ph), math.sin(th) * math.sin(ph), math.cos(th)])
+            uvs.append([i / nu, j / nv])
+    idx = np.arange((nv + 1) * (nu + 1)).reshape(nv + 1, nu + 1)
+    faces = []
+    for j in range(nv):
+        for i in range(nu):
+            a, b, c, d = idx[j, i], idx[j, i + 1], idx[j + 1, i + 1], idx[j + 1, i]
+            if j > 0:
+                faces.append([a, d, b])
+            if j < nv - 1:
+                faces.append([b, d, c])
+    v = np.asarray(verts) * radius + np.asarray(center, np.float64)
+    return v.astype(np.float32), np.asarray(faces, np.int64), np.asarray(uvs, np.float32)
+
+
+def smooth_texture(res: int, seed: int, lo: float, hi: float, channels: int = 3) -> np.ndarray:
+    """res x res x channels smoothed noise (fBm) mapped to [lo, hi]."""
+    g = (np.arange(res) + 0.5) / res * 4.0
+    X, Y = np.meshgrid(g, g, indexing="xy")
+    out = np.empty((res, res, channels), np.float32)
+    for c in range(channels):
+        P = np.stack([X + 17.3 * c, Y - 5.1 * c, np.full_like(X, 0.37 + c)], -1).reshape(-1, 3)
+        n = PerlinNoise(seed * 31 + c).fbm(P, octaves=4).reshape(res, res)
+        n = (n - n.min()) / max(n.max() - n.min(), 1e-9)
+        out[..., c] = lo + (hi - lo) * n
+    return out
+
+
+def inverse_scene(seed: int = 4, tex_res: int = 512, plane_n: int = 200, sphere_nu: int = 200, sphere_nv: int = 100,
+                  env_w: int = 128, env_h: int = 64, res: int = 256, spp: int = 32, depth: int = 6,
+                  target: bool = True) -> SceneSpec:
+    """Differentiable-rendering workload: a displaced UV-mapped plane and a UV sphere
+    (about 120k triangles at the defaults) sharing one Disney material whose basecolor
+    is texture "basecolor" and whose roughness (G) and metallic (B) are texture "rm";
+    a rectangle area light and a small sky.  target=True gives the hidden smoothed-noise
+    textures, target=False the constant 0.5 initial guess."""
+    pv, pf, puv = uv_plane(plane_n, 2.0, seed, 0.08)
+    sv, sf, suv = uv_sphere(sphere_nu, sphere_nv, 0.6, (0.0, 0.0, 0.7))
+    objs = [Mesh(pv, pf, "surf", uvs=puv), Mesh(sv, sf, "surf", uvs=suv),
+            Rect((-0.8, -0.8, 4.0), (-0.8, 0.8, 4.0), (0.8, 0.8, 4.0), (0.8, -0.8, 4.0), "surf",
+                 emittance=(12.0, 12.0, 11.0))]
+    if target:
+        base = smooth_texture(tex_res, seed, 0.1, 0.9)
+        rm = smooth_texture(tex_res, seed + 1, 0.1, 0.9)
+        rm[..., 0] = 0.0
+        rm[..., 2] = np.clip((rm[..., 2] - 0.3) * 1.6, 0.0, 1.0)
+    else:
+        base = np.full((tex_res, tex_res, 3), 0.5, np.float32)
+        rm = np.full((tex_res, tex_res, 3), 0.5, np.float32)
+        rm[..., 0] = 0.0
+    mats = [{"name": "surf", "type": "disney", "basecolor": {"image": "basecolor"}, "roughness": {"image": "rm"},
+             "metallic": {"image": "rm"}, "specular": 0.5}]
+    env = sky_env(env_w, env_h, seed + 2, sun_peak=40.0, sun_sigma_deg=5.0)
+    cam = inverse_views(1, seed + 1)[0]
+    ren = {"width": res, "height": res, "spp": spp, "depth": depth, "rr_depth": 3, "rr_coef": 0.85}
+    lights = [{"type": "env", "texture": "sky", "rotation": [0, 0, 0], "factor": 1.0}]
+    return SceneSpec(cam, ren, mats, objs, lights, {"basecolor": base, "rm": rm, "sky": env})
+
+
+def inverse_views(n: int = 16, seed: int = 5) -> list:
+    """n pinhole cameras around the inverse-rendering scene (seeded azimuth jitter)."""
+    rng = np.random.default_rng(seed)
+    cams = []
+    for k in range(n):
+        az = 2 * math.pi * (k + rng.uniform(-0.2, 0.2)) / n
+        el = math.radians(rng.uniform(25.0, 55.0))
+        r = 4.2
+        pos = [r * math.cos(el) * math.cos(az), r * math.cos(el) * math.sin(az), r * math.sin(el)]
+        cams.append({"type": "pin_hole", "pos": pos, "look_at": [0.0, 0.0, 0.3], "up": [0, 0, 1], "fov": 50.0,
+                     "aspect": 1.0})
+    return cams
+
+
+def gradient_scene(res: int = 48, tex_res: int = 4, base=None, rm=None, sky=None, probe=None, lam=(0.3, 0.5, 0.7)) -> SceneSpec:
+    """Small scene for gradient checks: a textured Disney plane ("surf": basecolor
+    texture "base", roughness (G) / metallic (B) texture "rm"), a Disney sphere with
+    constant parameters ("probe"), a Lambert sphere ("lam"), a rectangle light and a
+    soft 16x8 sky.  Texel values are RGBE-representable, so the reference reads the
+    written .hdr files exactly."""
+    pv, pf, puv = uv_plane(8, 1.5, 3, 0.05)
+    s1v, s1f, s1uv = uv_sphere(24, 12, 0.45, (0.55, 0.1, 0.45))
+    s2v, s2f, s2uv = uv_sphere(24, 12, 0.35, (-0.6, -0.2, 0.35))
+    objs = [Mesh(pv, pf, "surf", uvs=puv), Mesh(s1v, s1f, "probe", uvs=s1uv), Mesh(s2v, s2f, "lam", uvs=s2uv),
+            Rect((-0.5, -0.5, 3.0), (-0.5, 0.5, 3.0), (0.5, 0.5, 3.0), (0.5, -0.5, 3.0), "lam",
+                 emittance=(9.0, 9.0, 8.0))]
+    if base is None:
+        base = rgbe_quantize(smooth_texture(tex_res, 11, 0.2, 0.8))
+    if rm is None:
+        rm = smooth_texture(tex_res, 12, 0.25, 0.75)
+        rm[..., 0] = 0.0
+        rm = rgbe_quantize(rm)
+    if sky is None:
+        sky = sky_env(16, 8, 7, sun_peak=3.0, sun_sigma_deg=20.0)
+    p = dict(basecolor=[0.6, 0.35, 0.25], metallic=0.3, roughness=0.45)
+    if probe:
+        p.update(probe)
+    mats = [{"name": "surf", "type": "disney", "basecolor": {"image": "base"}, "roughness": {"image": "rm"},
+             "metallic": {"image": "rm"}, "specular": 0.5},
+            {"name": "probe", "type": "disney", "specular": 0.5, "clearcoat": 0.2, **p},
+            {"name": "lam", "type": "lambert_diffuse", "basecolor": list(lam)}]
+    cam = {"type": "pin_hole", "pos": [0.3, -3.0, 2.4], "look_at": [0.0, 0.0, 0.3], "up": [0, 0, 1], "fov": 45.0,
+           "aspect": 1.0}
+    ren = {"width": res, "height": res, "spp": 16, "depth": 5, "rr_depth": 3, "rr_coef": 0.85}
+    return SceneSpec(cam, ren, mats, objs, [{"type": "env", "texture": "sky", "factor": 1.0}],
+                     {"base": base, "rm": rm, "sky": sky})

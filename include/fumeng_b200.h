@@ -201,6 +201,11 @@ fm_status fm_scene_destroy(fm_ctx* ctx, fm_scene* scene);
 fm_status fm_scene_bvh_stats(fm_ctx* ctx, const fm_scene* scene, int64_t* nodes, int64_t* prims,
                              int32_t* depth, double* build_ms);
 
+/* Sizes of a created scene: objects, materials, textures, lights (area lights first).
+ * Any output may be NULL. */
+fm_status fm_scene_info(fm_ctx* ctx, const fm_scene* scene, int64_t* objects, int32_t* materials,
+                        int32_t* textures, int32_t* lights);
+
 /* Replaces: Aggregate::GetIntersect (core/aggregate.h:30, accelerator/bvh_aggregate.cpp:
  * 167-176).  rays: n x 8 floats.  obj_id[i] = object index of the closest hit or -1;
  * t[i] = its distance (+inf on a miss). */
@@ -274,6 +279,45 @@ fm_status fm_draw_frame(fm_ctx* ctx, const char* json_path);
  *     device (from different contexts or threads) race with each other. */
 fm_status fm_trace_closest_noalloc(fm_ctx* ctx, const fm_scene* scene, const float* rays, int64_t n,
                                    int32_t* obj_id, float* t);
+
+/* ---- differentiable rendering ------------------------------------------------------
+ * The reference renders forward only; the two entry points below have no counterpart
+ * in it. */
+
+/* Replaces texture contents in place (texels: width*height*3 floats in the texture's
+ * own size, row 0 = top; device pointer with FM_FLAG_DEVICE_PTRS).  If the texture is
+ * the environment light's, its importance-sampling tables are rebuilt. */
+fm_status fm_scene_update_texture(fm_ctx* ctx, fm_scene* scene, int32_t texture, const float* texels,
+                                  int32_t flags);
+
+/* Number of differentiated parameters per material: basecolor r, g, b, metallic,
+ * roughness (in this order). */
+enum { FM_GRAD_PARAMS = 5 };
+
+/* Gradient outputs of fm_render_adjoint.  Values are ADDED to what the buffers hold.
+ * texture_grads[t] (t a scene texture index) is NULL or width*height*3 doubles, the
+ * derivative with respect to each texel channel; a material parameter read from a
+ * texture sends its derivative there (basecolor: rgb, metallic: the third channel,
+ * roughness: the second), as does the environment light's texture.  material_grads is
+ * NULL or num_materials * FM_GRAD_PARAMS doubles: derivatives with respect to the
+ * constant (untextured) parameters of Lambert and Disney materials. */
+typedef struct {
+    double* const* texture_grads;   /* array of num_textures pointers, or NULL */
+    double* material_grads;
+} fm_grad_desc;
+
+/* Path-replay adjoint.  For views v of one scene (cameras[v], params[v]; wavefront mode),
+ * computes the gradient of  sum_v sum_pixels d_rgb[v] . image_v  with respect to the
+ * texels and material constants above, where image_v is the mean over params[v].spp
+ * samples (use a seed different from the forward render's for a decorrelated
+ * estimate).  Each sample's path is traced once for its radiance and replayed with the
+ * same random numbers to accumulate derivatives, so memory does not grow with depth or
+ * spp.  Sampling, pdfs and MIS weights are treated as constants.  rgb (NULL, or an
+ * array of per-view NULL or width*height*3 buffers) receives the primal image of the
+ * samples used.  Host buffers unless FM_FLAG_DEVICE_PTRS. */
+fm_status fm_render_adjoint(fm_ctx* ctx, const fm_scene* scene, int32_t num_views, const fm_camera* cameras,
+                            const fm_render_params* params, const float* const* d_rgb, float* const* rgb,
+                            const fm_grad_desc* grads, int32_t flags, fm_render_stats* stats);
 
 #ifdef __cplusplus
 }

@@ -3,7 +3,7 @@
 Run on a machine that has the reference sources (the oracle libraries are built from
 them by oracle/Makefile):
 
-    python tests/golden/make_golden.py [hit] [images]
+    python tests/golden/make_golden.py [hit] [images] [adjoint]
 
 Scenes and rays are regenerated from seeds by fumeng_b200.synth, so each fixture stores
 only the reference's answers plus a SHA-256 of the inputs, which the tests recompute to
@@ -91,6 +91,51 @@ def make_image(case):
     print(name, "spp", spp, "%.1fs" % dt, "mean", mean.mean(axis=(0, 1)))
 
 
+# Central differences of L = sum(w * image) from the reference's double build, for
+# constant material parameters of synth.gradient_scene (48x48), with common random
+# numbers across +-h: (material, JSON key, channel or None).
+ADJ_FD_CASES = [("probe", "basecolor", 0), ("probe", "metallic", None), ("probe", "roughness", None),
+                ("lam", "basecolor", 1)]
+ADJ_FD = {"spp": 1024, "seeds": [301, 302, 303, 304], "h": 0.02, "wseed": 5}
+
+
+def adjoint_fd_weights():
+    return np.random.default_rng(ADJ_FD["wseed"]).uniform(0.5, 1.5, (48, 48, 3)).astype(np.float32)
+
+
+def perturbed_gradient_scene(mat, key, ch, delta):
+    spec = synth.gradient_scene()
+    m = next(x for x in spec.materials if x["name"] == mat)
+    if ch is None:
+        m[key] = float(m[key]) + delta
+    else:
+        v = list(m[key])
+        v[ch] += delta
+        m[key] = v
+    return spec
+
+
+def make_adjoint_fd():
+    w = adjoint_fd_weights().astype(np.float64)
+    fd = np.zeros((len(ADJ_FD_CASES), len(ADJ_FD["seeds"])))
+    h, spp = ADJ_FD["h"], ADJ_FD["spp"]
+    for ci, (mat, key, ch) in enumerate(ADJ_FD_CASES):
+        for si, seed in enumerate(ADJ_FD["seeds"]):
+            L = []
+            for sign in (1.0, -1.0):
+                spec = perturbed_gradient_scene(mat, key, ch, sign * h)
+                with tempfile.TemporaryDirectory() as d:
+                    rs = fmref.RefScene(spec.write(Path(d)), "double")
+                    r = rs.render(spp, seed=seed)
+                    rs.close()
+                L.append(float((w * r["sum"] / spp).sum()))
+            fd[ci, si] = (L[0] - L[1]) / (2 * h)
+        print("adjoint fd", mat, key, ch, fd[ci].mean(), fd[ci].std(ddof=1) / np.sqrt(fd.shape[1]))
+    np.savez_compressed(GOLDEN / "adj_fd_ref.npz", fd=fd, spp=spp, h=h, seeds=np.asarray(ADJ_FD["seeds"]),
+                        wseed=ADJ_FD["wseed"],
+                        cases=np.asarray([f"{m}.{k}.{-1 if c is None else c}" for m, k, c in ADJ_FD_CASES]))
+
+
 if __name__ == "__main__":
     what = set(sys.argv[1:]) or {"hit"}
     t0 = time.time()
@@ -100,4 +145,6 @@ if __name__ == "__main__":
     if "images" in what:
         for c in IMAGE_CASES:
             make_image(c)
+    if "adjoint" in what:
+        make_adjoint_fd()
     print("done in %.1fs" % (time.time() - t0))
