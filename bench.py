@@ -221,6 +221,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scenes", type=int, default=NSCENES, help="batch size (profiling runs use fewer)")
     ap.add_argument("--adjoint-steps", type=int, default=2, help="timed adjoint/forward pairs (0 skips)")
+    ap.add_argument("--no-autotune", action="store_true", help="default tuning instead of the autotuner's")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -286,7 +287,7 @@ def main():
     outs = [torch.empty((p.height, p.width, 3), device="cuda", dtype=torch.float32) for p in params_wf]
     out_ptrs = [o.data_ptr() for o in outs]
 
-    tuning = ctx.autotune_batch(scenes, cams, params_wf)
+    tuning = fb.Tuning(1 << 21, 128, 128, 8) if args.no_autotune else ctx.autotune_batch(scenes, cams, params_wf)
 
     def step_wf(profile=False):
         return ctx.render_batch(scenes, cams, params_wf, tuning=tuning, device_outputs=out_ptrs, profile=profile)[3]

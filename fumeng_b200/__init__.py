@@ -304,7 +304,7 @@ class Scene:
         self.ctx.check(self.ctx.lib.fm_scene_update_texture(self.ctx.h, self.h, int(index), _ptr(texels), 0))
 
     def render_adjoint(self, cams, params, d_rgb, texture_shapes: dict, material_grads: bool = False,
-                       want_image: bool = False):
+                       want_image: bool = False, profile: bool = False):
         """Path-replay adjoint over views (cams[i], params[i]) with dLoss/dI images d_rgb[i].
 
         texture_shapes: {texture index: (height, width)} of the textures whose texel
@@ -328,7 +328,8 @@ class Scene:
             mg = np.zeros((info["materials"], GRAD_PARAMS), np.float64)
         gd = GradDesc(tarr if nt else None, mg.ctypes.data if mg is not None else None)
         stats = RenderStats()
-        self.ctx.check(self.ctx.lib.fm_render_adjoint(self.ctx.h, self.h, n, ca, pa, dp, ip, C.byref(gd), 0,
+        flags = FM_FLAG_PROFILE if profile else 0
+        self.ctx.check(self.ctx.lib.fm_render_adjoint(self.ctx.h, self.h, n, ca, pa, dp, ip, C.byref(gd), flags,
                                                       C.byref(stats)))
         return tg, mg, imgs, stats
 

@@ -17,6 +17,16 @@ __global__ void k_rgb_to_texels(const float* __restrict__ src, float4* __restric
         dst[i] = make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0f);
 }
 
+// out[i] += sum over the copies of acc (FP64 sums of the FP32 accumulators).
+__global__ void k_grad_reduce(const float* __restrict__ acc, int copies, size_t n, double* __restrict__ out)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        double sum = 0.0;
+        for (int k = 0; k < copies; ++k) sum += (double)acc[(size_t)k * n + i];
+        out[i] += sum;
+    }
+}
+
 // Device allocations of one call, released on every exit path.
 struct Allocs {
     cudaStream_t s;
@@ -139,11 +149,27 @@ extern "C" fm_status fm_render_adjoint(fm_ctx* ctx, const fm_scene* scene, int32
                             "render_adjoint");
             }
         }
-        double** d_tex_arr = a.get<double*>((size_t)(nt > 0 ? nt : 1));
+        // FP32 accumulators the kernels add to (kGradCopies per texture)
+        std::vector<float*> facc((size_t)nt, nullptr);
+        std::vector<size_t> tex_n((size_t)nt, 0);
+        for (int t = 0; t < nt; ++t) {
+            if (!dtex[t]) continue;
+            tex_n[t] = (size_t)scene->textures[t].w * scene->textures[t].h * 3;
+            facc[t] = a.get<float>(tex_n[t] * kGradCopies);
+            if (!facc[t]) return oom();
+            FM_CUDA_TRY(ctx, cudaMemsetAsync(facc[t], 0, tex_n[t] * kGradCopies * sizeof(float), s), "render_adjoint");
+        }
+        float* macc = nullptr;
+        if (dmat) {
+            macc = a.get<float>((size_t)nm * kGradParams);
+            if (!macc) return oom();
+            FM_CUDA_TRY(ctx, cudaMemsetAsync(macc, 0, (size_t)nm * kGradParams * sizeof(float), s), "render_adjoint");
+        }
+        float** d_tex_arr = a.get<float*>((size_t)(nt > 0 ? nt : 1));
         Counters* d_cnt = a.get<Counters>(1);
         if (!d_tex_arr || !d_cnt) return oom();
         if (nt > 0)
-            FM_CUDA_TRY(ctx, cudaMemcpyAsync(d_tex_arr, dtex.data(), sizeof(double*) * nt, cudaMemcpyHostToDevice, s),
+            FM_CUDA_TRY(ctx, cudaMemcpyAsync(d_tex_arr, facc.data(), sizeof(float*) * nt, cudaMemcpyHostToDevice, s),
                         "render_adjoint");
         FM_CUDA_TRY(ctx, cudaMemsetAsync(d_cnt, 0, sizeof(Counters), s), "render_adjoint");
         FM_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), s), "render_adjoint");
@@ -186,10 +212,18 @@ extern "C" fm_status fm_render_adjoint(fm_ctx* ctx, const fm_scene* scene, int32
             env_total = env_row + eh;
             FM_CUDA_TRY(ctx, cudaMemsetAsync(env_row, 0, sizeof(double) * (eh + 1), s), "render_adjoint");
         }
-        WfAdjoint adj{d_tex_arr, dmat, env_row, env_total};
+        WfAdjoint adj{d_tex_arr, macc, env_row, env_total};
         WfTuning wt;
         wt.profile = (flags & FM_FLAG_PROFILE) != 0;
         result = wavefront_adjoint(ctx, views, wt, adj, d_cnt, &tm);
+        if (result == FM_OK) {
+            const int grid = ctx->num_sms * 8;
+            for (int t = 0; t < nt; ++t)
+                if (facc[t]) k_grad_reduce<<<grid, 256, 0, s>>>(facc[t], kGradCopies, tex_n[t], dtex[t]);
+            if (macc) k_grad_reduce<<<grid, 256, 0, s>>>(macc, 1, (size_t)nm * kGradParams, dmat);
+            const cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) result = cuda_error(ctx, e, "render_adjoint reduce");
+        }
         if (result == FM_OK && env_row)
             result = env_grad_finalize(ctx, scene->textures[env_tex], env_row, env_total, dtex[env_tex]);
         if (result == FM_OK && !dev) {

@@ -103,9 +103,8 @@ FM_D void intersect_node(const uint4* __restrict__ nodes, int node, f3 o, f3 idi
 // (t > t_best || t <= 0) (triangle.cpp:211-225, bvh_aggregate.cpp:108-115); rectangle
 // halves skip the second check (rectangle.cpp:42-56); spheres use the inclusive range
 // (sphere.cpp:116-127).
-template <bool ANY>
 FM_D bool test_prim(const TraceScene& S, const RayPre& rp, f3 o, f3 d, int slot, float tmin, float& tbest,
-                    Hit& hit)
+                    Hit& hit, bool any)
 {
     const float4 a = __ldg(S.leaf + 3 * (size_t)slot);
     const uint32_t tag = __float_as_uint(a.w);
@@ -114,10 +113,10 @@ FM_D bool test_prim(const TraceScene& S, const RayPre& rp, f3 o, f3 d, int slot,
         const SphereDev& sp = S.spheres[sidx];
         float t;
         if (!intersect_sphere(sp.w2o, sp.radius, o, d, tmin, tbest, t)) return false;
-        if (!ANY) {
+        hit.prim = (int)(tag & ~kSphereFlag);
+        if (!any) {
             tbest = t;
             hit.t = t;
-            hit.prim = (int)(tag & ~kSphereFlag);
             hit.b1 = hit.b2 = 0.0f;
         }
         return true;
@@ -127,8 +126,11 @@ FM_D bool test_prim(const TraceScene& S, const RayPre& rp, f3 o, f3 d, int slot,
     float t, b0, b1, b2;
     if (!intersect_triangle(rp, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, f3{c.x, c.y, c.z}, tmin, tbest, t, b0, b1, b2))
         return false;
-    if (ANY) return true;
     const int prim = (int)tag;
+    if (any) {
+        hit.prim = prim;
+        return true;
+    }
     if (prim < S.num_tris && (t > tbest || t <= 0.0f)) return false;
     tbest = t;
     hit.t = t;
@@ -138,67 +140,102 @@ FM_D bool test_prim(const TraceScene& S, const RayPre& rp, f3 o, f3 d, int slot,
     return true;
 }
 
-// Closest hit (ANY = false) or occlusion (ANY = true) query.  Returns true on a hit.
-// *overflow is set when the traversal stack would overflow (the builder bounds the tree
-// depth so that this cannot happen for trees it accepted).
-template <bool ANY>
-FM_D bool trace_ray(const TraceScene& S, f3 o, f3 d, float tmin, float tmax, Hit& hit, uint32_t* overflow)
+// Resumable traversal: the state of one query, advanced one node at a time by
+// trav_step.  Kernels that keep a warp busy with a stream of rays (fetching a new ray
+// into a lane as soon as its query completes) drive it directly; trace_ray_any runs it
+// to completion.
+struct Traversal {
+    RayPre rp;        // rp.o is the ray origin
+    f3 d, idir;
+    uint32_t oct;
+    float tmin, tbest;
+    bool any;
+    int sp;
+    uint2 ngrp, pgrp;
+    Hit hit;
+};
+
+FM_D void trav_begin(Traversal& t, const TraceScene& S, f3 o, f3 d, float tmin, float tmax, bool any)
 {
-    hit.t = tmax;
-    hit.prim = -1;
-    if (S.num_nodes == 0) return false;
-    const RayPre rp = ray_pre(o, d);
+    t.hit.t = tmax;
+    t.hit.prim = -1;
+    t.hit.b1 = t.hit.b2 = 0.0f;
+    t.rp = ray_pre(o, d);
+    t.d = d;
     const float sdx = fabsf(d.x) < 1e-20f ? copysignf(1e-20f, d.x) : d.x;
     const float sdy = fabsf(d.y) < 1e-20f ? copysignf(1e-20f, d.y) : d.y;
     const float sdz = fabsf(d.z) < 1e-20f ? copysignf(1e-20f, d.z) : d.z;
-    const f3 idir = f3{1.0f / sdx, 1.0f / sdy, 1.0f / sdz};
-    const uint32_t oct = (d.x >= 0.0f ? 1u : 0u) | (d.y >= 0.0f ? 2u : 0u) | (d.z >= 0.0f ? 4u : 0u);
-    uint2 stack[kTraversalStack];
-    int sp = 0;
-    // Virtual parent of the root: one internal child in slot 0.
-    uint2 ngrp = make_uint2(0u, (1u << (24 + (0u ^ oct))) | 1u);
-    uint2 pgrp = make_uint2(0u, 0u);
-    float tbest = tmax;
-    bool found = false;
-    for (;;) {
-        if (ngrp.y > 0x00ffffffu) {
-            const uint32_t key = 31u - __clz(ngrp.y) - 24u;
-            ngrp.y &= ~(1u << (24u + key));
-            const uint32_t slot = key ^ oct;
-            const uint32_t imask = ngrp.y & 0xffu;
-            const int child = (int)(ngrp.x + __popc(imask & ((1u << slot) - 1u)));
-            if (ngrp.y > 0x00ffffffu) {
-                if (sp < kTraversalStack)
-                    stack[sp++] = ngrp;
-                else if (overflow)
-                    atomicOr(overflow, 1u);
-            }
-            uint32_t cb, nb, pb, pbits;
-            intersect_node(S.nodes, child, o, idir, oct, tmin, tbest, cb, nb, pb, pbits);
-            ngrp = make_uint2(cb, nb);
-            pgrp = make_uint2(pb, pbits);
+    t.idir = f3{1.0f / sdx, 1.0f / sdy, 1.0f / sdz};
+    t.oct = (d.x >= 0.0f ? 1u : 0u) | (d.y >= 0.0f ? 2u : 0u) | (d.z >= 0.0f ? 4u : 0u);
+    t.tmin = tmin;
+    t.tbest = tmax;
+    t.any = any;
+    t.sp = 0;
+    // virtual parent of the root: one internal child in slot 0 (none for an empty tree)
+    t.ngrp = S.num_nodes == 0 ? make_uint2(0u, 0u) : make_uint2(0u, (1u << (24 + (0u ^ t.oct))) | 1u);
+    t.pgrp = make_uint2(0u, 0u);
+}
+
+// Visits the nearest pending child node, tests the primitives it exposes and pops the
+// stack when the current group is exhausted.  Returns true when the query is complete
+// (t.hit.prim >= 0 on a hit).  *overflow is set when the traversal stack would overflow
+// (the builder bounds the tree depth so that this cannot happen for trees it accepted).
+FM_D bool trav_step(Traversal& t, const TraceScene& S, uint2* stack, uint32_t* overflow)
+{
+    if (t.ngrp.y > 0x00ffffffu) {
+        const uint32_t key = 31u - __clz(t.ngrp.y) - 24u;
+        t.ngrp.y &= ~(1u << (24u + key));
+        const uint32_t slot = key ^ t.oct;
+        const uint32_t imask = t.ngrp.y & 0xffu;
+        const int child = (int)(t.ngrp.x + __popc(imask & ((1u << slot) - 1u)));
+        if (t.ngrp.y > 0x00ffffffu) {
+            if (t.sp < kTraversalStack)
+                stack[t.sp++] = t.ngrp;
+            else if (overflow)
+                atomicOr(overflow, 1u);
         }
-        while (pgrp.y != 0u) {
-            const int bit = __ffs(pgrp.y) - 1;
-            pgrp.y &= pgrp.y - 1u;
-            if (test_prim<ANY>(S, rp, o, d, (int)pgrp.x + bit, tmin, tbest, hit)) {
-                found = true;
-                if (ANY) return true;
-            }
-        }
-        if (ngrp.y <= 0x00ffffffu) {
-            if (sp == 0) break;
-            ngrp = stack[--sp];
-        }
+        uint32_t cb, nb, pb, pbits;
+        intersect_node(S.nodes, child, t.rp.o, t.idir, t.oct, t.tmin, t.tbest, cb, nb, pb, pbits);
+        t.ngrp = make_uint2(cb, nb);
+        t.pgrp = make_uint2(pb, pbits);
     }
-    return found;
+    while (t.pgrp.y != 0u) {
+        const int bit = __ffs(t.pgrp.y) - 1;
+        t.pgrp.y &= t.pgrp.y - 1u;
+        if (test_prim(S, t.rp, t.rp.o, t.d, (int)t.pgrp.x + bit, t.tmin, t.tbest, t.hit, t.any) && t.any) return true;
+    }
+    if (t.ngrp.y <= 0x00ffffffu) {
+        if (t.sp == 0) return true;
+        t.ngrp = stack[--t.sp];
+    }
+    return false;
+}
+
+// Closest hit (any = false) or occlusion (any = true) query; hit.prim >= 0 on a hit.
+// Not inlined: a kernel that traces several kinds of rays holds one copy of the
+// traversal loop, which keeps its code within the instruction caches.
+static __device__ __noinline__ Hit trace_ray_any(TraceScene S, f3 o, f3 d, float tmin, float tmax, bool any,
+                                                 uint32_t* overflow)
+{
+    Traversal t;
+    uint2 stack[kTraversalStack];
+    trav_begin(t, S, o, d, tmin, tmax, any);
+    while (!trav_step(t, S, stack, overflow)) {
+    }
+    return t.hit;
+}
+
+template <bool ANY>
+FM_D bool trace_ray(const TraceScene& S, f3 o, f3 d, float tmin, float tmax, Hit& hit, uint32_t* overflow)
+{
+    hit = trace_ray_any(S, o, d, tmin, tmax, ANY, overflow);
+    return hit.prim >= 0;
 }
 
 template <bool ANY>
 FM_D bool trace_ray(const DevScene& S, f3 o, f3 d, float tmin, float tmax, Hit& hit, uint32_t* overflow)
 {
-    const TraceScene ts = trace_scene(S);
-    return trace_ray<ANY>(ts, o, d, tmin, tmax, hit, overflow);
+    return trace_ray<ANY>(trace_scene(S), o, d, tmin, tmax, hit, overflow);
 }
 
 }  // namespace fm

@@ -24,10 +24,11 @@ struct WfView {
     const float* drgb;       // adjoint renders: dLoss/dI per pixel (device, w*h*3)
 };
 
-// Gradient outputs of an adjoint render (device buffers, added to).
+// Gradient accumulators of an adjoint render (device buffers, zeroed by the caller).
+constexpr int kGradCopies = 4;   // FP32 copies of each texture's accumulator
 struct WfAdjoint {
-    double* const* tex_grad;   // device array over the scene's textures: NULL or w*h*3
-    double* mat_grad;          // num_materials * 5 (basecolor rgb, metallic, roughness) or NULL
+    float* const* tex_acc;     // device array over the scene's textures: NULL or kGradCopies x w*h*3
+    float* mat_acc;            // num_materials * 5 (basecolor rgb, metallic, roughness) or NULL
     double* env_row;           // env map height doubles, zeroed (score sums per row)
     double* env_total;         // one double, zeroed
 };

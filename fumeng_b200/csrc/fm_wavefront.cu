@@ -41,10 +41,11 @@ constexpr int kPending = 2;
 // adjoint renders: the slot is replaying its sample's path (second pass)
 constexpr int kReplay = 4;
 // queue counters: the three ray queues being filled for the next trace, the same three
-// being traced, slots still holding work, and the two shading queues
+// being traced, slots still holding work, the two shading queues, and the trace
+// kernel's next unclaimed ray
 constexpr int kQcCont = 0, kQcMis = 1, kQcShadow = 2;
 constexpr int kQcTraceCont = 3, kQcTraceMis = 4, kQcTraceShadow = 5;
-constexpr int kQcActive = 6, kQcDisney = 7, kQcSimple = 8;
+constexpr int kQcActive = 6, kQcDisney = 7, kQcSimple = 8, kQcTraceNext = 9;
 constexpr int kQcCount = 16;
 
 struct WfState {
@@ -85,11 +86,12 @@ struct WfState {
     uint32_t* status;
     // adjoint renders only (null otherwise)
     float4* lp;           // primal radiance of the slot's current sample
-    float4* dfr;          // [5 per slot] deferred continuation gradient: dlw[15] (c*5+i), material, u, v
+    float4* dfr;          // [5 per slot] the slot's current vertex: dlw[15] (c*5+i), material, u, v
+    float4* vg;           // [2 per slot] gradient collected for that vertex (g[5]; NEE / MIS, trace kernel)
     float4* sh_g;         // [3 per shadow ray] g[5], u, v, material, env weight e[3], env score s
     float4* mis_g;        // [8 per MIS ray] B[15] (c*5+i), material, u, v, e[3], a[5], b[5]
-    double* const* tex_grad;   // per scene texture: NULL or w*h*3
-    double* mat_grad;          // num_materials * 5, or NULL
+    float* const* tex_acc;     // per scene texture: NULL or kGradCopies x w*h*3 FP32 accumulators
+    float* mat_acc;            // num_materials * 5 FP32 accumulators, or NULL
     double* env_row;           // env importance: per-row and global score sums (see scatter_env_score)
     double* env_total;
 };
@@ -165,15 +167,38 @@ FM_D f3 pixel_delta(const WfState& st, int slot, const WfView& V)
     return f3{__ldg(d) * inv, __ldg(d + 1) * inv, __ldg(d + 2) * inv};
 }
 
+// Texel gradients are accumulated in FP32 (reductions with no return value) in
+// kGradCopies copies, a block writing to copy blockIdx % kGradCopies, which spreads the
+// updates neighbouring pixels make to the same texel; the copies are summed in FP64
+// after the render (fm_adjoint.cu).
+FM_D float* grad_copy(float* acc, const DevTexture& t)
+{
+    return acc + (size_t)(blockIdx.x % kGradCopies) * ((size_t)t.w * t.h * 3);
+}
+
 // Adds g[c] * (weight of each tap) to channel c0 + c of the taps tex_sample reads.
-FM_D void tex_scatter(const DevTexture& t, double* grad, float u, float v, int c0, int nc, const float* g)
+FM_D void tex_scatter(const DevTexture& t, float* acc, float u, float v, int c0, int nc, const float* g)
 {
     const TexTaps tp = tex_taps(t, u, v);
+    float* base = grad_copy(acc, t);
     for (int k = 0; k < tp.n; ++k) {
         if (tp.w[k] == 0.0f) continue;
-        double* at = grad + 3 * ((size_t)tp.y[k] * t.w + tp.x[k]) + c0;
+        float* at = base + 3 * ((size_t)tp.y[k] * t.w + tp.x[k]) + c0;
         for (int c = 0; c < nc; ++c)
-            if (g[c] != 0.0f) atomicAdd(at + c, (double)(tp.w[k] * g[c]));
+            if (g[c] != 0.0f) atomicAdd(at + c, tp.w[k] * g[c]);
+    }
+}
+
+// Lanes of the warp that pass the same key sum their n values; one lane per key adds
+// the sums to base[0..n).
+FM_D void warp_add_by_key(int key, const float* v, int n, float* base)
+{
+    const unsigned peers = __match_any_sync(__activemask(), key);
+    const int leader = __ffs(peers) - 1;
+    for (int i = 0; i < n; ++i) {
+        float sum = 0.0f;
+        for (unsigned m = peers; m; m &= m - 1u) sum += __shfl_sync(peers, v[i], __ffs(m) - 1);
+        if ((int)(threadIdx.x & 31) == leader && sum != 0.0f) atomicAdd(base + i, sum);
     }
 }
 
@@ -195,33 +220,35 @@ FM_D void scatter_params(const WfState& st, const DevScene& S, int mat, float u,
     const DevMaterial& M = S.materials[mat];
     const int which[3] = {MP_BASECOLOR, MP_METALLIC, MP_ROUGHNESS};
     const int first[3] = {0, 3, 4}, count[3] = {3, 1, 1}, chan[3] = {0, 2, 1};
+    float cst[kGradParams] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    bool any_cst = false;
     for (int k = 0; k < 3; ++k) {
         const float* gg = g + first[k];
+        const TexRef& r = M.p[which[k]];
+        if (r.tex < 0) {
+            for (int c = 0; c < count[k]; ++c) cst[first[k] + c] = gg[c];
+            any_cst = true;
+            continue;
+        }
         bool any = false;
         for (int c = 0; c < count[k]; ++c) any = any || gg[c] != 0.0f;
-        if (!any) continue;
-        const TexRef& r = M.p[which[k]];
-        if (r.tex >= 0) {
-            double* tg = st.tex_grad ? st.tex_grad[r.tex] : nullptr;
-            if (tg) tex_scatter(S.textures[r.tex], tg, u, v, chan[k], count[k], gg);
-        } else if (st.mat_grad) {
-            for (int c = 0; c < count[k]; ++c)
-                if (gg[c] != 0.0f) atomicAdd(st.mat_grad + (size_t)mat * kGradParams + first[k] + c, (double)gg[c]);
-        }
+        float* acc = st.tex_acc ? st.tex_acc[r.tex] : nullptr;
+        if (any && acc) tex_scatter(S.textures[r.tex], acc, u, v, chan[k], count[k], gg);
     }
+    if (any_cst && st.mat_acc) warp_add_by_key(mat, cst, kGradParams, st.mat_acc + (size_t)mat * kGradParams);
 }
 
 // Scatters e (per channel, before the env factor) to the env texels seen along `dir`.
 FM_D void scatter_env(const WfState& st, const DevScene& S, f3 dir, f3 e)
 {
-    if (!st.tex_grad || S.env_light < 0) return;
+    if (!st.tex_acc || S.env_light < 0) return;
     const DevEnv& E = S.env;
-    double* tg = st.tex_grad[E.tex];
-    if (!tg) return;
+    float* acc = st.tex_acc[E.tex];
+    if (!acc) return;
     float u, v, th;
     spherical_uv(xf_vec(E.w2l, dir), u, v, th);
     const float g[3] = {e.x * E.factor, e.y * E.factor, e.z * E.factor};
-    tex_scatter(S.textures[E.tex], tg, u, v, 0, 3, g);
+    tex_scatter(S.textures[E.tex], acc, u, v, 0, 3, g);
 }
 
 // Texel (i, j) of the env map that holds direction `dir` and its luminance (the cell
@@ -246,18 +273,54 @@ FM_D bool env_texel(const DevScene& S, f3 dir, int& i, int& j, float& lumt)
 // density: divided by the map's sum) and spread over the texels after the render.
 FM_D void scatter_env_score(const WfState& st, const DevScene& S, f3 dir, float s, bool per_row)
 {
-    if (s == 0.0f || !st.tex_grad || S.env_light < 0) return;
-    double* tg = st.tex_grad[S.env.tex];
-    if (!tg) return;
+    if (s == 0.0f || !st.tex_acc || S.env_light < 0) return;
+    float* acc = st.tex_acc[S.env.tex];
+    if (!acc) return;
     int i, j;
     float lumt;
     if (!env_texel(S, dir, i, j, lumt)) return;
-    double* at = tg + 3 * ((size_t)j * S.env.w + i);
+    float* at = grad_copy(acc, S.textures[S.env.tex]) + 3 * ((size_t)j * S.env.w + i);
     const float k = s / lumt;
-    atomicAdd(at, (double)(0.2126f * k));
-    atomicAdd(at + 1, (double)(0.7152f * k));
-    atomicAdd(at + 2, (double)(0.0722f * k));
-    atomicAdd(per_row ? st.env_row + j : st.env_total, (double)s);
+    atomicAdd(at, 0.2126f * k);
+    atomicAdd(at + 1, 0.7152f * k);
+    atomicAdd(at + 2, 0.0722f * k);
+    // one FP64 add per warp and target
+    const int key = per_row ? j : -1;
+    const unsigned peers = __match_any_sync(__activemask(), key);
+    double sum = 0.0;
+    for (unsigned m = peers; m; m &= m - 1u) sum += (double)__shfl_sync(peers, s, __ffs(m) - 1);
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(per_row ? st.env_row + j : st.env_total, sum);
+}
+
+// Adds the vertex gradient record of `slot` (NEE / MIS parts collected in vg, plus the
+// continuation part dLoss/dI * R . dlw with R the radiance still to come after that
+// vertex) to its material's parameters, and clears the record.
+FM_D void flush_vertex(const WfState& st, const DevScene& S, int slot, f3 wr)
+{
+    float4* D = st.dfr + 5 * (size_t)slot;
+    const float4 d3 = D[3];
+    const int mat = __float_as_int(d3.w);
+    if (mat < 0) return;
+    const float4 d0 = D[0], d1 = D[1], d2 = D[2], d4 = D[4];
+    const float4 v0 = st.vg[2 * (size_t)slot], v1 = st.vg[2 * (size_t)slot + 1];
+    const float dl[15] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w, d2.x, d2.y, d2.z, d2.w, d3.x, d3.y, d3.z};
+    const float vg[kGradParams] = {v0.x, v0.y, v0.z, v0.w, v1.x};
+    float g[kGradParams];
+    bool any = false;
+    for (int i = 0; i < kGradParams; ++i) {
+        g[i] = vg[i] + wr.x * dl[i] + wr.y * dl[5 + i] + wr.z * dl[10 + i];
+        any = any || g[i] != 0.0f;
+    }
+    D[3] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+    if (any) scatter_params(st, S, mat, d4.x, d4.y, g);
+}
+
+// NEE / MIS gradient of the slot's current vertex, once the ray's outcome is known.
+FM_D void add_vertex_grad(const WfState& st, int slot, const float* g)
+{
+    float* v = reinterpret_cast<float*>(st.vg + 2 * (size_t)slot);
+    for (int i = 0; i < kGradParams; ++i)
+        if (g[i] != 0.0f) atomicAdd(v + i, g[i]);
 }
 
 __global__ void k_wf_prep(WfState st)
@@ -271,153 +334,214 @@ __global__ void k_wf_prep(WfState st)
     st.qc[kQcActive] = 0;
     st.qc[kQcDisney] = 0;
     st.qc[kQcSimple] = 0;
+    st.qc[kQcTraceNext] = 0;
 }
 
+// Ray kinds of the trace kernel's combined index space [cont | MIS | shadow].
+constexpr int kRayCont = 0, kRayMis = 1, kRayShadow = 2;
+
+// Sets up the traversal of ray `idx` of the combined index space.
+FM_D int begin_ray(const WfState& st, int64_t idx, int64_t nc, int64_t nm, Traversal& t, const DevScene*& Sp)
+{
+    if (idx < nc) {
+        const int slot = st.cont_q[idx];
+        Sp = st.views[st.view[slot]].scene;
+        const float4 o4 = st.ro[slot], d4 = st.rd[slot];
+        trav_begin(t, trace_scene(*Sp), f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, 0.0f, kRealMax, false);
+        return kRayCont;
+    }
+    if (idx < nc + nm) {
+        const int64_t q = idx - nc;
+        const float4 o4 = st.mis_o[q], d4 = st.mis_d[q];
+        Sp = st.views[__float_as_int(st.mis_a[q].w)].scene;
+        trav_begin(t, trace_scene(*Sp), f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, 0.0f, kRealMax, false);
+        return kRayMis;
+    }
+    const int64_t q = idx - nc - nm;
+    const float4 o4 = st.sh_o[q], d4 = st.sh_d[q];
+    Sp = st.views[__float_as_int(st.sh_c[q].w)].scene;
+    trav_begin(t, trace_scene(*Sp), f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, kEps, o4.w, true);
+    return kRayShadow;
+}
+
+// A continuation ray's result: route the slot to the shading queue of the hit's material
+// class; a miss or a first-bounce emitter hit ends the path here.
+template <bool ADJ>
+FM_D void finish_cont(const WfState& st, int64_t idx, const DevScene& S, const Hit& h)
+{
+    const int cslot = st.cont_q[idx];
+    const float4 o4 = st.ro[cslot], d4 = st.rd[cslot];
+    const f3 o = f3{o4.x, o4.y, o4.z}, d = f3{d4.x, d4.y, d4.z};
+    const int cflags = st.flags[cslot];
+    const int depth = cflags >> 8;
+    int cls = -1;
+    if (h.prim < 0) {
+        // the camera ray's beta is 1
+        if (depth == 1 && S.env_light >= 0) {
+            acc_add(&st.acc[cslot], env_radiance(S, d));
+            if (ADJ && (cflags & kReplay)) scatter_env(st, S, d, pixel_delta(st, cslot, st.views[st.view[cslot]]));
+        }
+    } else {
+        const int obj = __ldg(S.prim_obj + h.prim);
+        const int li = depth == 1 ? __ldg(S.obj_light + obj) : -1;
+        if (li >= 0) {
+            const HitInfo lh = make_hit(S, o, d, h);
+            if (dot(lh.ng, lh.wo) > 0) acc_add(&st.acc[cslot], ld3(S.lights[li].radiance));
+        } else {
+            st.hit[cslot] = make_float4(h.t, __int_as_float(h.prim), h.b1, h.b2);
+            cls = material_class(S.materials[__ldg(S.obj_material + obj)].type);
+        }
+    }
+    const int64_t qd = wagg_append(&st.qc[kQcDisney], cls == kClsDisney);
+    if (cls == kClsDisney) st.disney_q[qd] = cslot;
+    const int64_t qs = wagg_append(&st.qc[kQcSimple], cls == kClsSimple);
+    if (cls == kClsSimple) st.simple_q[qs] = cslot;
+}
+
+// An MIS-BSDF ray's result: the emitter (or environment) it reaches, MIS-weighted.
+template <bool ADJ>
+FM_D void finish_mis(const WfState& st, int64_t q, const DevScene& S, const Hit& h)
+{
+    const float4 o4 = st.mis_o[q], d4 = st.mis_d[q], a4 = st.mis_a[q];
+    const int slot = __float_as_int(o4.w);
+    const f3 o = f3{o4.x, o4.y, o4.z}, d = f3{d4.x, d4.y, d4.z}, A = f3{a4.x, a4.y, a4.z};
+    const float pdf = d4.w;   // < 0: delta BSDF sample (no MIS weight)
+    f3 c = mk(0.0f), Le = mk(0.0f);
+    float w = 1.0f;
+    bool env_hit = false;
+    if (h.prim < 0) {
+        if (S.env_light >= 0) {
+            Le = env_radiance(S, d);
+            c = A * Le;
+            if (pdf >= 0.0f) {
+                w = power_heuristic(pdf, env_pdf(S, d));
+                c *= w;
+            }
+            env_hit = true;
+        }
+    } else {
+        const int obj = __ldg(S.prim_obj + h.prim);
+        const int li = __ldg(S.obj_light + obj);
+        if (li >= 0) {
+            const HitInfo lh = make_hit(S, o, d, h);
+            const f3 l2s = normalize(o - lh.pos);
+            const DevLight& L = S.lights[li];
+            const f3 rad = dot(lh.ng, l2s) > 0 ? ld3(L.radiance) : mk(0.0f);
+            if (length(rad) >= kEpsPdf) {
+                Le = rad;
+                c = A * rad;
+                if (pdf >= 0.0f) {
+                    w = power_heuristic(pdf, area_light_pdf(S, L, o, lh.pos, lh.ng, l2s));
+                    c *= w;
+                }
+            }
+        }
+    }
+    if (c.x == 0.0f && c.y == 0.0f && c.z == 0.0f) return;
+    acc_add(&st.acc[slot], c);
+    if (ADJ) {
+        const float4* P = st.mis_g + 8 * q;
+        const float4 p3 = P[3], p4 = P[4], p5 = P[5];
+        const int mat = __float_as_int(p3.w);
+        const f3 e = f3{p4.z, p4.w, p5.x};
+        // sum_c dLoss/dc_c * c_c (e = dLoss/dI * A, c = A Le w)
+        const float ec = e.x * Le.x * w + e.y * Le.y * w + e.z * Le.z * w;
+        if (mat >= 0) {
+            const float4 p0 = P[0], p1 = P[1], p2 = P[2], p6 = P[6], p7 = P[7];
+            const float B[15] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w,
+                                 p2.x, p2.y, p2.z, p2.w, p3.x, p3.y, p3.z};
+            const float a[kGradParams] = {p5.y, p5.z, p5.w, p6.x, p6.y};
+            const float b[kGradParams] = {p6.z, p6.w, p7.x, p7.y, p7.z};
+            const f3 u3 = Le * w;
+            const float wl = pdf >= 0.0f ? 1.0f - w : 0.0f;
+            float g[kGradParams];
+            for (int i = 0; i < kGradParams; ++i)
+                g[i] = u3.x * B[i] + u3.y * B[5 + i] + u3.z * B[10 + i] + ec * (a[i] + wl * b[i]);
+            add_vertex_grad(st, slot, g);
+        }
+        if (env_hit && (e.x != 0.0f || e.y != 0.0f || e.z != 0.0f)) {
+            scatter_env(st, S, d, e * w);
+            // MIS weight w_b = pdf_b^2 / (pdf_b^2 + pdf_env^2), pdf_env the reported
+            // (per-row normalised) density
+            if (pdf >= 0.0f) scatter_env_score(st, S, d, -2.0f * (1.0f - w) * ec, true);
+        }
+    }
+}
+
+// A shadow ray's result: the NEE contribution when unoccluded.
+template <bool ADJ>
+FM_D void finish_shadow(const WfState& st, int64_t q, const DevScene& S, const Hit& h)
+{
+    if (h.prim >= 0) return;
+    const float4 d4 = st.sh_d[q], c4 = st.sh_c[q];
+    const int slot = __float_as_int(d4.w);
+    acc_add(&st.acc[slot], f3{c4.x, c4.y, c4.z});
+    if (ADJ) {
+        const float4* P = st.sh_g + 3 * q;
+        const float4 p1 = P[1], p2 = P[2];
+        const int mat = __float_as_int(p1.w);
+        if (mat >= 0) {
+            const float4 p0 = P[0];
+            const float g[kGradParams] = {p0.x, p0.y, p0.z, p0.w, p1.x};
+            add_vertex_grad(st, slot, g);
+        }
+        if (p2.x != 0.0f || p2.y != 0.0f || p2.z != 0.0f) {
+            const f3 dir = f3{d4.x, d4.y, d4.z};
+            scatter_env(st, S, dir, f3{p2.x, p2.y, p2.z});
+            // env NEE: 1 / pdf_sample, its MIS weight and the score of the sampling
+            // density leave 2 (1 - w_l) d log pdf_sample
+            scatter_env_score(st, S, dir, p2.w, false);
+        }
+    }
+}
+
+// Traces every queued ray: continuation rays (closest hit), MIS-BSDF rays (closest hit,
+// resolved against emitters and the environment) and shadow rays (occlusion).  Warps
+// are persistent over the combined index space: a lane whose query completes takes the
+// next unclaimed ray (one atomic per warp and refill), so lanes do not idle while the
+// warp's slowest traversal finishes.
 template <bool ADJ>
 __global__ void __launch_bounds__(256) k_wf_trace(WfState st)
 {
     const int64_t nc = st.qc[kQcTraceCont], nm = st.qc[kQcTraceMis], ns = st.qc[kQcTraceShadow];
     const int64_t total = nc + nm + ns;
     unsigned long long n_closest = 0, n_shadow = 0;
-    for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < total; i0 += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = i0 + threadIdx.x;
-        // continuation rays: trace, then route the slot to the shading queue of the hit's
-        // material class; a miss or a first-bounce emitter hit ends the path here
-        int cls = -1;
-        int cslot = 0;
-        if (i < nc) {
-            cslot = st.cont_q[i];
-            const WfView& V = st.views[st.view[cslot]];
-            const DevScene& S = *V.scene;
-            const float4 o4 = st.ro[cslot], d4 = st.rd[cslot];
-            const f3 o = f3{o4.x, o4.y, o4.z}, d = f3{d4.x, d4.y, d4.z};
-            const int cflags = st.flags[cslot];
-            const int depth = cflags >> 8;
-            Hit h;
-            const bool hit = trace_ray<false>(S, o, d, 0.0f, kRealMax, h, st.status);
-            ++n_closest;
-            if (!hit) {
-                // the camera ray's beta is 1
-                if (depth == 1 && S.env_light >= 0) {
-                    acc_add(&st.acc[cslot], env_radiance(S, d));
-                    if (ADJ && (cflags & kReplay)) scatter_env(st, S, d, pixel_delta(st, cslot, V));
-                }
-            } else {
-                const int obj = __ldg(S.prim_obj + h.prim);
-                const int li = depth == 1 ? __ldg(S.obj_light + obj) : -1;
-                if (li >= 0) {
-                    const HitInfo lh = make_hit(S, o, d, h);
-                    if (dot(lh.ng, lh.wo) > 0) acc_add(&st.acc[cslot], ld3(S.lights[li].radiance));
-                } else {
-                    st.hit[cslot] = make_float4(h.t, __int_as_float(h.prim), h.b1, h.b2);
-                    cls = material_class(S.materials[__ldg(S.obj_material + obj)].type);
-                }
+    uint2 stack[kTraversalStack];
+    Traversal t;
+    const DevScene* Sp = nullptr;
+    int kind = -1;   // ray kind held by this lane, -1 for none
+    int64_t idx = 0;
+    bool exhausted = false;
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        const bool need = kind < 0 && !exhausted;
+        const unsigned m = __ballot_sync(0xffffffffu, need);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            unsigned base = 0;
+            if (lane == leader) base = atomicAdd(&st.qc[kQcTraceNext], (unsigned)__popc(m));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (need) {
+                idx = (int64_t)base + __popc(m & lanemask_lt());
+                if (idx >= total)
+                    exhausted = true;
+                else
+                    kind = begin_ray(st, idx, nc, nm, t, Sp);
             }
         }
-        {
-            const int64_t qd = wagg_append(&st.qc[kQcDisney], cls == kClsDisney);
-            if (cls == kClsDisney) st.disney_q[qd] = cslot;
-            const int64_t qs = wagg_append(&st.qc[kQcSimple], cls == kClsSimple);
-            if (cls == kClsSimple) st.simple_q[qs] = cslot;
-        }
-        if (i >= total || i < nc) {
-        } else if (i < nc + nm) {
-            const int64_t q = i - nc;
-            const float4 o4 = st.mis_o[q], d4 = st.mis_d[q], a4 = st.mis_a[q];
-            const int slot = __float_as_int(o4.w);
-            const DevScene& S = *st.views[__float_as_int(a4.w)].scene;
-            const f3 o = f3{o4.x, o4.y, o4.z}, d = f3{d4.x, d4.y, d4.z}, A = f3{a4.x, a4.y, a4.z};
-            const float pdf = d4.w;   // < 0: delta BSDF sample (no MIS weight)
-            Hit h;
-            ++n_closest;
-            f3 c = mk(0.0f), Le = mk(0.0f);
-            float w = 1.0f;
-            bool env_hit = false;
-            if (!trace_ray<false>(S, o, d, 0.0f, kRealMax, h, st.status)) {
-                if (S.env_light >= 0) {
-                    Le = env_radiance(S, d);
-                    c = A * Le;
-                    if (pdf >= 0.0f) {
-                        w = power_heuristic(pdf, env_pdf(S, d));
-                        c *= w;
-                    }
-                    env_hit = true;
-                }
+        if (__ballot_sync(0xffffffffu, kind >= 0) == 0) break;
+        if (kind >= 0 && trav_step(t, trace_scene(*Sp), stack, st.status)) {
+            if (kind == kRayCont) {
+                ++n_closest;
+                finish_cont<ADJ>(st, idx, *Sp, t.hit);
+            } else if (kind == kRayMis) {
+                ++n_closest;
+                finish_mis<ADJ>(st, idx - nc, *Sp, t.hit);
             } else {
-                const int obj = __ldg(S.prim_obj + h.prim);
-                const int li = __ldg(S.obj_light + obj);
-                if (li >= 0) {
-                    const HitInfo lh = make_hit(S, o, d, h);
-                    const f3 l2s = normalize(o - lh.pos);
-                    const DevLight& L = S.lights[li];
-                    const f3 rad = dot(lh.ng, l2s) > 0 ? ld3(L.radiance) : mk(0.0f);
-                    if (length(rad) >= kEpsPdf) {
-                        Le = rad;
-                        c = A * rad;
-                        if (pdf >= 0.0f) {
-                            w = power_heuristic(pdf, area_light_pdf(S, L, o, lh.pos, lh.ng, l2s));
-                            c *= w;
-                        }
-                    }
-                }
+                ++n_shadow;
+                finish_shadow<ADJ>(st, idx - nc - nm, *Sp, t.hit);
             }
-            if (c.x != 0.0f || c.y != 0.0f || c.z != 0.0f) {
-                acc_add(&st.acc[slot], c);
-                if (ADJ) {
-                    const float4* P = st.mis_g + 8 * q;
-                    const float4 p3 = P[3], p4 = P[4], p5 = P[5];
-                    const int mat = __float_as_int(p3.w);
-                    const f3 e = f3{p4.z, p4.w, p5.x};
-                    // sum_c dLoss/dc_c * c_c (e = dLoss/dI * A, c = A Le w)
-                    const float ec = e.x * Le.x * w + e.y * Le.y * w + e.z * Le.z * w;
-                    if (mat >= 0) {
-                        const float4 p0 = P[0], p1 = P[1], p2 = P[2], p6 = P[6], p7 = P[7];
-                        const float B[15] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w,
-                                             p2.x, p2.y, p2.z, p2.w, p3.x, p3.y, p3.z};
-                        const float a[kGradParams] = {p5.y, p5.z, p5.w, p6.x, p6.y};
-                        const float b[kGradParams] = {p6.z, p6.w, p7.x, p7.y, p7.z};
-                        const f3 u3 = Le * w;
-                        const float wl = pdf >= 0.0f ? 1.0f - w : 0.0f;
-                        float g[kGradParams];
-                        for (int i = 0; i < kGradParams; ++i)
-                            g[i] = u3.x * B[i] + u3.y * B[5 + i] + u3.z * B[10 + i] + ec * (a[i] + wl * b[i]);
-                        scatter_params(st, S, mat, p4.x, p4.y, g);
-                    }
-                    if (env_hit && (e.x != 0.0f || e.y != 0.0f || e.z != 0.0f)) {
-                        scatter_env(st, S, d, e * w);
-                        // MIS weight w_b = pdf_b^2 / (pdf_b^2 + pdf_env^2), pdf_env the
-                        // reported (per-row normalised) density
-                        if (pdf >= 0.0f) scatter_env_score(st, S, d, -2.0f * (1.0f - w) * ec, true);
-                    }
-                }
-            }
-        } else {
-            const int64_t q = i - nc - nm;
-            const float4 o4 = st.sh_o[q], d4 = st.sh_d[q], c4 = st.sh_c[q];
-            const int slot = __float_as_int(d4.w);
-            const DevScene& S = *st.views[__float_as_int(c4.w)].scene;
-            Hit h;
-            ++n_shadow;
-            if (!trace_ray<true>(S, f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, kEps, o4.w, h, st.status)) {
-                acc_add(&st.acc[slot], f3{c4.x, c4.y, c4.z});
-                if (ADJ) {
-                    const float4* P = st.sh_g + 3 * q;
-                    const float4 p1 = P[1], p2 = P[2];
-                    const int mat = __float_as_int(p1.w);
-                    if (mat >= 0) {
-                        const float4 p0 = P[0];
-                        const float g[kGradParams] = {p0.x, p0.y, p0.z, p0.w, p1.x};
-                        scatter_params(st, S, mat, p1.y, p1.z, g);
-                    }
-                    if (p2.x != 0.0f || p2.y != 0.0f || p2.z != 0.0f) {
-                        const f3 dir = f3{d4.x, d4.y, d4.z};
-                        scatter_env(st, S, dir, f3{p2.x, p2.y, p2.z});
-                        // env NEE: 1 / pdf_sample, its MIS weight and the score of the
-                        // sampling density leave 2 (1 - w_l) d log pdf_sample
-                        scatter_env_score(st, S, dir, p2.w, false);
-                    }
-                }
-            }
+            kind = -1;
         }
     }
     // per-warp counter aggregation
@@ -425,7 +549,7 @@ __global__ void __launch_bounds__(256) k_wf_trace(WfState st)
         n_closest += __shfl_xor_sync(0xffffffffu, n_closest, off);
         n_shadow += __shfl_xor_sync(0xffffffffu, n_shadow, off);
     }
-    if ((threadIdx.x & 31) == 0 && (n_closest | n_shadow)) {
+    if (lane == 0 && (n_closest | n_shadow)) {
         atomicAdd(&st.cnt->closest, n_closest);
         atomicAdd(&st.cnt->shadow, n_shadow);
     }
@@ -520,21 +644,17 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfState st)
             if (ADJ && replay) {
                 delta = pixel_delta(st, slot, V);
                 tgt = grad_target(S, h);
-                // the previous vertex's continuation gradient: L - C_<=k-1 is known now
-                const float4* D = st.dfr + 5 * (size_t)slot;
-                const float4 d3 = D[3];
-                const int dmat = __float_as_int(d3.w);
-                if (dmat >= 0) {
-                    const float4 a4 = st.acc[slot], c4 = st.col[slot], l4 = st.lp[slot];
-                    const f3 R = f3{l4.x - (c4.x + a4.x), l4.y - (c4.y + a4.y), l4.z - (c4.z + a4.z)};
-                    const f3 wr = delta * R;
-                    const float4 d0 = D[0], d1 = D[1], d2 = D[2], d4 = D[4];
-                    const float dl[15] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w,
-                                          d2.x, d2.y, d2.z, d2.w, d3.x, d3.y, d3.z};
-                    float g[kGradParams];
-                    for (int i = 0; i < kGradParams; ++i) g[i] = wr.x * dl[i] + wr.y * dl[5 + i] + wr.z * dl[10 + i];
-                    scatter_params(st, S, dmat, d4.x, d4.y, g);
-                }
+                // the previous vertex's record: its NEE / MIS rays are resolved and the
+                // radiance after it, L - C_<=k-1, is known now
+                const float4 a4 = st.acc[slot], c4 = st.col[slot], l4 = st.lp[slot];
+                const f3 R = f3{l4.x - (c4.x + a4.x), l4.y - (c4.y + a4.y), l4.z - (c4.z + a4.z)};
+                flush_vertex(st, S, slot, delta * R);
+                // this vertex's record: target now, continuation part below
+                float4* D = st.dfr + 5 * (size_t)slot;
+                D[0] = D[1] = D[2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                D[3] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(tgt));
+                D[4] = make_float4(h.u, h.v, 0.0f, 0.0f);
+                st.vg[2 * (size_t)slot] = st.vg[2 * (size_t)slot + 1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             }
             if (depth == 1 && !replay) {
                 const f3 al = bsdf_albedo(b);
@@ -673,8 +793,9 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfState st)
                         flags = kNextCont | (flags & (kPending | kReplay)) | ((depth + 1) << 8);
                         enqueue_cont = true;
                         if (ADJ && replay) {
-                            // d log f / dp at the continuation direction, consumed at the
-                            // next shaded vertex
+                            // d log (f / pdf_b) / dp at the continuation direction (and the
+                            // score of the sampler's density), used when the vertex's
+                            // record is flushed
                             float4* D = st.dfr + 5 * (size_t)slot;
                             if (tgt >= 0) {
                                 const DV3 fd = bsdf_f_grad<CLS>(b, h.wo, sc.wi);
@@ -690,9 +811,6 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfState st)
                                 D[1] = make_float4(dl[4], dl[5], dl[6], dl[7]);
                                 D[2] = make_float4(dl[8], dl[9], dl[10], dl[11]);
                                 D[3] = make_float4(dl[12], dl[13], dl[14], __int_as_float(tgt));
-                                D[4] = make_float4(h.u, h.v, 0.0f, 0.0f);
-                            } else {
-                                D[3] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
                             }
                         }
                     }
@@ -755,6 +873,12 @@ __global__ void __launch_bounds__(256) k_wf_logic(WfState st)
             } else {
                 const int vid = st.view[slot];
                 const WfView& V = st.views[vid];
+                if (ADJ) {
+                    // the last vertex's record (its NEE / MIS rays are resolved)
+                    const float4 l4 = st.lp[slot];
+                    const f3 R = f3{l4.x - col.x, l4.y - col.y, l4.z - col.z};
+                    flush_vertex(st, *V.scene, slot, pixel_delta(st, slot, V) * R);
+                }
                 ++n_paths;
                 if (!isfinite(col.x) || !isfinite(col.y) || !isfinite(col.z)) ++n_nans;
                 float4 sum = st.isum[slot], cmp = st.icomp[slot];
@@ -953,10 +1077,11 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
     if (ADJ) {
         A(st.lp, pool);
         A(st.dfr, 5 * (size_t)pool);
+        A(st.vg, 2 * (size_t)pool);
         A(st.sh_g, 3 * (size_t)st.cap_sh);
         A(st.mis_g, 8 * (size_t)st.cap_mis);
-        st.tex_grad = adj->tex_grad;
-        st.mat_grad = adj->mat_grad;
+        st.tex_acc = adj->tex_acc;
+        st.mat_acc = adj->mat_acc;
         st.env_row = adj->env_row;
         st.env_total = adj->env_total;
     }
