@@ -342,9 +342,9 @@ def main():
     alg_bytes = totals["closest"] * closest_b + totals["shadow"] * shadow_b
     peak, peak_kind = measured_peak_hbm()
     achieved = alg_bytes / (totals["trace_ms"] / 1e3) / 1e9 if totals["trace_ms"] > 0 else None
-    # five launches per wavefront iteration (prep, trace, two shade kernels, logic) plus
-    # one init and one reduce per view per step
-    launches_trace = max(1, (totals["launches"] - args.steps * (1 + len(specs))) // 5)
+    # six launches per wavefront iteration (prep, trace, resolve, two shade kernels,
+    # logic) plus one init and one reduce per view per step
+    launches_trace = max(1, (totals["launches"] - args.steps * (1 + len(specs))) // 6)
     traffic = None
     if TRACE_DRAM_BYTES_PER_RAY is not None:
         traffic = TRACE_DRAM_BYTES_PER_RAY * (totals["closest"] + totals["shadow"]) / launches_trace

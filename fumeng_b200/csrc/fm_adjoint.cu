@@ -149,16 +149,25 @@ extern "C" fm_status fm_render_adjoint(fm_ctx* ctx, const fm_scene* scene, int32
                             "render_adjoint");
             }
         }
-        // FP32 accumulators the kernels add to (kGradCopies per texture)
+        // FP32 accumulators the kernels add to: 8 copies of a texture, more for small
+        // ones (up to about 8M floats, at most 256 copies)
         std::vector<float*> facc((size_t)nt, nullptr);
         std::vector<size_t> tex_n((size_t)nt, 0);
+        std::vector<int32_t> copies((size_t)(nt > 0 ? nt : 1), 1);
         for (int t = 0; t < nt; ++t) {
             if (!dtex[t]) continue;
             tex_n[t] = (size_t)scene->textures[t].w * scene->textures[t].h * 3;
-            facc[t] = a.get<float>(tex_n[t] * kGradCopies);
+            int k = 8;
+            while (k < 256 && (size_t)(2 * k) * tex_n[t] <= ((size_t)8 << 20)) k *= 2;
+            copies[t] = k;
+            facc[t] = a.get<float>(tex_n[t] * k);
             if (!facc[t]) return oom();
-            FM_CUDA_TRY(ctx, cudaMemsetAsync(facc[t], 0, tex_n[t] * kGradCopies * sizeof(float), s), "render_adjoint");
+            FM_CUDA_TRY(ctx, cudaMemsetAsync(facc[t], 0, tex_n[t] * k * sizeof(float), s), "render_adjoint");
         }
+        int32_t* d_copies = a.get<int32_t>(copies.size());
+        if (!d_copies) return oom();
+        FM_CUDA_TRY(ctx, cudaMemcpyAsync(d_copies, copies.data(), sizeof(int32_t) * copies.size(), cudaMemcpyHostToDevice, s),
+                    "render_adjoint");
         float* macc = nullptr;
         if (dmat) {
             macc = a.get<float>((size_t)nm * kGradParams);
@@ -212,14 +221,14 @@ extern "C" fm_status fm_render_adjoint(fm_ctx* ctx, const fm_scene* scene, int32
             env_total = env_row + eh;
             FM_CUDA_TRY(ctx, cudaMemsetAsync(env_row, 0, sizeof(double) * (eh + 1), s), "render_adjoint");
         }
-        WfAdjoint adj{d_tex_arr, macc, env_row, env_total};
+        WfAdjoint adj{d_tex_arr, d_copies, macc, env_row, env_total};
         WfTuning wt;
         wt.profile = (flags & FM_FLAG_PROFILE) != 0;
         result = wavefront_adjoint(ctx, views, wt, adj, d_cnt, &tm);
         if (result == FM_OK) {
             const int grid = ctx->num_sms * 8;
             for (int t = 0; t < nt; ++t)
-                if (facc[t]) k_grad_reduce<<<grid, 256, 0, s>>>(facc[t], kGradCopies, tex_n[t], dtex[t]);
+                if (facc[t]) k_grad_reduce<<<grid, 256, 0, s>>>(facc[t], copies[t], tex_n[t], dtex[t]);
             if (macc) k_grad_reduce<<<grid, 256, 0, s>>>(macc, 1, (size_t)nm * kGradParams, dmat);
             const cudaError_t e = cudaGetLastError();
             if (e != cudaSuccess) result = cuda_error(ctx, e, "render_adjoint reduce");

@@ -103,9 +103,8 @@ FM_D DV3 dsg_fakess(const Disney& d, const DisneyG& g, f3 wo, f3 wi)
 }
 
 // disney_f on dual numbers; wo, wi in the shading frame
-FM_D DV3 disney_f_grad(const Disney& d, f3 wo, f3 wi)
+FM_D DV3 disney_f_grad(const Disney& d, const DisneyG& g, f3 wo, f3 wi)
 {
-    const DisneyG g = disney_grad_setup(d);
     DV3 r = dv3_zero();
     if (wo.z * wi.z < 0) {
         if (d.thin) {
@@ -124,24 +123,6 @@ FM_D DV3 disney_f_grad(const Disney& d, f3 wo, f3 wi)
     r = r + dsg_spec(d, g, wo, wi);
     if (d.clearcoat > 0.0f) r = r + ds_cc_eval(d, wo, wi);
     return r;
-}
-
-// bsdf_f with derivatives.  Lambert: f = basecolor / pi; conductor and dielectric have
-// no differentiated parameters (and a zero non-delta value).
-template <int CLS = kClsAny>
-FM_D DV3 bsdf_f_grad(const Bsdf& b, f3 wo_w, f3 wi_w)
-{
-    if (CLS != kClsDisney) {
-        if (b.type == 0) {
-            DV3 r = dv3(b.color * kInvPi);
-            r.x.d[GP_BASE_R] = kInvPi;
-            r.y.d[GP_BASE_G] = kInvPi;
-            r.z.d[GP_BASE_B] = kInvPi;
-            return r;
-        }
-        if (b.type == 1 || b.type == 2 || CLS == kClsSimple) return dv3_zero();
-    }
-    return disney_f_grad(b.d, to_local(b, wo_w), to_local(b, wi_w));
 }
 
 // ---- sampling densities ---------------------------------------------------------------
@@ -202,9 +183,8 @@ struct PdfQ {
 };
 
 // disney_pdf and the sampler's density at wi, with derivatives (wo, wi local).
-FM_D PdfQ disney_pdfs_grad(const Disney& d, f3 wo, f3 wi)
+FM_D PdfQ disney_pdfs_grad(const Disney& d, const DisneyG& g, f3 wo, f3 wi)
 {
-    const DisneyG g = disney_grad_setup(d);
     const DisneyWG w = disney_weights_grad(d, g, wo.z);
     const D5 zero = dconst<kGradParams>(0.0f);
     PdfQ r;
@@ -250,18 +230,46 @@ FM_D PdfQ disney_pdfs_grad(const Disney& d, f3 wo, f3 wi)
     return r;
 }
 
-// d log p / dp_i and d log q / dp_i - d log p / dp_i at wi for the BSDF's class.
-template <int CLS>
-FM_D void pdf_log_derivs(const Bsdf& b, f3 wo_w, f3 wi_w, float dlogp[kGradParams], float dscore[kGradParams])
+// Everything the adjoint needs at one sampled direction, from one parameter set-up:
+// df/dp per channel, d log pdf_b/dp (pdf_b the density the reference's Pdf reports)
+// and d log q/dp - d log pdf_b/dp (q the sampler's density).
+struct BsdfGrads {
+    DV3 f;
+    float dlogp[kGradParams];
+    float dscore[kGradParams];
+};
+
+// Not inlined: the replay shading kernel calls it for every NEE, MIS and continuation
+// direction, and one copy keeps its code and register use down.
+static __device__ __noinline__ void disney_grads(const Disney& d, f3 wo, f3 wi, BsdfGrads* out)
 {
-    for (int i = 0; i < kGradParams; ++i) dlogp[i] = dscore[i] = 0.0f;
-    if (CLS == kClsSimple || (CLS == kClsAny && b.type != 3)) return;
-    const PdfQ pq = disney_pdfs_grad(b.d, to_local(b, wo_w), to_local(b, wi_w));
-    if (!(pq.p.v > 0.0f) || !(pq.q.v > 0.0f)) return;
+    const DisneyG g = disney_grad_setup(d);
+    out->f = disney_f_grad(d, g, wo, wi);
+    const PdfQ pq = disney_pdfs_grad(d, g, wo, wi);
+    const bool ok = pq.p.v > 0.0f && pq.q.v > 0.0f;
     for (int i = 0; i < kGradParams; ++i) {
-        dlogp[i] = pq.p.d[i] / pq.p.v;
-        dscore[i] = pq.q.d[i] / pq.q.v - dlogp[i];
+        out->dlogp[i] = ok ? pq.p.d[i] / pq.p.v : 0.0f;
+        out->dscore[i] = ok ? pq.q.d[i] / pq.q.v - out->dlogp[i] : 0.0f;
     }
+}
+
+// bsdf_f with derivatives, and the density terms (zero where the sampler draws the
+// reported density).  Lambert: f = basecolor / pi; conductor and dielectric have no
+// differentiated parameters (and a zero non-delta value).
+template <int CLS = kClsAny>
+FM_D void bsdf_grads(const Bsdf& b, f3 wo_w, f3 wi_w, BsdfGrads& out)
+{
+    if (CLS != kClsDisney && (b.type != 3 || CLS == kClsSimple)) {
+        out.f = b.type == 0 ? dv3(b.color * kInvPi) : dv3_zero();
+        if (b.type == 0) {
+            out.f.x.d[GP_BASE_R] = kInvPi;
+            out.f.y.d[GP_BASE_G] = kInvPi;
+            out.f.z.d[GP_BASE_B] = kInvPi;
+        }
+        for (int i = 0; i < kGradParams; ++i) out.dlogp[i] = out.dscore[i] = 0.0f;
+        return;
+    }
+    disney_grads(b.d, to_local(b, wo_w), to_local(b, wi_w), &out);
 }
 
 // sum_c w_c * dF_c / dp_i for the five parameters

@@ -936,23 +936,23 @@ int bvh_build(cudaStream_t stream, const PrimSource& src, BvhResult& out, std::s
     FM_BUILD_CHECK(cudaEventCreate(&ev0));
     FM_BUILD_CHECK(cudaEventCreate(&ev1));
     FM_BUILD_CHECK(cudaEventRecord(ev0, stream));
-    FM_BUILD_CHECK(cudaMalloc(&plo, sizeof(float4) * n));
-    FM_BUILD_CHECK(cudaMalloc(&phi, sizeof(float4) * n));
-    FM_BUILD_CHECK(cudaMalloc(&pidx, sizeof(int32_t) * n));
-    FM_BUILD_CHECK(cudaMalloc(&pidx2, sizeof(int32_t) * n));
-    FM_BUILD_CHECK(cudaMalloc(&pos_task, sizeof(int32_t) * n));
-    FM_BUILD_CHECK(cudaMalloc(&pos_task2, sizeof(int32_t) * n));
-    FM_BUILD_CHECK(cudaMalloc(&flags, sizeof(int32_t) * n));
-    FM_BUILD_CHECK(cudaMalloc(&scan, sizeof(int32_t) * (n + 1)));
-    FM_BUILD_CHECK(cudaMalloc(&tile_sums, sizeof(int32_t) * (ntiles + 1)));
-    FM_BUILD_CHECK(cudaMalloc(&small_list, sizeof(int32_t) * 3 * (n + 1)));
-    FM_BUILD_CHECK(cudaMalloc(&counters, sizeof(int32_t) * 8));
-    FM_BUILD_CHECK(cudaMalloc(&rb, sizeof(uint32_t) * 12));
-    FM_BUILD_CHECK(cudaMalloc(&bnodes, sizeof(BNode) * max_nodes));
-    FM_BUILD_CHECK(cudaMalloc(&tasks, sizeof(Task) * max_tasks));
-    FM_BUILD_CHECK(cudaMalloc(&tasks2, sizeof(Task) * max_tasks));
-    FM_BUILD_CHECK(cudaMalloc(&splits, sizeof(Split) * max_tasks));
-    FM_BUILD_CHECK(cudaMalloc(&bins, sizeof(Bins) * max_tasks));
+    FM_BUILD_CHECK(cudaMallocAsync(&plo, sizeof(float4) * n, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&phi, sizeof(float4) * n, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&pidx, sizeof(int32_t) * n, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&pidx2, sizeof(int32_t) * n, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&pos_task, sizeof(int32_t) * n, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&pos_task2, sizeof(int32_t) * n, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&flags, sizeof(int32_t) * n, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&scan, sizeof(int32_t) * (n + 1), stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&tile_sums, sizeof(int32_t) * (ntiles + 1), stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&small_list, sizeof(int32_t) * 3 * (n + 1), stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&counters, sizeof(int32_t) * 8, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&rb, sizeof(uint32_t) * 12, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&bnodes, sizeof(BNode) * max_nodes, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&tasks, sizeof(Task) * max_tasks, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&tasks2, sizeof(Task) * max_tasks, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&splits, sizeof(Split) * max_tasks, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&bins, sizeof(Bins) * max_tasks, stream));
 
     k_prim_bounds<<<grid_for(n, 256), 256, 0, stream>>>(src, plo, phi);
     {
@@ -1001,10 +1001,10 @@ int bvh_build(cudaStream_t stream, const PrimSource& src, BvhResult& out, std::s
     FM_BUILD_CHECK(cudaGetLastError());
 
     // Collapse.  Wide node count <= binary internal nodes; leaf slots == n.
-    FM_BUILD_CHECK(cudaMalloc(&out.nodes, sizeof(uint4) * 5 * (size_t)(n + 1)));
-    FM_BUILD_CHECK(cudaMalloc(&leaf_prim, sizeof(int32_t) * n));
-    FM_BUILD_CHECK(cudaMalloc(&front, sizeof(int2) * (n + 1)));
-    FM_BUILD_CHECK(cudaMalloc(&front2, sizeof(int2) * (n + 1)));
+    FM_BUILD_CHECK(cudaMallocAsync(&out.nodes, sizeof(uint4) * 5 * (size_t)(n + 1), stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&leaf_prim, sizeof(int32_t) * n, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&front, sizeof(int2) * (n + 1), stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&front2, sizeof(int2) * (n + 1), stream));
     {
         const int2 r0 = make_int2(0, 0);
         FM_BUILD_CHECK(cudaMemcpyAsync(front, &r0, sizeof(int2), cudaMemcpyHostToDevice, stream));
@@ -1034,7 +1034,7 @@ int bvh_build(cudaStream_t stream, const PrimSource& src, BvhResult& out, std::s
         err = "bvh build: tree deeper than the traversal stack";
         goto fail;
     }
-    FM_BUILD_CHECK(cudaMalloc(&out.leaf, sizeof(float4) * 3 * (size_t)n));
+    FM_BUILD_CHECK(cudaMallocAsync(&out.leaf, sizeof(float4) * 3 * (size_t)n, stream));
     k_fill_leaf<<<grid_for(n, 256), 256, 0, stream>>>(leaf_prim, n, src, out.leaf);
     FM_BUILD_CHECK(cudaGetLastError());
     FM_BUILD_CHECK(cudaEventRecord(ev1, stream));
@@ -1047,53 +1047,53 @@ int bvh_build(cudaStream_t stream, const PrimSource& src, BvhResult& out, std::s
     out.num_nodes = nwide;
     out.num_leaf = nleaf;
     out.depth = depth;
-    cudaFree(plo);
-    cudaFree(phi);
-    cudaFree(pidx);
-    cudaFree(pidx2);
-    cudaFree(pos_task);
-    cudaFree(pos_task2);
-    cudaFree(flags);
-    cudaFree(scan);
-    cudaFree(tile_sums);
-    cudaFree(small_list);
-    cudaFree(counters);
-    cudaFree(rb);
-    cudaFree(bnodes);
-    cudaFree(tasks);
-    cudaFree(tasks2);
-    cudaFree(splits);
-    cudaFree(bins);
-    cudaFree(front);
-    cudaFree(front2);
-    cudaFree(leaf_prim);
+    cudaFreeAsync(plo, stream);
+    cudaFreeAsync(phi, stream);
+    cudaFreeAsync(pidx, stream);
+    cudaFreeAsync(pidx2, stream);
+    cudaFreeAsync(pos_task, stream);
+    cudaFreeAsync(pos_task2, stream);
+    cudaFreeAsync(flags, stream);
+    cudaFreeAsync(scan, stream);
+    cudaFreeAsync(tile_sums, stream);
+    cudaFreeAsync(small_list, stream);
+    cudaFreeAsync(counters, stream);
+    cudaFreeAsync(rb, stream);
+    cudaFreeAsync(bnodes, stream);
+    cudaFreeAsync(tasks, stream);
+    cudaFreeAsync(tasks2, stream);
+    cudaFreeAsync(splits, stream);
+    cudaFreeAsync(bins, stream);
+    cudaFreeAsync(front, stream);
+    cudaFreeAsync(front2, stream);
+    cudaFreeAsync(leaf_prim, stream);
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
     return 0;
 fail:
     cudaStreamSynchronize(stream);
-    cudaFree(plo);
-    cudaFree(phi);
-    cudaFree(pidx);
-    cudaFree(pidx2);
-    cudaFree(pos_task);
-    cudaFree(pos_task2);
-    cudaFree(flags);
-    cudaFree(scan);
-    cudaFree(tile_sums);
-    cudaFree(small_list);
-    cudaFree(counters);
-    cudaFree(rb);
-    cudaFree(bnodes);
-    cudaFree(tasks);
-    cudaFree(tasks2);
-    cudaFree(splits);
-    cudaFree(bins);
-    cudaFree(front);
-    cudaFree(front2);
-    cudaFree(leaf_prim);
-    cudaFree(out.nodes);
-    cudaFree(out.leaf);
+    cudaFreeAsync(plo, stream);
+    cudaFreeAsync(phi, stream);
+    cudaFreeAsync(pidx, stream);
+    cudaFreeAsync(pidx2, stream);
+    cudaFreeAsync(pos_task, stream);
+    cudaFreeAsync(pos_task2, stream);
+    cudaFreeAsync(flags, stream);
+    cudaFreeAsync(scan, stream);
+    cudaFreeAsync(tile_sums, stream);
+    cudaFreeAsync(small_list, stream);
+    cudaFreeAsync(counters, stream);
+    cudaFreeAsync(rb, stream);
+    cudaFreeAsync(bnodes, stream);
+    cudaFreeAsync(tasks, stream);
+    cudaFreeAsync(tasks2, stream);
+    cudaFreeAsync(splits, stream);
+    cudaFreeAsync(bins, stream);
+    cudaFreeAsync(front, stream);
+    cudaFreeAsync(front2, stream);
+    cudaFreeAsync(leaf_prim, stream);
+    cudaFreeAsync(out.nodes, stream);
+    cudaFreeAsync(out.leaf, stream);
     out = BvhResult{};
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);

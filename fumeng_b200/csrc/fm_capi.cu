@@ -17,8 +17,9 @@ fm_status upload(fm_ctx* ctx, fm_scene* sc, const T* host, size_t count, const T
     *dev_out = nullptr;
     if (!host || count == 0) return FM_OK;
     void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, sizeof(T) * count);
-    if (e != cudaSuccess) return set_error(ctx, FM_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    // stream-ordered allocation from the device's memory pool: no device-wide sync
+    cudaError_t e = cudaMallocAsync(&p, sizeof(T) * count, ctx->stream);
+    if (e != cudaSuccess) return set_error(ctx, FM_ERR_OOM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
     sc->allocations.push_back(p);
     e = cudaMemcpyAsync(p, host, sizeof(T) * count, cudaMemcpyHostToDevice, ctx->stream);
     if (e != cudaSuccess) return cuda_error(ctx, e, "upload");
@@ -200,6 +201,14 @@ fm_status fm_ctx_create(int device, fm_ctx** out)
         return FM_ERR_CUDA;
     }
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+    // Scenes, BVH builds and renders allocate from the device's default memory pool with
+    // stream-ordered calls; keeping freed blocks in the pool makes creating and
+    // destroying scenes cheap (no release to the driver at every synchronisation).
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     *out = ctx;
     return FM_OK;
 }
@@ -474,7 +483,7 @@ fm_status fm_scene_create(fm_ctx* ctx, const fm_scene_desc* d, fm_scene** out)
         S.num_nodes = sc->bvh.num_nodes;
         S.num_leaf = sc->bvh.num_leaf;
         void* dd = nullptr;
-        FM_CUDA_TRY(ctx, cudaMalloc(&dd, sizeof(DevScene)), "scene alloc");
+        FM_CUDA_TRY(ctx, cudaMallocAsync(&dd, sizeof(DevScene), ctx->stream), "scene alloc");
         sc->allocations.push_back(dd);
         sc->d_dev = static_cast<DevScene*>(dd);
         FM_CUDA_TRY(ctx, cudaMemcpyAsync(dd, &S, sizeof(DevScene), cudaMemcpyHostToDevice, ctx->stream), "scene copy");
@@ -484,8 +493,8 @@ fm_status fm_scene_create(fm_ctx* ctx, const fm_scene_desc* d, fm_scene** out)
     *out = sc;
     return FM_OK;
 fail:
+    for (void* p : sc->allocations) cudaFreeAsync(p, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
-    for (void* p : sc->allocations) cudaFree(p);
     delete sc;
     return st;
 }
@@ -495,8 +504,8 @@ fm_status fm_scene_destroy(fm_ctx* ctx, fm_scene* sc)
     if (!ctx) return FM_ERR_INVALID;
     if (!sc) return FM_OK;
     cudaSetDevice(ctx->device);
+    for (void* p : sc->allocations) cudaFreeAsync(p, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
-    for (void* p : sc->allocations) cudaFree(p);
     delete sc;
     return FM_OK;
 }

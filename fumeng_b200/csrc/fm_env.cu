@@ -201,24 +201,24 @@ fm_status env_build_tables(fm_ctx* ctx, fm_scene* scene, const DevTexture& tex, 
         marg_prob = const_cast<float*>(env.marg_prob);
         marg_alias = const_cast<int32_t*>(env.marg_alias);
     } else {
-        FM_CUDA_TRY(ctx, cudaMalloc(&pdf_sample, n * sizeof(float)), "env tables");
+        FM_CUDA_TRY(ctx, cudaMallocAsync(&pdf_sample, n * sizeof(float), ctx->stream), "env tables");
         track(pdf_sample);
-        FM_CUDA_TRY(ctx, cudaMalloc(&pdf_eval, n * sizeof(float)), "env tables");
+        FM_CUDA_TRY(ctx, cudaMallocAsync(&pdf_eval, n * sizeof(float), ctx->stream), "env tables");
         track(pdf_eval);
-        FM_CUDA_TRY(ctx, cudaMalloc(&row_prob, n * sizeof(float)), "env tables");
+        FM_CUDA_TRY(ctx, cudaMallocAsync(&row_prob, n * sizeof(float), ctx->stream), "env tables");
         track(row_prob);
-        FM_CUDA_TRY(ctx, cudaMalloc(&row_alias, n * sizeof(int32_t)), "env tables");
+        FM_CUDA_TRY(ctx, cudaMallocAsync(&row_alias, n * sizeof(int32_t), ctx->stream), "env tables");
         track(row_alias);
-        FM_CUDA_TRY(ctx, cudaMalloc(&marg_prob, h * sizeof(float)), "env tables");
+        FM_CUDA_TRY(ctx, cudaMallocAsync(&marg_prob, h * sizeof(float), ctx->stream), "env tables");
         track(marg_prob);
-        FM_CUDA_TRY(ctx, cudaMalloc(&marg_alias, h * sizeof(int32_t)), "env tables");
+        FM_CUDA_TRY(ctx, cudaMallocAsync(&marg_alias, h * sizeof(int32_t), ctx->stream), "env tables");
         track(marg_alias);
     }
     // temporaries
-    FM_CUDA_TRY(ctx, cudaMalloc(&lum, n * sizeof(float)), "env tables");
-    FM_CUDA_TRY(ctx, cudaMalloc(&scratch, 2 * n * sizeof(int32_t)), "env tables");
-    FM_CUDA_TRY(ctx, cudaMalloc(&rowsum, h * sizeof(double)), "env tables");
-    FM_CUDA_TRY(ctx, cudaMalloc(&totals, 2 * sizeof(double)), "env tables");
+    FM_CUDA_TRY(ctx, cudaMallocAsync(&lum, n * sizeof(float), ctx->stream), "env tables");
+    FM_CUDA_TRY(ctx, cudaMallocAsync(&scratch, 2 * n * sizeof(int32_t), ctx->stream), "env tables");
+    FM_CUDA_TRY(ctx, cudaMallocAsync(&rowsum, h * sizeof(double), ctx->stream), "env tables");
+    FM_CUDA_TRY(ctx, cudaMallocAsync(&totals, 2 * sizeof(double), ctx->stream), "env tables");
     cudaStream_t st = ctx->stream;
     k_env_lum<<<(int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096), 256, 0, st>>>(tex, w, h, lum);
     k_env_rowsum<<<h, 256, 0, st>>>(lum, w, rowsum);
@@ -227,11 +227,11 @@ fm_status env_build_tables(fm_ctx* ctx, fm_scene* scene, const DevTexture& tex, 
                                                                                        pdf_sample, pdf_eval);
     k_env_alias_rows<<<(h + 63) / 64, 64, 0, st>>>(lum, w, h, row_prob, row_alias, scratch);
     k_env_alias_marg<<<1, 1, 0, st>>>(rowsum, h, marg_prob, marg_alias, scratch);
+    cudaFreeAsync(lum, st);
+    cudaFreeAsync(scratch, st);
+    cudaFreeAsync(rowsum, st);
+    cudaFreeAsync(totals, st);
     cudaError_t e = cudaStreamSynchronize(st);
-    cudaFree(lum);
-    cudaFree(scratch);
-    cudaFree(rowsum);
-    cudaFree(totals);
     if (e != cudaSuccess) return cuda_error(ctx, e, "env tables");
     FM_CUDA_TRY(ctx, cudaGetLastError(), "env tables");
     env.w = w;

@@ -25,9 +25,9 @@ struct WfView {
 };
 
 // Gradient accumulators of an adjoint render (device buffers, zeroed by the caller).
-constexpr int kGradCopies = 4;   // FP32 copies of each texture's accumulator
 struct WfAdjoint {
-    float* const* tex_acc;     // device array over the scene's textures: NULL or kGradCopies x w*h*3
+    float* const* tex_acc;     // device array over the scene's textures: NULL or tex_copies[t] x w*h*3
+    const int32_t* tex_copies; // device array: FP32 copies per texture
     float* mat_acc;            // num_materials * 5 (basecolor rgb, metallic, roughness) or NULL
     double* env_row;           // env map height doubles, zeroed (score sums per row)
     double* env_total;         // one double, zeroed

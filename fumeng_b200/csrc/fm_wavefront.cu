@@ -1,21 +1,23 @@
-// Wavefront path tracer: a pool of path slots advanced one bounce per iteration by
-// three kernels (prep, trace, shade), replayed from a CUDA graph until every work item
-// is done.  Works on any number of views (one view = one camera over one scene), which
-// is how a batch of scenes renders in one launch.
+// Wavefront path tracer: a pool of path slots advanced one bounce per iteration by a
+// fixed sequence of kernels, replayed from a CUDA graph until every work item is done.
+// Works on any number of views (one view = one camera over one scene), which is how a
+// batch of scenes renders in one launch.
 //
-// One iteration is five launches: prep (swap queue counters), trace, shade for Disney
+// One iteration is six launches: prep (swap queue counters), trace (traversal only),
+// resolve (emission, MIS and NEE contributions; shading queues), shade for Disney
 // surfaces, shade for the other materials, logic (finish samples, start new ones).
+// Adjoint renders add the two shading kernels of replayed vertices.
 // Ray queues (filled by the shade and logic kernels, consumed by the next trace):
 //   cont    slot ids whose continuation ray is in the slot's ray registers
 //   mis     MIS-BSDF rays (origin|slot, direction|pdf, weight|view)
 //   shadow  NEE shadow rays (origin|t_max, direction|slot, contribution|view)
-// Shading queues (filled by the trace kernel, consumed by the shade kernels):
+// Shading queues (filled by the resolve kernel, consumed by the shade kernels):
 //   disney / simple   slot ids whose continuation ray hit a surface of that class
 // Entries are appended with warp-aggregated atomics (one atomic per warp and queue:
 // ballot, popcount, prefix), so each queue is dense and its float4 records are read
-// coalesced.  The trace kernel resolves MIS and shadow rays itself, and the emission a
-// continuation ray sees at the first bounce, by adding their contribution to the
-// slot's accumulator; the logic kernel folds it into the path.
+// coalesced.  The resolve kernel adds MIS and shadow contributions, and the emission a
+// continuation ray sees at the first bounce, to the slot's accumulator; the logic
+// kernel folds it into the path.
 //
 // Work items are (view, pixel, chunk of `chunk` consecutive samples).  A slot runs its
 // item's samples one after another with Kahan-compensated sums and writes the item's
@@ -41,11 +43,12 @@ constexpr int kPending = 2;
 // adjoint renders: the slot is replaying its sample's path (second pass)
 constexpr int kReplay = 4;
 // queue counters: the three ray queues being filled for the next trace, the same three
-// being traced, slots still holding work, the two shading queues, and the trace
-// kernel's next unclaimed ray
+// being traced, slots still holding work, the shading queues (two classes, and in
+// adjoint renders two more for replayed vertices) and the trace kernel's next
+// unclaimed ray
 constexpr int kQcCont = 0, kQcMis = 1, kQcShadow = 2;
 constexpr int kQcTraceCont = 3, kQcTraceMis = 4, kQcTraceShadow = 5;
-constexpr int kQcActive = 6, kQcDisney = 7, kQcSimple = 8, kQcTraceNext = 9;
+constexpr int kQcActive = 6, kQcDisney = 7, kQcSimple = 8, kQcTraceNext = 9, kQcDisneyR = 10, kQcSimpleR = 11;
 constexpr int kQcCount = 16;
 
 struct WfState {
@@ -74,12 +77,16 @@ struct WfState {
     int32_t* cont_q;
     int32_t* disney_q;    // slots whose continuation ray hit a Disney surface
     int32_t* simple_q;    // ... a Lambert, conductor or dielectric surface
+    int32_t* disney_r;    // adjoint renders: the same for slots replaying their path
+    int32_t* simple_r;
     float4* mis_o;
     float4* mis_d;
     float4* mis_a;
     float4* sh_o;
     float4* sh_d;
     float4* sh_c;
+    float4* mis_h;        // trace results: MIS ray hits (t, prim, b1, b2)
+    uint32_t* sh_h;       // ... shadow ray occluded (1) or not (0)
     int64_t cap_cont, cap_mis, cap_sh;
     unsigned* qc;         // kQc* counters
     Counters* cnt;
@@ -90,7 +97,8 @@ struct WfState {
     float4* vg;           // [2 per slot] gradient collected for that vertex (g[5]; NEE / MIS, trace kernel)
     float4* sh_g;         // [3 per shadow ray] g[5], u, v, material, env weight e[3], env score s
     float4* mis_g;        // [8 per MIS ray] B[15] (c*5+i), material, u, v, e[3], a[5], b[5]
-    float* const* tex_acc;     // per scene texture: NULL or kGradCopies x w*h*3 FP32 accumulators
+    float* const* tex_acc;     // per scene texture: NULL or tex_copies[t] x w*h*3 FP32 accumulators
+    const int32_t* tex_copies;
     float* mat_acc;            // num_materials * 5 FP32 accumulators, or NULL
     double* env_row;           // env importance: per-row and global score sums (see scatter_env_score)
     double* env_total;
@@ -167,25 +175,43 @@ FM_D f3 pixel_delta(const WfState& st, int slot, const WfView& V)
     return f3{__ldg(d) * inv, __ldg(d + 1) * inv, __ldg(d + 2) * inv};
 }
 
-// Texel gradients are accumulated in FP32 (reductions with no return value) in
-// kGradCopies copies, a block writing to copy blockIdx % kGradCopies, which spreads the
-// updates neighbouring pixels make to the same texel; the copies are summed in FP64
-// after the render (fm_adjoint.cu).
-FM_D float* grad_copy(float* acc, const DevTexture& t)
+// Texel gradients are accumulated in FP32 (reductions with no return value) in several
+// copies per texture (more for small textures, whose texels are hit more often), a
+// block writing to copy blockIdx % copies, which spreads the updates that concurrent
+// blocks make to the same texel; the copies are summed in FP64 after the render
+// (fm_adjoint.cu).
+FM_D float* grad_copy(const WfState& st, int tex, const DevTexture& t)
 {
-    return acc + (size_t)(blockIdx.x % kGradCopies) * ((size_t)t.w * t.h * 3);
+    const int copies = st.tex_copies[tex];
+    return st.tex_acc[tex] + (size_t)(blockIdx.x % copies) * ((size_t)t.w * t.h * 3);
+}
+
+// Sum of v over the lanes in `peers` (which must all be active and call this together).
+FM_D float peer_sum(unsigned peers, float v)
+{
+    float sum = 0.0f;
+    for (unsigned m = peers; m; m &= m - 1u) sum += __shfl_sync(peers, v, __ffs(m) - 1);
+    return sum;
 }
 
 // Adds g[c] * (weight of each tap) to channel c0 + c of the taps tex_sample reads.
-FM_D void tex_scatter(const DevTexture& t, float* acc, float u, float v, int c0, int nc, const float* g)
+// Neighbouring pixels often read the same taps; lanes of the warp whose taps coincide
+// (same accumulator, texture and first tap, hence the same four taps) add their values
+// together first, and one lane issues the reductions.
+FM_D void tex_scatter(const WfState& st, int tex, const DevTexture& t, float u, float v, int c0, int nc,
+                      const float* g)
 {
     const TexTaps tp = tex_taps(t, u, v);
-    float* base = grad_copy(acc, t);
+    float* base = grad_copy(st, tex, t);
+    float* first = base + 3 * ((size_t)tp.y[0] * t.w + tp.x[0]) + c0;
+    const unsigned peers = __match_any_sync(__activemask(), (unsigned long long)(uintptr_t)first);
+    const bool leader = (int)(threadIdx.x & 31) == __ffs(peers) - 1;
     for (int k = 0; k < tp.n; ++k) {
-        if (tp.w[k] == 0.0f) continue;
         float* at = base + 3 * ((size_t)tp.y[k] * t.w + tp.x[k]) + c0;
-        for (int c = 0; c < nc; ++c)
-            if (g[c] != 0.0f) atomicAdd(at + c, tp.w[k] * g[c]);
+        for (int c = 0; c < nc; ++c) {
+            const float sum = peer_sum(peers, tp.w[k] * g[c]);
+            if (leader && sum != 0.0f) atomicAdd(at + c, sum);
+        }
     }
 }
 
@@ -232,8 +258,7 @@ FM_D void scatter_params(const WfState& st, const DevScene& S, int mat, float u,
         }
         bool any = false;
         for (int c = 0; c < count[k]; ++c) any = any || gg[c] != 0.0f;
-        float* acc = st.tex_acc ? st.tex_acc[r.tex] : nullptr;
-        if (any && acc) tex_scatter(S.textures[r.tex], acc, u, v, chan[k], count[k], gg);
+        if (any && st.tex_acc && st.tex_acc[r.tex]) tex_scatter(st, r.tex, S.textures[r.tex], u, v, chan[k], count[k], gg);
     }
     if (any_cst && st.mat_acc) warp_add_by_key(mat, cst, kGradParams, st.mat_acc + (size_t)mat * kGradParams);
 }
@@ -243,12 +268,11 @@ FM_D void scatter_env(const WfState& st, const DevScene& S, f3 dir, f3 e)
 {
     if (!st.tex_acc || S.env_light < 0) return;
     const DevEnv& E = S.env;
-    float* acc = st.tex_acc[E.tex];
-    if (!acc) return;
+    if (!st.tex_acc[E.tex]) return;
     float u, v, th;
     spherical_uv(xf_vec(E.w2l, dir), u, v, th);
     const float g[3] = {e.x * E.factor, e.y * E.factor, e.z * E.factor};
-    tex_scatter(S.textures[E.tex], acc, u, v, 0, 3, g);
+    tex_scatter(st, E.tex, S.textures[E.tex], u, v, 0, 3, g);
 }
 
 // Texel (i, j) of the env map that holds direction `dir` and its luminance (the cell
@@ -274,16 +298,18 @@ FM_D bool env_texel(const DevScene& S, f3 dir, int& i, int& j, float& lumt)
 FM_D void scatter_env_score(const WfState& st, const DevScene& S, f3 dir, float s, bool per_row)
 {
     if (s == 0.0f || !st.tex_acc || S.env_light < 0) return;
-    float* acc = st.tex_acc[S.env.tex];
-    if (!acc) return;
+    if (!st.tex_acc[S.env.tex]) return;
     int i, j;
     float lumt;
     if (!env_texel(S, dir, i, j, lumt)) return;
-    float* at = grad_copy(acc, S.textures[S.env.tex]) + 3 * ((size_t)j * S.env.w + i);
-    const float k = s / lumt;
-    atomicAdd(at, 0.2126f * k);
-    atomicAdd(at + 1, 0.7152f * k);
-    atomicAdd(at + 2, 0.0722f * k);
+    float* at = grad_copy(st, S.env.tex, S.textures[S.env.tex]) + 3 * ((size_t)j * S.env.w + i);
+    const unsigned tpeers = __match_any_sync(__activemask(), (unsigned long long)(uintptr_t)at);
+    const float k = peer_sum(tpeers, s / lumt);
+    if ((int)(threadIdx.x & 31) == __ffs(tpeers) - 1) {
+        atomicAdd(at, 0.2126f * k);
+        atomicAdd(at + 1, 0.7152f * k);
+        atomicAdd(at + 2, 0.0722f * k);
+    }
     // one FP64 add per warp and target
     const int key = per_row ? j : -1;
     const unsigned peers = __match_any_sync(__activemask(), key);
@@ -334,6 +360,8 @@ __global__ void k_wf_prep(WfState st)
     st.qc[kQcActive] = 0;
     st.qc[kQcDisney] = 0;
     st.qc[kQcSimple] = 0;
+    st.qc[kQcDisneyR] = 0;
+    st.qc[kQcSimpleR] = 0;
     st.qc[kQcTraceNext] = 0;
 }
 
@@ -388,14 +416,23 @@ FM_D void finish_cont(const WfState& st, int64_t idx, const DevScene& S, const H
             const HitInfo lh = make_hit(S, o, d, h);
             if (dot(lh.ng, lh.wo) > 0) acc_add(&st.acc[cslot], ld3(S.lights[li].radiance));
         } else {
-            st.hit[cslot] = make_float4(h.t, __int_as_float(h.prim), h.b1, h.b2);
             cls = material_class(S.materials[__ldg(S.obj_material + obj)].type);
         }
     }
-    const int64_t qd = wagg_append(&st.qc[kQcDisney], cls == kClsDisney);
-    if (cls == kClsDisney) st.disney_q[qd] = cslot;
-    const int64_t qs = wagg_append(&st.qc[kQcSimple], cls == kClsSimple);
-    if (cls == kClsSimple) st.simple_q[qs] = cslot;
+    // replayed vertices of an adjoint render go to their own queues, so that primal
+    // vertices run in the forward shading kernels
+    // (one warp-aggregated append per queue: all lanes take part in each)
+    const bool rep = ADJ && (cflags & kReplay);
+    const int64_t qd = wagg_append(&st.qc[kQcDisney], cls == kClsDisney && !rep);
+    if (cls == kClsDisney && !rep) st.disney_q[qd] = cslot;
+    const int64_t qs = wagg_append(&st.qc[kQcSimple], cls == kClsSimple && !rep);
+    if (cls == kClsSimple && !rep) st.simple_q[qs] = cslot;
+    if (ADJ) {
+        const int64_t rd = wagg_append(&st.qc[kQcDisneyR], cls == kClsDisney && rep);
+        if (cls == kClsDisney && rep) st.disney_r[rd] = cslot;
+        const int64_t rs = wagg_append(&st.qc[kQcSimpleR], cls == kClsSimple && rep);
+        if (cls == kClsSimple && rep) st.simple_r[rs] = cslot;
+    }
 }
 
 // An MIS-BSDF ray's result: the emitter (or environment) it reaches, MIS-weighted.
@@ -439,7 +476,8 @@ FM_D void finish_mis(const WfState& st, int64_t q, const DevScene& S, const Hit&
     }
     if (c.x == 0.0f && c.y == 0.0f && c.z == 0.0f) return;
     acc_add(&st.acc[slot], c);
-    if (ADJ) {
+    // only rays of replayed vertices carry a gradient payload
+    if (ADJ && (st.flags[slot] & kReplay)) {
         const float4* P = st.mis_g + 8 * q;
         const float4 p3 = P[3], p4 = P[4], p5 = P[5];
         const int mat = __float_as_int(p3.w);
@@ -476,7 +514,7 @@ FM_D void finish_shadow(const WfState& st, int64_t q, const DevScene& S, const H
     const float4 d4 = st.sh_d[q], c4 = st.sh_c[q];
     const int slot = __float_as_int(d4.w);
     acc_add(&st.acc[slot], f3{c4.x, c4.y, c4.z});
-    if (ADJ) {
+    if (ADJ && (st.flags[slot] & kReplay)) {
         const float4* P = st.sh_g + 3 * q;
         const float4 p1 = P[1], p2 = P[2];
         const int mat = __float_as_int(p1.w);
@@ -495,17 +533,16 @@ FM_D void finish_shadow(const WfState& st, int64_t q, const DevScene& S, const H
     }
 }
 
-// Traces every queued ray: continuation rays (closest hit), MIS-BSDF rays (closest hit,
-// resolved against emitters and the environment) and shadow rays (occlusion).  Warps
-// are persistent over the combined index space: a lane whose query completes takes the
-// next unclaimed ray (one atomic per warp and refill), so lanes do not idle while the
-// warp's slowest traversal finishes.
-template <bool ADJ>
+// Traces every queued ray: continuation rays (closest hit), MIS-BSDF rays (closest hit)
+// and shadow rays (occlusion), and stores the results; k_wf_resolve turns them into
+// radiance and shading work.  Warps are persistent over the combined index space: a
+// lane whose query completes takes the next unclaimed ray (one atomic per warp and
+// refill), so lanes do not idle while the warp's slowest traversal finishes, and the
+// loop holds nothing but traversal.
 __global__ void __launch_bounds__(256) k_wf_trace(WfState st)
 {
     const int64_t nc = st.qc[kQcTraceCont], nm = st.qc[kQcTraceMis], ns = st.qc[kQcTraceShadow];
     const int64_t total = nc + nm + ns;
-    unsigned long long n_closest = 0, n_shadow = 0;
     uint2 stack[kTraversalStack];
     Traversal t;
     const DevScene* Sp = nullptr;
@@ -531,17 +568,47 @@ __global__ void __launch_bounds__(256) k_wf_trace(WfState st)
         }
         if (__ballot_sync(0xffffffffu, kind >= 0) == 0) break;
         if (kind >= 0 && trav_step(t, trace_scene(*Sp), stack, st.status)) {
-            if (kind == kRayCont) {
-                ++n_closest;
-                finish_cont<ADJ>(st, idx, *Sp, t.hit);
-            } else if (kind == kRayMis) {
-                ++n_closest;
-                finish_mis<ADJ>(st, idx - nc, *Sp, t.hit);
-            } else {
-                ++n_shadow;
-                finish_shadow<ADJ>(st, idx - nc - nm, *Sp, t.hit);
-            }
+            const Hit& h = t.hit;
+            if (kind == kRayCont)
+                st.hit[st.cont_q[idx]] = make_float4(h.t, __int_as_float(h.prim), h.b1, h.b2);
+            else if (kind == kRayMis)
+                st.mis_h[idx - nc] = make_float4(h.t, __int_as_float(h.prim), h.b1, h.b2);
+            else
+                st.sh_h[idx - nc - nm] = h.prim >= 0 ? 1u : 0u;
             kind = -1;
+        }
+    }
+}
+
+// Turns the trace results into radiance (emission, MIS and NEE contributions added to
+// the slots' accumulators, and their gradients in adjoint renders) and fills the
+// shading queues, over the same combined index space as k_wf_trace.
+template <bool ADJ>
+__global__ void __launch_bounds__(256) k_wf_resolve(WfState st)
+{
+    const int64_t nc = st.qc[kQcTraceCont], nm = st.qc[kQcTraceMis], ns = st.qc[kQcTraceShadow];
+    const int64_t total = nc + nm + ns;
+    unsigned long long n_closest = 0, n_shadow = 0;
+    for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < total; i0 += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = i0 + threadIdx.x;
+        if (i >= total) continue;
+        if (i < nc) {
+            ++n_closest;
+            const int slot = st.cont_q[i];
+            const float4 h4 = st.hit[slot];
+            finish_cont<ADJ>(st, i, *st.views[st.view[slot]].scene,
+                             Hit{h4.x, __float_as_int(h4.y), h4.z, h4.w});
+        } else if (i < nc + nm) {
+            ++n_closest;
+            const int64_t q = i - nc;
+            const float4 h4 = st.mis_h[q];
+            finish_mis<ADJ>(st, q, *st.views[__float_as_int(st.mis_a[q].w)].scene,
+                            Hit{h4.x, __float_as_int(h4.y), h4.z, h4.w});
+        } else {
+            ++n_shadow;
+            const int64_t q = i - nc - nm;
+            if (st.sh_h[q] == 0u)
+                finish_shadow<ADJ>(st, q, *st.views[__float_as_int(st.sh_c[q].w)].scene, Hit{0.0f, -1, 0.0f, 0.0f});
         }
     }
     // per-warp counter aggregation
@@ -549,7 +616,7 @@ __global__ void __launch_bounds__(256) k_wf_trace(WfState st)
         n_closest += __shfl_xor_sync(0xffffffffu, n_closest, off);
         n_shadow += __shfl_xor_sync(0xffffffffu, n_shadow, off);
     }
-    if (lane == 0 && (n_closest | n_shadow)) {
+    if ((threadIdx.x & 31) == 0 && (n_closest | n_shadow)) {
         atomicAdd(&st.cnt->closest, n_closest);
         atomicAdd(&st.cnt->shadow, n_shadow);
     }
@@ -608,8 +675,9 @@ FM_D void start_sample(const WfState& st, int slot, const WfView& V, int64_t ite
 template <int CLS, bool ADJ>
 __global__ void __launch_bounds__(256) k_wf_shade(WfState st)
 {
-    const int64_t n = st.qc[CLS == kClsDisney ? kQcDisney : kQcSimple];
-    const int32_t* queue = CLS == kClsDisney ? st.disney_q : st.simple_q;
+    // ADJ: the replayed vertices of an adjoint render; otherwise forward (or primal) ones
+    const int64_t n = st.qc[CLS == kClsDisney ? (ADJ ? kQcDisneyR : kQcDisney) : (ADJ ? kQcSimpleR : kQcSimple)];
+    const int32_t* queue = CLS == kClsDisney ? (ADJ ? st.disney_r : st.disney_q) : (ADJ ? st.simple_r : st.simple_q);
     unsigned long long n_bounces = 0;
     for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = i0 + threadIdx.x;
@@ -623,7 +691,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfState st)
             const DevScene& S = *V.scene;
             const int flags0 = st.flags[slot];
             const int depth = flags0 >> 8;
-            const bool replay = ADJ && (flags0 & kReplay);
+            const bool replay = ADJ;
             int flags = (depth << 8) | (flags0 & kReplay);
             const float4 h4 = st.hit[slot];
             const float4 o4 = st.ro[slot], d4 = st.rd[slot];
@@ -698,12 +766,11 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfState st)
                                     const float dc = dot(delta, c);   // sum_c dLoss/dc_c * c_c
                                     float g[kGradParams] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
                                     if (tgt >= 0) {
-                                        contract(bsdf_f_grad<CLS>(b, h.wo, ls.wi), delta * base * ls.radiance, g);
-                                        if (!ls.delta) {
-                                            float dlogp[kGradParams], dscore[kGradParams];
-                                            pdf_log_derivs<CLS>(b, h.wo, ls.wi, dlogp, dscore);
-                                            for (int i = 0; i < kGradParams; ++i) g[i] -= 2.0f * (1.0f - mis) * dc * dlogp[i];
-                                        }
+                                        BsdfGrads bg;
+                                        bsdf_grads<CLS>(b, h.wo, ls.wi, bg);
+                                        contract(bg.f, delta * base * ls.radiance, g);
+                                        if (!ls.delta)
+                                            for (int i = 0; i < kGradParams; ++i) g[i] -= 2.0f * (1.0f - mis) * dc * bg.dlogp[i];
                                     }
                                     const bool env = L.kind == LK_ENV;
                                     const f3 e = env ? delta * base * f : mk(0.0f);
@@ -711,9 +778,6 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfState st)
                                     P[0] = make_float4(g[0], g[1], g[2], g[3]);
                                     P[1] = make_float4(g[4], h.u, h.v, __int_as_float(tgt));
                                     P[2] = make_float4(e.x, e.y, e.z, senv);
-                                } else {
-                                    P[1] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
-                                    P[2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                                 }
                             }
                             flags |= kPending;
@@ -740,18 +804,19 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfState st)
                                 for (int k = 0; k < 15; ++k) B[k] = 0.0f;
                                 for (int k = 0; k < kGradParams; ++k) a[k] = bb[k] = 0.0f;
                                 if (tgt >= 0) {
-                                    const DV3 fd = bsdf_f_grad<CLS>(b, h.wo, ms.wi);
+                                    BsdfGrads bg;
+                                    bsdf_grads<CLS>(b, h.wo, ms.wi, bg);
                                     const f3 base = delta * beta * (absdot(h.ng, wi) / ms.pdf * inv_dl);
                                     for (int i = 0; i < kGradParams; ++i) {
-                                        B[i] = base.x * fd.x.d[i];
-                                        B[5 + i] = base.y * fd.y.d[i];
-                                        B[10 + i] = base.z * fd.z.d[i];
+                                        B[i] = base.x * bg.f.x.d[i];
+                                        B[5 + i] = base.y * bg.f.y.d[i];
+                                        B[10 + i] = base.z * bg.f.z.d[i];
                                     }
-                                    if (!ms.delta) {
-                                        float dlogp[kGradParams];
-                                        pdf_log_derivs<CLS>(b, h.wo, ms.wi, dlogp, a);
-                                        for (int i = 0; i < kGradParams; ++i) bb[i] = 2.0f * dlogp[i];
-                                    }
+                                    if (!ms.delta)
+                                        for (int i = 0; i < kGradParams; ++i) {
+                                            a[i] = bg.dscore[i];
+                                            bb[i] = 2.0f * bg.dlogp[i];
+                                        }
                                 }
                                 const f3 e = delta * A;
                                 P[0] = make_float4(B[0], B[1], B[2], B[3]);
@@ -762,10 +827,6 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfState st)
                                 P[5] = make_float4(e.z, a[0], a[1], a[2]);
                                 P[6] = make_float4(a[3], a[4], bb[0], bb[1]);
                                 P[7] = make_float4(bb[2], bb[3], bb[4], 0.0f);
-                            } else {
-                                P[3] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
-                                P[4] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                                P[5] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                             }
                         }
                         flags |= kPending;
@@ -798,9 +859,10 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfState st)
                             // record is flushed
                             float4* D = st.dfr + 5 * (size_t)slot;
                             if (tgt >= 0) {
-                                const DV3 fd = bsdf_f_grad<CLS>(b, h.wo, sc.wi);
-                                float dlogp[kGradParams], dscore[kGradParams];
-                                pdf_log_derivs<CLS>(b, h.wo, sc.wi, dlogp, dscore);
+                                BsdfGrads bg;
+                                bsdf_grads<CLS>(b, h.wo, sc.wi, bg);
+                                const DV3& fd = bg.f;
+                                const float* dscore = bg.dscore;
                                 float dl[15];
                                 for (int i = 0; i < kGradParams; ++i) {
                                     dl[i] = fd.x.v > 0.0f ? fd.x.d[i] / fd.x.v + dscore[i] : 0.0f;
@@ -1067,12 +1129,18 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
     A(st.cont_q, st.cap_cont);
     A(st.disney_q, pool);
     A(st.simple_q, pool);
+    if (ADJ) {
+        A(st.disney_r, pool);
+        A(st.simple_r, pool);
+    }
     A(st.mis_o, st.cap_mis);
     A(st.mis_d, st.cap_mis);
     A(st.mis_a, st.cap_mis);
     A(st.sh_o, st.cap_sh);
     A(st.sh_d, st.cap_sh);
     A(st.sh_c, st.cap_sh);
+    A(st.mis_h, st.cap_mis);
+    A(st.sh_h, st.cap_sh);
     A(st.qc, kQcCount);
     if (ADJ) {
         A(st.lp, pool);
@@ -1081,6 +1149,7 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
         A(st.sh_g, 3 * (size_t)st.cap_sh);
         A(st.mis_g, 8 * (size_t)st.cap_mis);
         st.tex_acc = adj->tex_acc;
+        st.tex_copies = adj->tex_copies;
         st.mat_acc = adj->mat_acc;
         st.env_row = adj->env_row;
         st.env_total = adj->env_total;
@@ -1107,6 +1176,7 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
     const int trace_grid = sms * 16;
     const int shade_grid = (int)std::min<int64_t>((pool + tune.shade_block - 1) / tune.shade_block, (int64_t)sms * 32);
     const int logic_grid = (int)std::min<int64_t>((pool + 255) / 256, (int64_t)sms * 32);
+    const int resolve_grid = sms * 16;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     fm_status result = FM_OK;
@@ -1122,10 +1192,15 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
         for (int it = 0; it < tune.iters_per_graph; ++it) {
             k_wf_prep<<<1, 1, 0, s>>>(st);
             if (tune.profile) cudaEventRecordWithFlags(pev[3 * it], s, cudaEventRecordExternal);
-            k_wf_trace<ADJ><<<trace_grid, tune.trace_block, 0, s>>>(st);
+            k_wf_trace<<<trace_grid, tune.trace_block, 0, s>>>(st);
             if (tune.profile) cudaEventRecordWithFlags(pev[3 * it + 1], s, cudaEventRecordExternal);
-            k_wf_shade<kClsDisney, ADJ><<<shade_grid, tune.shade_block, 0, s>>>(st);
-            k_wf_shade<kClsSimple, ADJ><<<shade_grid, tune.shade_block, 0, s>>>(st);
+            k_wf_resolve<ADJ><<<resolve_grid, 256, 0, s>>>(st);
+            k_wf_shade<kClsDisney, false><<<shade_grid, tune.shade_block, 0, s>>>(st);
+            k_wf_shade<kClsSimple, false><<<shade_grid, tune.shade_block, 0, s>>>(st);
+            if (ADJ) {
+                k_wf_shade<kClsDisney, true><<<shade_grid, tune.shade_block, 0, s>>>(st);
+                k_wf_shade<kClsSimple, true><<<shade_grid, tune.shade_block, 0, s>>>(st);
+            }
             k_wf_logic<ADJ><<<logic_grid, 256, 0, s>>>(st);
             if (tune.profile) cudaEventRecordWithFlags(pev[3 * it + 2], s, cudaEventRecordExternal);
         }
@@ -1187,7 +1262,7 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, e0, e1);
     if (times) {
-        times->launches = 1 + graph_launches * 5 * tune.iters_per_graph + (int64_t)views.size();
+        times->launches = 1 + graph_launches * (ADJ ? 8 : 6) * tune.iters_per_graph + (int64_t)views.size();
         times->total_ms = ms;
         times->trace_ms = trace_ms;
         times->shade_ms = shade_ms;
