@@ -241,7 +241,7 @@ struct BsdfGrads {
 
 // Not inlined: the replay shading kernel calls it for every NEE, MIS and continuation
 // direction, and one copy keeps its code and register use down.
-static __device__ __noinline__ void disney_grads(const Disney& d, f3 wo, f3 wi, BsdfGrads* out)
+FM_D void disney_grads(const Disney& d, f3 wo, f3 wi, BsdfGrads* out)
 {
     const DisneyG g = disney_grad_setup(d);
     out->f = disney_f_grad(d, g, wo, wi);

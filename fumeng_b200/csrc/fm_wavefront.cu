@@ -6,7 +6,8 @@
 // One iteration is six launches: prep (swap queue counters), trace (traversal only),
 // resolve (emission, MIS and NEE contributions; shading queues), shade for Disney
 // surfaces, shade for the other materials, logic (finish samples, start new ones).
-// Adjoint renders add the two shading kernels of replayed vertices.
+// Adjoint renders add the two shading kernels of replayed vertices and a kernel that
+// scatters finished vertices' parameter gradients onto texels and material constants.
 // Ray queues (filled by the shade and logic kernels, consumed by the next trace):
 //   cont    slot ids whose continuation ray is in the slot's ray registers
 //   mis     MIS-BSDF rays (origin|slot, direction|pdf, weight|view)
@@ -49,6 +50,7 @@ constexpr int kReplay = 4;
 constexpr int kQcCont = 0, kQcMis = 1, kQcShadow = 2;
 constexpr int kQcTraceCont = 3, kQcTraceMis = 4, kQcTraceShadow = 5;
 constexpr int kQcActive = 6, kQcDisney = 7, kQcSimple = 8, kQcTraceNext = 9, kQcDisneyR = 10, kQcSimpleR = 11;
+constexpr int kQcGrad = 12;
 constexpr int kQcCount = 16;
 
 struct WfState {
@@ -94,7 +96,9 @@ struct WfState {
     // adjoint renders only (null otherwise)
     float4* lp;           // primal radiance of the slot's current sample
     float4* dfr;          // [5 per slot] the slot's current vertex: dlw[15] (c*5+i), material, u, v
-    float4* vg;           // [2 per slot] gradient collected for that vertex (g[5]; NEE / MIS, trace kernel)
+    float4* vg;           // [2 per slot] gradient collected for that vertex (g[5]; NEE / MIS, resolve kernel)
+    float4* gq;           // [3 per entry] finished vertices' gradients: g[5], u, v, material, view
+    int64_t cap_grad;
     float4* sh_g;         // [3 per shadow ray] g[5], u, v, material, env weight e[3], env score s
     float4* mis_g;        // [8 per MIS ray] B[15] (c*5+i), material, u, v, e[3], a[5], b[5]
     float* const* tex_acc;     // per scene texture: NULL or tex_copies[t] x w*h*3 FP32 accumulators
@@ -318,10 +322,12 @@ FM_D void scatter_env_score(const WfState& st, const DevScene& S, f3 dir, float 
     if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(per_row ? st.env_row + j : st.env_total, sum);
 }
 
-// Adds the vertex gradient record of `slot` (NEE / MIS parts collected in vg, plus the
-// continuation part dLoss/dI * R . dlw with R the radiance still to come after that
-// vertex) to its material's parameters, and clears the record.
-FM_D void flush_vertex(const WfState& st, const DevScene& S, int slot, f3 wr)
+// Completes the vertex gradient record of `slot` (NEE / MIS parts collected in vg, plus
+// the continuation part dLoss/dI * R . dlw with R the radiance still to come after that
+// vertex), queues it for k_wf_grad_scatter and clears the record.  The scatter runs in
+// its own small kernel: done here, its tap arithmetic and atomics ran at the low
+// occupancy of the replay shading kernels.
+FM_D void flush_vertex(const WfState& st, int vid, int slot, f3 wr)
 {
     float4* D = st.dfr + 5 * (size_t)slot;
     const float4 d3 = D[3];
@@ -338,7 +344,16 @@ FM_D void flush_vertex(const WfState& st, const DevScene& S, int slot, f3 wr)
         any = any || g[i] != 0.0f;
     }
     D[3] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
-    if (any) scatter_params(st, S, mat, d4.x, d4.y, g);
+    const int64_t q = wagg_append(&st.qc[kQcGrad], any);
+    if (!any) return;
+    if (q < st.cap_grad) {
+        float4* E = st.gq + 3 * q;
+        E[0] = make_float4(g[0], g[1], g[2], g[3]);
+        E[1] = make_float4(g[4], d4.x, d4.y, __int_as_float(mat));
+        E[2] = make_float4(__int_as_float(vid), 0.0f, 0.0f, 0.0f);
+    } else {
+        atomicOr(st.status, 2u);
+    }
 }
 
 // NEE / MIS gradient of the slot's current vertex, once the ray's outcome is known.
@@ -362,6 +377,7 @@ __global__ void k_wf_prep(WfState st)
     st.qc[kQcSimple] = 0;
     st.qc[kQcDisneyR] = 0;
     st.qc[kQcSimpleR] = 0;
+    st.qc[kQcGrad] = 0;
     st.qc[kQcTraceNext] = 0;
 }
 
@@ -716,7 +732,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfState st)
                 // radiance after it, L - C_<=k-1, is known now
                 const float4 a4 = st.acc[slot], c4 = st.col[slot], l4 = st.lp[slot];
                 const f3 R = f3{l4.x - (c4.x + a4.x), l4.y - (c4.y + a4.y), l4.z - (c4.z + a4.z)};
-                flush_vertex(st, S, slot, delta * R);
+                flush_vertex(st, vid, slot, delta * R);
                 // this vertex's record: target now, continuation part below
                 float4* D = st.dfr + 5 * (size_t)slot;
                 D[0] = D[1] = D[2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -939,7 +955,7 @@ __global__ void __launch_bounds__(256) k_wf_logic(WfState st)
                     // the last vertex's record (its NEE / MIS rays are resolved)
                     const float4 l4 = st.lp[slot];
                     const f3 R = f3{l4.x - col.x, l4.y - col.y, l4.z - col.z};
-                    flush_vertex(st, *V.scene, slot, pixel_delta(st, slot, V) * R);
+                    flush_vertex(st, vid, slot, pixel_delta(st, slot, V) * R);
                 }
                 ++n_paths;
                 if (!isfinite(col.x) || !isfinite(col.y) || !isfinite(col.z)) ++n_nans;
@@ -1012,6 +1028,20 @@ __global__ void __launch_bounds__(256) k_wf_logic(WfState st)
             atomicAdd(&st.cnt->nans, n_nans);
         }
         if (n_active) atomicAdd(&st.qc[kQcActive], n_active);
+    }
+}
+
+// Scatters the gradients of the vertices finished this iteration (queued by the replay
+// shading and logic kernels) to the textures and constants of their materials.
+__global__ void __launch_bounds__(256) k_wf_grad_scatter(WfState st)
+{
+    const int64_t n = min((int64_t)st.qc[kQcGrad], st.cap_grad);
+    for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = i0 + threadIdx.x;
+        if (i >= n) continue;
+        const float4 e0 = st.gq[3 * i], e1 = st.gq[3 * i + 1], e2 = st.gq[3 * i + 2];
+        const float g[kGradParams] = {e0.x, e0.y, e0.z, e0.w, e1.x};
+        scatter_params(st, *st.views[__float_as_int(e2.x)].scene, __float_as_int(e1.w), e1.y, e1.z, g);
     }
 }
 
@@ -1146,6 +1176,8 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
         A(st.lp, pool);
         A(st.dfr, 5 * (size_t)pool);
         A(st.vg, 2 * (size_t)pool);
+        st.cap_grad = 2 * pool;   // a slot can finish two vertices in one iteration
+        A(st.gq, 3 * (size_t)st.cap_grad);
         A(st.sh_g, 3 * (size_t)st.cap_sh);
         A(st.mis_g, 8 * (size_t)st.cap_mis);
         st.tex_acc = adj->tex_acc;
@@ -1202,6 +1234,7 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
                 k_wf_shade<kClsSimple, true><<<shade_grid, tune.shade_block, 0, s>>>(st);
             }
             k_wf_logic<ADJ><<<logic_grid, 256, 0, s>>>(st);
+            if (ADJ) k_wf_grad_scatter<<<sms * 8, 256, 0, s>>>(st);
             if (tune.profile) cudaEventRecordWithFlags(pev[3 * it + 2], s, cudaEventRecordExternal);
         }
         e = cudaStreamEndCapture(s, &graph);
@@ -1262,7 +1295,7 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, e0, e1);
     if (times) {
-        times->launches = 1 + graph_launches * (ADJ ? 8 : 6) * tune.iters_per_graph + (int64_t)views.size();
+        times->launches = 1 + graph_launches * (ADJ ? 9 : 6) * tune.iters_per_graph + (int64_t)views.size();
         times->total_ms = ms;
         times->trace_ms = trace_ms;
         times->shade_ms = shade_ms;
