@@ -12,6 +12,10 @@ Metric: camera paths per second (a path = one pixel sample, counted when complet
 
 value  : device-resident scenes, device output images; time = device time of the K
          timed steps (CUDA events, max over ranks).
+roofline: the trace kernel's algorithmic bytes (fixed per-ray formula, live ray counts)
+         over its device time in the timed steps, taken from the GPU's global timer
+         inside the kernel (earliest block start to latest block end of each launch;
+         the render runs as one conditional CUDA graph, which admits no event nodes).
 e2e    : the same metric through the C-ABI from host memory: every step creates the 64
          scenes from host descriptors (upload + device BVH build + env tables), renders
          into host images and destroys the scenes.
@@ -41,9 +45,10 @@ sys.path.insert(0, str(ROOT))
 METRIC = "Mpaths/s batched wavefront vs plain megakernel at relMSE≤1e-3; adjoint/fwd ratio"
 WORKLOAD = "batched: 64 scenes x (1-40 displaced icosphere/box meshes, 1k-200k tris), 512x256 HDR env + 1 area light, 128^2-512^2, 4-64 spp, depth 8"
 NSCENES = 64
-# DRAM bytes the trace kernel moved per traced ray in one ncu capture of this workload
-# (profiles/k_wf_trace_batched64.md); None until captured.
-TRACE_DRAM_BYTES_PER_RAY = None
+# DRAM bytes the trace kernel moves per traced ray (read + write, cold L2 at each
+# launch), from ncu over every trace launch of the 8-scene case of this workload
+# (profiles/k_wf_trace_batched8.md); traffic grows with the rays a launch traces.
+TRACE_DRAM_BYTES_PER_RAY = 77.6
 
 
 def measured_peak_hbm():
@@ -119,10 +124,6 @@ def desc_bytes(holder) -> int:
             n += a.nbytes
     n += sum(a.nbytes for a in holder.tex_arrays)
     return n
-
-
-def scene_indices(rank: int, n: int = NSCENES):
-    return [rank * NSCENES + s for s in range(n)]
 
 
 # ---- reference arm (CPU) ---------------------------------------------------------------
@@ -255,27 +256,12 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
 
-    def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    from fumeng_b200.replicas import RankGroup, batch_indices
+    group = RankGroup(dist, "cuda")
+    barrier, max_over_ranks, sum_over_ranks = group.barrier, group.max, group.sum
 
     ctx = fb.Context(local_rank)
-    specs = [synth.batch_scene(s) for s in scene_indices(rank, args.scenes)]
+    specs = [synth.batch_scene(s) for s in batch_indices(rank, args.scenes, NSCENES)]
     holders = [s.to_desc() for s in specs]
     cams = [s.camera_struct() for s in specs]
     params_wf = [s.render_params(seed=1, mode=fb.FM_MODE_WAVEFRONT) for s in specs]
@@ -301,7 +287,7 @@ def main():
     with ClockSampler(local_rank) as clk:
         ev0.record()
         for _ in range(args.steps):
-            st = step_wf(profile=True)
+            st = step_wf()
             totals["paths"] += st.paths
             totals["closest"] += st.closest_rays
             totals["shadow"] += st.shadow_rays
@@ -343,8 +329,10 @@ def main():
     peak, peak_kind = measured_peak_hbm()
     achieved = alg_bytes / (totals["trace_ms"] / 1e3) / 1e9 if totals["trace_ms"] > 0 else None
     # six launches per wavefront iteration (prep, trace, resolve, two shade kernels,
-    # logic) plus one init and one reduce per view per step
-    launches_trace = max(1, (totals["launches"] - args.steps * (1 + len(specs))) // 6)
+    # logic), one loop-condition kernel per graph body of iters_per_graph iterations,
+    # and one init and one reduce per view per step
+    it = tuning.iters_per_graph
+    launches_trace = max(1, (totals["launches"] - args.steps * (1 + len(specs))) * it // (6 * it + 1))
     traffic = None
     if TRACE_DRAM_BYTES_PER_RAY is not None:
         traffic = TRACE_DRAM_BYTES_PER_RAY * (totals["closest"] + totals["shadow"]) / launches_trace

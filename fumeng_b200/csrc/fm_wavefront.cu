@@ -50,7 +50,7 @@ constexpr int kReplay = 4;
 constexpr int kQcCont = 0, kQcMis = 1, kQcShadow = 2;
 constexpr int kQcTraceCont = 3, kQcTraceMis = 4, kQcTraceShadow = 5;
 constexpr int kQcActive = 6, kQcDisney = 7, kQcSimple = 8, kQcTraceNext = 9, kQcDisneyR = 10, kQcSimpleR = 11;
-constexpr int kQcGrad = 12;
+constexpr int kQcGrad = 12, kQcBodies = 13;
 constexpr int kQcCount = 16;
 
 struct WfState {
@@ -91,6 +91,9 @@ struct WfState {
     uint32_t* sh_h;       // ... shadow ray occluded (1) or not (0)
     int64_t cap_cont, cap_mis, cap_sh;
     unsigned* qc;         // kQc* counters
+    // trace kernel span of the current iteration (earliest block start, latest block
+    // end, device global timer in ns) and the sum of the spans so far
+    unsigned long long* tspan;
     Counters* cnt;
     uint32_t* status;
     // adjoint renders only (null otherwise)
@@ -364,6 +367,17 @@ FM_D void add_vertex_grad(const WfState& st, int slot, const float* g)
         if (g[i] != 0.0f) atomicAdd(v + i, g[i]);
 }
 
+// Last kernel of a conditional graph body (iters_per_graph iterations): run the body
+// again while any slot holds work and the iteration bound is not reached (status bit 4
+// reports that the bound stopped the loop).
+__global__ void k_wf_continue(WfState st, cudaGraphConditionalHandle handle, unsigned max_bodies)
+{
+    const unsigned active = st.qc[kQcActive];
+    const unsigned bodies = ++st.qc[kQcBodies];
+    if (active != 0u && bodies >= max_bodies) atomicOr(st.status, 4u);
+    cudaGraphSetConditional(handle, (active != 0u && bodies < max_bodies) ? 1u : 0u);
+}
+
 __global__ void k_wf_prep(WfState st)
 {
     st.qc[kQcTraceCont] = st.qc[kQcCont];
@@ -379,6 +393,15 @@ __global__ void k_wf_prep(WfState st)
     st.qc[kQcSimpleR] = 0;
     st.qc[kQcGrad] = 0;
     st.qc[kQcTraceNext] = 0;
+    st.tspan[0] = ~0ull;
+    st.tspan[1] = 0ull;
+}
+
+FM_D unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
 }
 
 // Ray kinds of the trace kernel's combined index space [cont | MIS | shadow].
@@ -566,6 +589,7 @@ __global__ void __launch_bounds__(256) k_wf_trace(WfState st)
     int64_t idx = 0;
     bool exhausted = false;
     const int lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) atomicMin(&st.tspan[0], global_ns());
     for (;;) {
         const bool need = kind < 0 && !exhausted;
         const unsigned m = __ballot_sync(0xffffffffu, need);
@@ -594,6 +618,8 @@ __global__ void __launch_bounds__(256) k_wf_trace(WfState st)
             kind = -1;
         }
     }
+    __syncthreads();
+    if (threadIdx.x == 0) atomicMax(&st.tspan[1], global_ns());
 }
 
 // Turns the trace results into radiance (emission, MIS and NEE contributions added to
@@ -604,6 +630,7 @@ __global__ void __launch_bounds__(256) k_wf_resolve(WfState st)
 {
     const int64_t nc = st.qc[kQcTraceCont], nm = st.qc[kQcTraceMis], ns = st.qc[kQcTraceShadow];
     const int64_t total = nc + nm + ns;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && st.tspan[1] > st.tspan[0]) st.tspan[2] += st.tspan[1] - st.tspan[0];
     unsigned long long n_closest = 0, n_shadow = 0;
     for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < total; i0 += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = i0 + threadIdx.x;
@@ -1172,6 +1199,7 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
     A(st.mis_h, st.cap_mis);
     A(st.sh_h, st.cap_sh);
     A(st.qc, kQcCount);
+    A(st.tspan, 4);
     if (ADJ) {
         A(st.lp, pool);
         A(st.dfr, 5 * (size_t)pool);
@@ -1197,14 +1225,15 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
                 "wavefront views");
     FM_CUDA_TRY(ctx, cudaMemsetAsync(st.next_item, 0, sizeof(unsigned long long), s), "wavefront");
     FM_CUDA_TRY(ctx, cudaMemsetAsync(st.qc, 0, sizeof(unsigned) * kQcCount, s), "wavefront");
+    FM_CUDA_TRY(ctx, cudaMemsetAsync(st.tspan, 0, sizeof(unsigned long long) * 4, s), "wavefront");
     const int sms = ctx->num_sms;
     k_wf_init<<<sms * 8, 256, 0, s>>>(st);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, s);
-    // one graph = `iters_per_graph` iterations of prep -> trace -> shade (Disney) ->
-    // shade (other materials) -> logic
+    // one graph body = `iters_per_graph` iterations of prep -> trace -> resolve -> shade
+    // (Disney) -> shade (other materials) [-> replay shading] -> logic [-> gradient scatter]
     const int trace_grid = sms * 16;
     const int shade_grid = (int)std::min<int64_t>((pool + tune.shade_block - 1) / tune.shade_block, (int64_t)sms * 32);
     const int logic_grid = (int)std::min<int64_t>((pool + 255) / 256, (int64_t)sms * 32);
@@ -1212,6 +1241,16 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     fm_status result = FM_OK;
+    // Bound on iterations: every sample takes at most depth + 1 iterations and a slot
+    // runs its samples one after another.
+    int max_depth = 1, max_chunk = 1;
+    for (const auto& v : views) {
+        max_depth = std::max(max_depth, v.cfg.depth);
+        max_chunk = std::max(max_chunk, v.chunk);
+    }
+    const double iter_bound =
+        (total_samples / (double)pool + 4.0 * max_chunk + 8.0) * (max_depth + 2) * 4.0 * (ADJ ? 2.0 : 1.0) + 1000.0;
+    const int64_t max_launches = (int64_t)(iter_bound / tune.iters_per_graph) + 16;
     // optional per-kernel timing: event-record nodes around every trace and shade launch
     std::vector<cudaEvent_t> pev;
     if (tune.profile) {
@@ -1219,8 +1258,7 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
         for (auto& ev : pev) cudaEventCreate(&ev);
     }
     double trace_ms = 0.0, shade_ms = 0.0;
-    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess) {
+    auto capture_iterations = [&]() {
         for (int it = 0; it < tune.iters_per_graph; ++it) {
             k_wf_prep<<<1, 1, 0, s>>>(st);
             if (tune.profile) cudaEventRecordWithFlags(pev[3 * it], s, cudaEventRecordExternal);
@@ -1237,48 +1275,85 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
             if (ADJ) k_wf_grad_scatter<<<sms * 8, 256, 0, s>>>(st);
             if (tune.profile) cudaEventRecordWithFlags(pev[3 * it + 2], s, cudaEventRecordExternal);
         }
-        e = cudaStreamEndCapture(s, &graph);
+    };
+    cudaError_t e = cudaSuccess;
+    if (!tune.profile) {
+        // The whole render is one launch: a conditional WHILE node repeats the body
+        // (iters_per_graph iterations and k_wf_continue) on the device until no slot
+        // holds work, so the host never waits between iterations.
+        e = cudaGraphCreate(&graph, 0);
+        cudaGraphConditionalHandle handle{};
+        if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&handle, graph, 1u, cudaGraphCondAssignDefault);
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cnode = nullptr;
+        if (e == cudaSuccess) e = cudaGraphAddNode(&cnode, graph, nullptr, 0, &cp);
+        cudaGraph_t body = e == cudaSuccess ? cp.conditional.phGraph_out[0] : nullptr;
+        if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            capture_iterations();
+            k_wf_continue<<<1, 1, 0, s>>>(st, handle, (unsigned)std::min<int64_t>(max_launches, 0x7fffffff));
+            e = cudaStreamEndCapture(s, &body);
+        }
+    } else {
+        e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            capture_iterations();
+            e = cudaStreamEndCapture(s, &graph);
+        }
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
     if (e != cudaSuccess) {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
+        for (auto& ev : pev) cudaEventDestroy(ev);
+        if (graph) cudaGraphDestroy(graph);
         free_all();
         return cuda_error(ctx, e, "wavefront graph");
     }
     unsigned* h_qc = nullptr;
     cudaMallocHost(&h_qc, sizeof(unsigned) * kQcCount);
-    // Bound on graph launches: every sample takes at most depth + 1 iterations and a slot
-    // runs its samples one after another.
-    int max_depth = 1, max_chunk = 1;
-    for (const auto& v : views) {
-        max_depth = std::max(max_depth, v.cfg.depth);
-        max_chunk = std::max(max_chunk, v.chunk);
-    }
-    const double iter_bound =
-        (total_samples / (double)pool + 4.0 * max_chunk + 8.0) * (max_depth + 2) * 4.0 * (ADJ ? 2.0 : 1.0) + 1000.0;
-    const int64_t max_launches = (int64_t)(iter_bound / tune.iters_per_graph) + 16;
-    int64_t guard = 0, graph_launches = 0;
-    for (;;) {
+    int64_t graph_launches = 0;
+    if (!tune.profile) {
+        uint32_t hs = 0;
+        unsigned long long span[4] = {0, 0, 0, 0};
         e = cudaGraphLaunch(exec, s);
-        if (e != cudaSuccess) break;
-        ++graph_launches;
-        e = cudaMemcpyAsync(h_qc, st.qc, sizeof(unsigned) * kQcCount, cudaMemcpyDeviceToHost, s);
-        if (e != cudaSuccess) break;
-        e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) break;
-        for (int it = 0; it < (int)pev.size() / 3; ++it) {
-            float a = 0.0f, b = 0.0f;
-            cudaEventElapsedTime(&a, pev[3 * it], pev[3 * it + 1]);
-            cudaEventElapsedTime(&b, pev[3 * it + 1], pev[3 * it + 2]);
-            trace_ms += a;
-            shade_ms += b;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h_qc, st.qc, sizeof(unsigned) * kQcCount, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&hs, st.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(span, st.tspan, sizeof(span), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e == cudaSuccess) {
+            graph_launches = h_qc[kQcBodies];
+            // the resolve launch after each trace launch adds that launch's span
+            trace_ms = 1e-6 * (double)span[2];
+            if (hs & 4u) result = set_error(ctx, FM_ERR_TIMEOUT, "wavefront: iteration limit reached");
         }
-        // done when no slot holds work after the last shade
-        if (h_qc[kQcActive] == 0u) break;
-        if (++guard > max_launches) {
-            result = set_error(ctx, FM_ERR_TIMEOUT, "wavefront: iteration limit reached");
-            break;
+    } else {
+        int64_t guard = 0;
+        for (;;) {
+            e = cudaGraphLaunch(exec, s);
+            if (e != cudaSuccess) break;
+            ++graph_launches;
+            e = cudaMemcpyAsync(h_qc, st.qc, sizeof(unsigned) * kQcCount, cudaMemcpyDeviceToHost, s);
+            if (e != cudaSuccess) break;
+            e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) break;
+            for (int it = 0; it < (int)pev.size() / 3; ++it) {
+                float a = 0.0f, b = 0.0f;
+                cudaEventElapsedTime(&a, pev[3 * it], pev[3 * it + 1]);
+                cudaEventElapsedTime(&b, pev[3 * it + 1], pev[3 * it + 2]);
+                trace_ms += a;
+                shade_ms += b;
+            }
+            // done when no slot holds work after the last shade
+            if (h_qc[kQcActive] == 0u) break;
+            if (++guard > max_launches) {
+                result = set_error(ctx, FM_ERR_TIMEOUT, "wavefront: iteration limit reached");
+                break;
+            }
         }
     }
     if (e != cudaSuccess) result = cuda_error(ctx, e, "wavefront loop");
@@ -1295,10 +1370,12 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, e0, e1);
     if (times) {
-        times->launches = 1 + graph_launches * (ADJ ? 9 : 6) * tune.iters_per_graph + (int64_t)views.size();
+        times->launches = 1 + graph_launches * ((ADJ ? 9 : 6) * tune.iters_per_graph + (tune.profile ? 0 : 1)) +
+                          (int64_t)views.size();
         times->total_ms = ms;
         times->trace_ms = trace_ms;
-        times->shade_ms = shade_ms;
+        // without event timing, everything but the trace kernel counts as shading
+        times->shade_ms = tune.profile ? shade_ms : std::max(0.0, (double)ms - trace_ms);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -3,7 +3,7 @@
 Run on a machine that has the reference sources (the oracle libraries are built from
 them by oracle/Makefile):
 
-    python tests/golden/make_golden.py [hit] [images] [adjoint]
+    python tests/golden/make_golden.py [hit] [images] [adjoint] [batch]
 
 Scenes and rays are regenerated from seeds by fumeng_b200.synth, so each fixture stores
 only the reference's answers plus a SHA-256 of the inputs, which the tests recompute to
@@ -91,6 +91,34 @@ def make_image(case):
     print(name, "spp", spp, "%.1fs" % dt, "mean", mean.mean(axis=(0, 1)))
 
 
+# Scenes of the batched workload (synth.batch_scene index) and the 64x64 tile at the
+# centre of each image, rendered by the double build at 4096 spp: two 128^2 and two
+# 256^2 scenes of 22k-175k triangles with Disney, Lambert and dielectric materials.
+BATCH_CASES = [16, 26, 39, 43]
+BATCH_SPP, BATCH_SEED, BATCH_TILE = 4096, 9, 64
+
+
+def batch_tile(spec):
+    w, h = int(spec.renderer["width"]), int(spec.renderer["height"])
+    return ((w - BATCH_TILE) // 2, (h - BATCH_TILE) // 2, BATCH_TILE, BATCH_TILE)
+
+
+def make_batch(s):
+    spec = synth.batch_scene(s)
+    tile = batch_tile(spec)
+    with tempfile.TemporaryDirectory() as d:
+        rs = fmref.RefScene(spec.write(Path(d)), "double")
+        t0 = time.time()
+        r = rs.render(BATCH_SPP, seed=BATCH_SEED, tile=tile)
+        dt = time.time() - t0
+        rs.close()
+    mean = r["sum"] / BATCH_SPP
+    var = np.maximum(r["sumsq"] / BATCH_SPP - mean * mean, 0.0) * BATCH_SPP / (BATCH_SPP - 1)
+    np.savez_compressed(GOLDEN / f"batch_s{s}.npz", mean=mean.astype(np.float32), var=var.astype(np.float32),
+                        spp=BATCH_SPP, tile=np.asarray(tile), stride=1)
+    print(f"batch_s{s}", "tile", tile, "%.1fs" % dt, "mean", mean.mean(axis=(0, 1)))
+
+
 # Central differences of L = sum(w * image) from the reference's double build, for
 # constant material parameters of synth.gradient_scene (48x48), with common random
 # numbers across +-h: (material, JSON key, channel or None).
@@ -147,4 +175,7 @@ if __name__ == "__main__":
             make_image(c)
     if "adjoint" in what:
         make_adjoint_fd()
+    if "batch" in what:
+        for s in BATCH_CASES:
+            make_batch(s)
     print("done in %.1fs" % (time.time() - t0))

@@ -18,7 +18,8 @@ import numpy as np
 import pytest
 
 import fumeng_b200 as fb
-from golden.make_golden import IMAGE_CASES
+from fumeng_b200 import synth
+from golden.make_golden import BATCH_CASES, IMAGE_CASES
 
 GOLDEN_DIR = Path(__file__).resolve().parent / "golden"
 BATCHES, BATCH_SPP = 16, 256
@@ -100,3 +101,38 @@ def test_wavefront_matches_megakernel_on_same_random_streams(ctx):
     b = render_batches(ctx, spec, fb.FM_MODE_WAVEFRONT, batches=1, spp=64)[0][0]
     rel = np.abs(a - b) / (np.abs(a) + 1e-3)
     assert np.mean(rel < 1e-3) > 0.97, float(np.mean(rel < 1e-3))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", [fb.FM_MODE_MEGAKERNEL, fb.FM_MODE_WAVEFRONT], ids=["megakernel", "wavefront"])
+def test_batched_scenes_match_reference(ctx, mode):
+    """Four scenes of the batched workload rendered together through fm_render_batch
+    (one graph-captured wavefront, or the megakernel view after view), 16 x 256 spp, against
+    64x64 tiles of the reference's double build at 4096 spp (tests/golden/batch_s*.npz)."""
+    specs = [synth.batch_scene(s) for s in BATCH_CASES]
+    scenes = [ctx.create_scene(sp.to_desc()) for sp in specs]
+    try:
+        cams = [sp.camera_struct() for sp in specs]
+        out = [[] for _ in specs]
+        for b in range(BATCHES):
+            params = [sp.render_params(spp=BATCH_SPP, seed=1234, mode=mode, sample_offset=b * BATCH_SPP) for sp in specs]
+            rgb, _, _, st = ctx.render_batch(scenes, cams, params)
+            assert st.paths == sum(p.width * p.height * p.spp for p in params)
+            for i, img in enumerate(rgb):
+                out[i].append(img)
+    finally:
+        for sc in scenes:
+            sc.destroy()
+    for i, s in enumerate(BATCH_CASES):
+        g = np.load(GOLDEN_DIR / f"batch_s{s}.npz")
+        x0, y0, w, h = (int(v) for v in g["tile"])
+        tiles = np.stack(out[i]).astype(np.float64)[:, y0:y0 + h, x0:x0 + w]
+        assert np.all(np.isfinite(tiles))
+        res = compare(tiles, g)
+        res.update(case=f"batch_s{s}", mode="megakernel" if mode == fb.FM_MODE_MEGAKERNEL else "wavefront")
+        print(json.dumps(res))
+        if RESULTS.is_dir():
+            with open(RESULTS / "image_parity.jsonl", "a") as f:
+                f.write(json.dumps(res) + "\n")
+        assert res["frac_3sigma"] < 0.01, res
+        assert res["relmse_bias"] < 1e-3, res
