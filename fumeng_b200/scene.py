@@ -223,16 +223,22 @@ class SceneSpec:
             mats.append(j)
         objs = []
         for i, o in enumerate(self.objects):
+            extra = {}
             if isinstance(o, Mesh):
                 fn = f"mesh_{i}.obj"
                 self._write_obj(root / fn, o)
                 shape = {"type": "triangle_mesh", "path": fn}
+                if o.vattr is not None:
+                    # per-vertex attributes (extension): raw float32, V x dim
+                    va = np.ascontiguousarray(o.vattr, np.float32)
+                    (root / f"mesh_{i}.vattr").write_bytes(va.tobytes())
+                    extra["fm_vertex_attributes"] = {"path": f"mesh_{i}.vattr", "dim": int(va.shape[1])}
             elif isinstance(o, Rect):
                 shape = {"type": "rectangle", **{k: [float(fmt(x)) for x in getattr(o, k)] for k in ("pa", "pb", "pc", "pd")}}
             else:
                 shape = {"type": "sphere", "radius": float(fmt(o.radius)), "translation": [float(fmt(x)) for x in o.translation],
                          "rotation": [float(fmt(x)) for x in o.rotation], "scale": [float(fmt(x)) for x in o.scale]}
-            e = {"shape": shape, "material": o.material}
+            e = {"shape": shape, "material": o.material, **extra}
             if o.emittance is not None:
                 e["emittance"] = [float(fmt(x)) for x in o.emittance]
             objs.append(e)

@@ -79,6 +79,7 @@
 #include <geometry/triangle.h>
 #include <engine/core/fresnel.h>
 #include <material/disney.h>
+#include <material/disney.cpp>
 #undef private
 #undef protected
 
@@ -103,9 +104,99 @@ namespace {
 
 thread_local std::string g_error;
 
+// ---- per-vertex Disney parameters ---------------------------------------------------
+//
+// A scene-file extension the reference's loader cannot express: a triangle-mesh entry
+// may carry "fm_vertex_attributes": {"path": <raw float32 V x dim file>, "dim": dim},
+// giving each vertex basecolor r, g, b, roughness, metallic, clearcoat (at the offset
+// its Disney material's "vertex_attributes" names).  The harness registers, under that
+// material's name, a Material that interpolates the hit triangle's vertex values with
+// barycentrics recovered from the hit position and builds the reference's own
+// DisneyBSDF from them; the material's other parameters come from its JSON entry,
+// parsed and sampled by the reference's DisneyConfig and textures.
+struct VertexTri {
+    fe::vec3 p[3];
+    double a[3][6];
+};
+
+class VertexDisneyMaterial : public fe::Material {
+public:
+    const std::unordered_map<const fe::RenderObject*, VertexTri>* tris = nullptr;
+    fe::SP<fe::Texture> specular, specularTint, anisotropic, sheen, sheenTint, clearcoatGloss, specTrans,
+        specTransRoughness, diffTrans, flatness, ior;
+    bool thin = false;
+
+    explicit VertexDisneyMaterial(const fe::DisneyConfig& c)
+    {
+        specular = fe::CreateTexture(c.specular);
+        specularTint = fe::CreateTexture(c.specularTint);
+        anisotropic = fe::CreateTexture(c.anisotropic);
+        sheen = fe::CreateTexture(c.sheen);
+        sheenTint = fe::CreateTexture(c.sheenTint);
+        clearcoatGloss = fe::CreateTexture(c.clearcoatGloss);
+        specTrans = fe::CreateTexture(c.specTrans);
+        specTransRoughness = fe::CreateTexture(c.specTransRoughness);
+        diffTrans = fe::CreateTexture(c.diffTrans);
+        flatness = fe::CreateTexture(c.flatness);
+        ior = fe::CreateTexture(c.ior);
+        thin = c.thin;
+    }
+
+    void CreateBSDF(fe::HitPoint& hp) const override
+    {
+        const VertexTri& t = tris->at(hp.object);
+        // barycentrics of hp.pos in the triangle (least squares in the triangle's plane)
+        const fe::vec3 e1 = t.p[1] - t.p[0], e2 = t.p[2] - t.p[0], q = hp.pos - t.p[0];
+        const double d11 = glm::dot(e1, e1), d12 = glm::dot(e1, e2), d22 = glm::dot(e2, e2);
+        const double q1 = glm::dot(q, e1), q2 = glm::dot(q, e2);
+        const double den = d11 * d22 - d12 * d12;
+        const double b1 = den != 0.0 ? (d22 * q1 - d12 * q2) / den : 0.0;
+        const double b2 = den != 0.0 ? (d11 * q2 - d12 * q1) / den : 0.0;
+        const double b0 = 1.0 - b1 - b2;
+        double v[6];
+        for (int k = 0; k < 6; ++k) v[k] = b0 * t.a[0][k] + b1 * t.a[1][k] + b2 * t.a[2][k];
+        const vec2 uv = hp.uv;
+        hp.bsdf = fe::MakeSP<fe::DisneyBSDF>(hp, vec3(real(v[0]), real(v[1]), real(v[2])), real(v[4]),
+                                             specular->Sample(uv).x, specularTint->Sample(uv).x, real(v[3]),
+                                             anisotropic->Sample(uv).x, sheen->Sample(uv).x, sheenTint->Sample(uv).x,
+                                             real(v[5]), clearcoatGloss->Sample(uv).x, specTrans->Sample(uv).x,
+                                             specTransRoughness->Sample(uv).x, diffTrans->Sample(uv).x,
+                                             flatness->Sample(uv).x, ior->Sample(uv).x, thin);
+    }
+};
+
+// Triangles of an OBJ written by the scene generator ("v x y z" lines and triangular
+// "f" lines whose first index of each corner is the vertex): positions and indices.
+// Parsed with C stdio (the Python process that loads this library may carry an older
+// C++ runtime than the one this file was compiled against).
+void read_obj_triangles(const std::string& path, std::vector<fe::vec3>& verts, std::vector<std::array<int, 3>>& faces)
+{
+    FILE* f = std::fopen(path.c_str(), "r");
+    if (!f) throw std::runtime_error("cannot open " + path);
+    char line[512];
+    while (std::fgets(line, sizeof(line), f)) {
+        if (line[0] == 'v' && line[1] == ' ') {
+            double x = 0, y = 0, z = 0;
+            if (std::sscanf(line + 2, "%lf %lf %lf", &x, &y, &z) == 3) verts.emplace_back(real(x), real(y), real(z));
+        } else if (line[0] == 'f' && line[1] == ' ') {
+            std::array<int, 3> tri{};
+            char* p = line + 2;
+            for (int k = 0; k < 3; ++k) {
+                char* end = nullptr;
+                tri[k] = int(std::strtol(p, &end, 10)) - 1;
+                p = end;
+                while (*p && *p != ' ' && *p != '\t' && *p != '\n') ++p;   // skip "/vt/vn"
+            }
+            faces.push_back(tri);
+        }
+    }
+    std::fclose(f);
+}
+
 struct RefScene {
     fe::SceneLoader loader;
     std::unordered_map<const fe::RenderObject*, int> obj_index;
+    std::unordered_map<const fe::RenderObject*, VertexTri> vertex_tris;
     fe::PathTracerConfig pt_config;
     int width = 1, height = 1, spp = 1;
 };
@@ -211,10 +302,60 @@ void* fmref_load(const char* json_path)
                 L.m_materials.emplace(name, fe::CreateSpecularReflection(color, eta_i, eta_t, k));
             }
         }
+        // per-vertex Disney materials, registered before the loader builds its own
+        std::map<std::string, std::pair<fe::SP<VertexDisneyMaterial>, int>> vmats;   // name -> (material, offset)
+        if (L.m_config.contains("scene") && L.m_config["scene"].contains("materials")) {
+            for (auto& m : L.m_config["scene"]["materials"]) {
+                if (m.value("type", std::string()) != "disney" || !m.contains("vertex_attributes")) continue;
+                fe::DisneyConfig dc;
+                dc.Load(m);
+                auto vm = std::make_shared<VertexDisneyMaterial>(dc);
+                vm->tris = &s->vertex_tris;
+                const std::string name = m.value("name", std::string());
+                vmats[name] = {vm, m["vertex_attributes"].value("offset", 0)};
+                L.m_materials.emplace(name, vm);
+            }
+        }
         L.ParseScene();
         L.ParsePostProcess();
         for (size_t i = 0; i < L.m_render_objects.size(); ++i)
             s->obj_index[L.m_render_objects[i].get()] = int(i);
+        // vertex attributes of the triangles of meshes that carry them: render objects
+        // follow the scene file's entries in order, one per triangle of a mesh
+        if (!vmats.empty()) {
+            size_t obj = 0;
+            for (auto& e : L.m_config["scene"]["render_objects"]) {
+                const auto& shape = e["shape"];
+                const std::string type = shape.value("type", std::string());
+                if (type != "triangle_mesh") {
+                    ++obj;
+                    continue;
+                }
+                std::vector<fe::vec3> verts;
+                std::vector<std::array<int, 3>> faces;
+                read_obj_triangles(L.m_scene_root + shape.value("path", std::string()), verts, faces);
+                if (e.contains("fm_vertex_attributes") && vmats.count(e.value("material", std::string()))) {
+                    const auto& va = e["fm_vertex_attributes"];
+                    const int dim = va.value("dim", 6);
+                    const int off = vmats[e.value("material", std::string())].second;
+                    std::vector<float> attr(verts.size() * size_t(dim));
+                    FILE* af = std::fopen((L.m_scene_root + va.value("path", std::string())).c_str(), "rb");
+                    const size_t got = af ? std::fread(attr.data(), sizeof(float), attr.size(), af) : 0;
+                    if (af) std::fclose(af);
+                    if (got != attr.size()) throw std::runtime_error("short vertex attribute file");
+                    for (size_t f = 0; f < faces.size(); ++f) {
+                        VertexTri t;
+                        for (int k = 0; k < 3; ++k) {
+                            t.p[k] = verts[size_t(faces[f][k])];
+                            for (int q = 0; q < 6; ++q) t.a[k][q] = attr[size_t(faces[f][k]) * dim + off + q];
+                        }
+                        s->vertex_tris[L.m_render_objects.at(obj + f).get()] = t;
+                    }
+                }
+                obj += faces.size();
+            }
+            if (obj != L.m_render_objects.size()) throw std::runtime_error("vertex attributes: object count mismatch");
+        }
         fe::RendererConfig::SetRootPath(L.m_scene_root);
         s->pt_config.Load(L.m_config["renderer"]);
         s->width = s->pt_config.width;

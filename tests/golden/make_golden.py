@@ -3,7 +3,7 @@
 Run on a machine that has the reference sources (the oracle libraries are built from
 them by oracle/Makefile):
 
-    python tests/golden/make_golden.py [hit] [images] [adjoint] [batch]
+    python tests/golden/make_golden.py [hit] [images] [adjoint] [batch] [single]
 
 Scenes and rays are regenerated from seeds by fumeng_b200.synth, so each fixture stores
 only the reference's answers plus a SHA-256 of the inputs, which the tests recompute to
@@ -91,11 +91,12 @@ def make_image(case):
     print(name, "spp", spp, "%.1fs" % dt, "mean", mean.mean(axis=(0, 1)))
 
 
-# Scenes of the batched workload (synth.batch_scene index) and the 64x64 tile at the
-# centre of each image, rendered by the double build at 4096 spp: two 128^2 and two
-# 256^2 scenes of 22k-175k triangles with Disney, Lambert and dielectric materials.
+# Scenes of the batched workload (synth.batch_scene index) and a tile at the centre of
+# each image, rendered by the double build (each fixture records its tile and spp):
+# two 128^2 and two 256^2 scenes of 22k-175k triangles with Disney, Lambert and
+# dielectric materials.
 BATCH_CASES = [16, 26, 39, 43]
-BATCH_SPP, BATCH_SEED, BATCH_TILE = 4096, 9, 64
+BATCH_SPP, BATCH_SEED, BATCH_TILE = 2048, 9, 48
 
 
 def batch_tile(spec):
@@ -104,6 +105,8 @@ def batch_tile(spec):
 
 
 def make_batch(s):
+    if (GOLDEN / f"batch_s{s}.npz").exists():
+        return
     spec = synth.batch_scene(s)
     tile = batch_tile(spec)
     with tempfile.TemporaryDirectory() as d:
@@ -117,6 +120,33 @@ def make_batch(s):
     np.savez_compressed(GOLDEN / f"batch_s{s}.npz", mean=mean.astype(np.float32), var=var.astype(np.float32),
                         spp=BATCH_SPP, tile=np.asarray(tile), stride=1)
     print(f"batch_s{s}", "tile", tile, "%.1fs" % dt, "mean", mean.mean(axis=(0, 1)))
+
+
+# The single-mesh configuration (1.31 M-triangle displaced icosphere with per-vertex
+# Disney parameters, thin lens, 2048x1024 sky with a sharp sun) at 480x270: 48x48 tiles
+# at the centre of the sphere and across its silhouette, double build, 4096 spp.
+SINGLE_RES = (480, 270)
+SINGLE_TILES = [(216, 111, 48, 48), (315, 111, 48, 48)]
+SINGLE_SPP, SINGLE_SEED = 4096, 11
+
+
+def single_scene():
+    return synth.single_mesh_scene(width=SINGLE_RES[0], height=SINGLE_RES[1])
+
+
+def make_single():
+    spec = single_scene()
+    with tempfile.TemporaryDirectory() as d:
+        rs = fmref.RefScene(spec.write(Path(d)), "double")
+        for k, tile in enumerate(SINGLE_TILES):
+            t0 = time.time()
+            r = rs.render(SINGLE_SPP, seed=SINGLE_SEED, tile=tile)
+            mean = r["sum"] / SINGLE_SPP
+            var = np.maximum(r["sumsq"] / SINGLE_SPP - mean * mean, 0.0) * SINGLE_SPP / (SINGLE_SPP - 1)
+            np.savez_compressed(GOLDEN / f"single_t{k}.npz", mean=mean.astype(np.float32), var=var.astype(np.float32),
+                                spp=SINGLE_SPP, tile=np.asarray(tile), stride=1)
+            print(f"single_t{k}", tile, "%.1fs" % (time.time() - t0), "mean", mean.mean(axis=(0, 1)))
+        rs.close()
 
 
 # Central differences of L = sum(w * image) from the reference's double build, for
@@ -178,4 +208,6 @@ if __name__ == "__main__":
     if "batch" in what:
         for s in BATCH_CASES:
             make_batch(s)
+    if "single" in what:
+        make_single()
     print("done in %.1fs" % (time.time() - t0))

@@ -19,7 +19,7 @@ import pytest
 
 import fumeng_b200 as fb
 from fumeng_b200 import synth
-from golden.make_golden import BATCH_CASES, IMAGE_CASES
+from golden.make_golden import BATCH_CASES, IMAGE_CASES, SINGLE_TILES, single_scene
 
 GOLDEN_DIR = Path(__file__).resolve().parent / "golden"
 BATCHES, BATCH_SPP = 16, 256
@@ -133,6 +133,31 @@ def test_batched_scenes_match_reference(ctx, mode):
         assert np.all(np.isfinite(tiles))
         res = compare(tiles, g)
         res.update(case=f"batch_s{s}", mode="megakernel" if mode == fb.FM_MODE_MEGAKERNEL else "wavefront")
+        print(json.dumps(res))
+        if RESULTS.is_dir():
+            with open(RESULTS / "image_parity.jsonl", "a") as f:
+                f.write(json.dumps(res) + "\n")
+        assert res["frac_3sigma"] < 0.01, res
+        assert res["relmse_bias"] < 1e-3, res
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", [fb.FM_MODE_MEGAKERNEL, fb.FM_MODE_WAVEFRONT], ids=["megakernel", "wavefront"])
+def test_single_mesh_scene_matches_reference(ctx, mode):
+    """The single-mesh configuration (1.31 M triangles, per-vertex Disney parameters,
+    thin lens, 2048x1024 sky with a sharp sun) at 480x270, 16 x 256 spp, against 48x48
+    tiles of the reference's double build at 4096 spp (tests/golden/single_t*.npz)."""
+    tiles = [k for k in range(len(SINGLE_TILES)) if (GOLDEN_DIR / f"single_t{k}.npz").exists()]
+    if not tiles:
+        pytest.skip("no single-mesh fixtures (tests/golden/make_golden.py single)")
+    rgb, _, _ = render_batches(ctx, single_scene(), mode)
+    for k in tiles:
+        g = np.load(GOLDEN_DIR / f"single_t{k}.npz")
+        x0, y0, w, h = (int(v) for v in g["tile"])
+        t = rgb[:, y0:y0 + h, x0:x0 + w]
+        assert np.all(np.isfinite(t))
+        res = compare(t, g)
+        res.update(case=f"single_t{k}", mode="megakernel" if mode == fb.FM_MODE_MEGAKERNEL else "wavefront")
         print(json.dumps(res))
         if RESULTS.is_dir():
             with open(RESULTS / "image_parity.jsonl", "a") as f:
