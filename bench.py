@@ -392,6 +392,10 @@ def main():
                          "shadow_rays": totals["shadow"] / totals["paths"],
                          "bounces": totals["bounces"] / totals["paths"]},
             "nan_samples": int(totals["nans"]),
+            # device time inside the render calls (first kernel to last) against the
+            # timed steps: the difference is host time between calls
+            "render_device_ms_per_step": totals["kernel_ms"] / args.steps,
+            "trace_ms_per_step": totals["trace_ms"] / args.steps,
             "adjoint": adj,
         }
         print(json.dumps(line))

@@ -578,7 +578,7 @@ FM_D void finish_shadow(const WfState& st, int64_t q, const DevScene& S, const H
 // lane whose query completes takes the next unclaimed ray (one atomic per warp and
 // refill), so lanes do not idle while the warp's slowest traversal finishes, and the
 // loop holds nothing but traversal.
-__global__ void __launch_bounds__(256) k_wf_trace(WfState st)
+__global__ void __launch_bounds__(256, 4) k_wf_trace(WfState st)
 {
     const int64_t nc = st.qc[kQcTraceCont], nm = st.qc[kQcTraceMis], ns = st.qc[kQcTraceShadow];
     const int64_t total = nc + nm + ns;
