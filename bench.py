@@ -211,6 +211,123 @@ def measure_adjoint(ctx, args, barrier, max_over_ranks):
             "timing": "device time of the wavefront loop (CUDA events), same default tuning for both passes"}
 
 
+LARGE_WORKLOAD = ("large: 8x8 grid of displaced meshes, 124,848 tris each (7.99 M), Disney (glass-like, diffuse, "
+                  "general) + Lambert ground, 2048x1024 HDR env + 4 area lights, 8 views 1920x1080, 128 spp, depth 16")
+
+
+def run_large(args, ctx, group, rank, world):
+    """The large combined workload: forward Mpaths/s over the 8 views, a bounded
+    megakernel sample, end to end from host memory, and the adjoint with respect to a
+    512x256 env parameter grid (the 2048x1024 env map is that grid upsampled 4x by
+    replication, so the grid's gradient is the sum of each 4x4 block of texel gradients)
+    and the 64 per-mesh roughness values, against its forward at the same spp."""
+    import torch
+    import fumeng_b200 as fb
+    from fumeng_b200 import synth
+    from fumeng_b200.scene import camera_struct
+    spec = synth.large_scene()
+    holder = spec.to_desc()
+    sc = ctx.create_scene(holder)
+    build_ms = sc.bvh_stats()["build_ms"]
+    cams = [camera_struct(c) for c in synth.large_views(8)]
+    params = [spec.render_params(seed=1 + v) for v in range(8)]
+    paths = sum(p.width * p.height * p.spp for p in params)
+    outs = [torch.empty((p.height, p.width, 3), device="cuda") for p in params]
+    ptrs = [o.data_ptr() for o in outs]
+    tune = fb.Tuning(1 << 22, 128, 128, 8)
+
+    def step():
+        return ctx.render_batch([sc] * 8, cams, params, tuning=tune, device_outputs=ptrs)[3]
+    for _ in range(args.warmup):
+        step()
+    group.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    tot = {"paths": 0, "closest": 0, "shadow": 0, "trace_ms": 0.0, "kernel_ms": 0.0, "launches": 0, "nans": 0}
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        ev0.record()
+        for _ in range(args.steps):
+            st = step()
+            tot["paths"] += st.paths
+            tot["closest"] += st.closest_rays
+            tot["shadow"] += st.shadow_rays
+            tot["trace_ms"] += st.trace_ms
+            tot["kernel_ms"] += st.kernel_ms
+            tot["launches"] += st.launches
+            tot["nans"] += st.nan_samples
+        ev1.record()
+        group.barrier()
+    clocks = clk.summary()
+    ms = group.max(ev0.elapsed_time(ev1))
+    value = group.sum(float(tot["paths"])) / (ms / 1e3) / 1e6
+    assert tot["paths"] == paths * args.steps
+    # megakernel on one view at 8 spp (a bounded sample of the same work)
+    mk_p = [spec.render_params(spp=8, seed=1, mode=fb.FM_MODE_MEGAKERNEL)]
+    ctx.render_batch([sc], cams[:1], mk_p, device_outputs=ptrs[:1])
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    group.barrier()
+    e0.record()
+    ctx.render_batch([sc], cams[:1], mk_p, device_outputs=ptrs[:1])
+    e1.record()
+    group.barrier()
+    mk_paths = mk_p[0].width * mk_p[0].height * mk_p[0].spp
+    mk_value = group.sum(float(mk_paths)) / (group.max(e0.elapsed_time(e1)) / 1e3) / 1e6
+    # roofline of the trace kernel
+    D = bvh_depth_estimate(holder.desc.num_triangles + 2 * holder.desc.num_rects)
+    closest_b, shadow_b = 32 + 16 + 80 * D + 160, 32 + 4 + 80 * D + 160
+    peak, peak_kind = measured_peak_hbm()
+    achieved = (tot["closest"] * closest_b + tot["shadow"] * shadow_b) / (tot["trace_ms"] / 1e3) / 1e9
+    launches_trace = max(1, (tot["launches"] - args.steps * 9) * 8 // 49)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": TRACE_DRAM_BYTES_PER_RAY * (tot["closest"] + tot["shadow"]) / launches_trace,
+                "kernel": "k_wf_trace", "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+                "alg_bytes_per_closest_ray": closest_b, "alg_bytes_per_shadow_ray": shadow_b,
+                "trace_share_of_step": tot["trace_ms"] / max(tot["kernel_ms"], 1e-9)}
+    # end to end: scene from host descriptors, render into host images
+    e2e = None
+    if args.e2e_steps > 0:
+        t0 = time.perf_counter()
+        sc2 = ctx.create_scene(holder)
+        ctx.render_batch([sc2] * 8, cams, params, tuning=tune)
+        sc2.destroy()
+        e2e_ms = group.max(1e3 * (time.perf_counter() - t0))
+        e2e = {"value": group.sum(float(paths)) / (e2e_ms / 1e3) / 1e6, "unit": "Mpaths/s",
+               "h2d_bytes_per_step": int(desc_bytes(holder)),
+               "d2h_bytes_per_step": int(sum(p.width * p.height * 12 for p in params)), "ms_per_step": e2e_ms,
+               "timing": "host wall clock around scene creation, render and image copies"}
+    # adjoint w.r.t. the env parameter grid and the per-mesh roughness values, 32 spp
+    adj = None
+    if args.adjoint_steps > 0:
+        ti, mi = holder.texture_index, holder.material_index
+        fwd = [spec.render_params(spp=32, seed=100 + v) for v in range(8)]
+        adjp = [spec.render_params(spp=32, seed=900 + v) for v in range(8)]
+        d_rgb = [np.random.default_rng(v).standard_normal((p.height, p.width, 3)).astype(np.float32) * 1e-4
+                 for v, p in enumerate(adjp)]
+        sky = spec.textures["sky"]
+        f_st = ctx.render_batch([sc] * 8, cams, fwd, tuning=tune, device_outputs=ptrs)[3]
+        tg, mg, _, a_st = sc.render_adjoint(cams, adjp, d_rgb, {ti["sky"]: sky.shape[:2]}, material_grads=True)
+        grid = tg[ti["sky"]].reshape(sky.shape[0] // 4, 4, sky.shape[1] // 4, 4, 3).sum(axis=(1, 3))
+        rough = np.array([mg[mi[f"m{k}"], 4] for k in range(64)])
+        adj = {"workload": "large scene, 8 views 1080p, 32 spp forward + 32 spp adjoint, depth 16; gradients of a "
+                           "random linear loss w.r.t. the 512x256x3 env grid and the 64 per-mesh roughness values",
+               "forward_ms": f_st.kernel_ms, "adjoint_ms": a_st.kernel_ms,
+               "adjoint_over_forward": a_st.kernel_ms / f_st.kernel_ms, "env_grid_shape": list(grid.shape),
+               "env_grid_grad_l2": float(np.linalg.norm(grid)), "roughness_grad_l2": float(np.linalg.norm(rough)),
+               "nan_samples": int(a_st.nan_samples)}
+    sc.destroy()
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": LARGE_WORKLOAD, "triangles": int(holder.desc.num_triangles), "views": 8,
+                       "paths_per_step": int(paths), "depth": 16, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2", "bvh_build_ms": build_ms, "tuning": tune.as_dict()},
+            "roofline": roofline, "cpu_baseline": None, "e2e": e2e, "gpu_launches": int(tot["launches"]),
+            "clocks": clocks, "megakernel": {"value": mk_value, "sample": "1 view at 8 spp"},
+            "wavefront_vs_megakernel": value / mk_value, "adjoint": adj, "nan_samples": int(tot["nans"]),
+            "render_device_ms_per_step": tot["kernel_ms"] / args.steps}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -223,6 +340,8 @@ def main():
     ap.add_argument("--scenes", type=int, default=NSCENES, help="batch size (profiling runs use fewer)")
     ap.add_argument("--adjoint-steps", type=int, default=2, help="timed adjoint/forward pairs (0 skips)")
     ap.add_argument("--no-autotune", action="store_true", help="default tuning instead of the autotuner's")
+    ap.add_argument("--workload", default="batched", choices=["batched", "large"],
+                    help="batched: 64 scenes (the headline); large: 8 M triangles, 8 views of 1080p, depth 16")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -261,6 +380,12 @@ def main():
     barrier, max_over_ranks, sum_over_ranks = group.barrier, group.max, group.sum
 
     ctx = fb.Context(local_rank)
+    if args.workload == "large":
+        run_large(args, ctx, group, rank, world)
+        ctx.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     specs = [synth.batch_scene(s) for s in batch_indices(rank, args.scenes, NSCENES)]
     holders = [s.to_desc() for s in specs]
     cams = [s.camera_struct() for s in specs]

@@ -488,3 +488,58 @@ def single_mesh_scene(level: int = 8, width: int = 1920, height: int = 1080, spp
     ren = {"width": width, "height": height, "spp": spp, "depth": depth, "rr_depth": 3, "rr_coef": 0.85}
     lights = [{"type": "env", "texture": "sky", "rotation": [0, 0, 0], "factor": 1.0}]
     return SceneSpec(cam, ren, mats, objs, lights, {"sky": env})
+
+
+# ---- large combined workload -----------------------------------------------------------
+
+
+def large_scene(grid: int = 8, box_n: int = 102, width: int = 1920, height: int = 1080, spp: int = 128,
+                depth: int = 16, env_w: int = 2048, env_h: int = 1024, seed: int = 7) -> SceneSpec:
+    """grid x grid displaced meshes (subdivided cubes pushed onto a sphere and displaced
+    by 0.08 fBm; box_n = 102 gives 124,848 triangles each, 8 M in all) on a ground plane,
+    each with its own Disney material and roughness (the per-mesh scalars an adjoint
+    differentiates): a third glass-like (specTrans 1), a third diffuse (specular 0), a
+    third general; a 2048x1024 sky with a sharp sun and four rectangle lights."""
+    rng = np.random.default_rng(seed)
+    bv, bf = subdivided_box(box_n)
+    unit = bv / np.linalg.norm(bv, axis=1, keepdims=True)
+    objs, mats = [], []
+    half = grid / 2.0
+    for gy in range(grid):
+        for gx in range(grid):
+            k = gy * grid + gx
+            disp = unit * (1.0 + 0.08 * PerlinNoise(seed * 1000 + k).fbm(unit, octaves=4))[:, None]
+            c = np.array([(gx - half + 0.5) * 2.2, (gy - half + 0.5) * 2.2, 0.85])
+            objs.append(Mesh((disp * 0.8 + c).astype(np.float32), bf, f"m{k}"))
+            kind = k % 3
+            m = {"name": f"m{k}", "type": "disney", "basecolor": list(rng.uniform(0.15, 0.9, 3)),
+                 "roughness": float(rng.uniform(0.1, 0.9)), "specular": 0.5}
+            if kind == 0:
+                m.update(specTrans=1.0, specTransRoughness=0.1, ior=float(rng.uniform(1.3, 1.7)))
+            elif kind == 1:
+                m.update(specular=0.0)
+            else:
+                m.update(metallic=float(rng.random() < 0.5), clearcoat=float(rng.uniform(0, 1)))
+            mats.append(m)
+    mats.append({"name": "ground", "type": "lambert_diffuse", "basecolor": [0.45, 0.45, 0.42]})
+    objs.append(Rect((-12, -12, 0), (12, -12, 0), (12, 12, 0), (-12, 12, 0), "ground"))
+    for lx, ly in ((-4, -4), (4, -4), (-4, 4), (4, 4)):
+        objs.append(Rect((lx - 0.7, ly - 0.7, 6.0), (lx - 0.7, ly + 0.7, 6.0), (lx + 0.7, ly + 0.7, 6.0),
+                         (lx + 0.7, ly - 0.7, 6.0), "ground", emittance=(8.0, 8.0, 7.5)))
+    env = sky_env(env_w, env_h, seed, sun_peak=5e4, sun_sigma_deg=0.5)
+    cams = large_views(1, seed)
+    ren = {"width": width, "height": height, "spp": spp, "depth": depth, "rr_depth": 3, "rr_coef": 0.85}
+    lights = [{"type": "env", "texture": "sky", "rotation": [0, 0, 0], "factor": 1.0}]
+    return SceneSpec(cams[0], ren, mats, objs, lights, {"sky": env})
+
+
+def large_views(n: int = 8, seed: int = 7, aspect: float = 16 / 9) -> list:
+    """n pinhole cameras around the large workload's grid."""
+    rng = np.random.default_rng(seed + 1)
+    cams = []
+    for k in range(n):
+        az = 2 * math.pi * (k + rng.uniform(-0.15, 0.15)) / n
+        r, z = 17.0, float(rng.uniform(5.0, 9.0))
+        cams.append({"type": "pin_hole", "pos": [r * math.cos(az), r * math.sin(az), z], "look_at": [0.0, 0.0, 0.5],
+                     "up": [0, 0, 1], "fov": 50.0, "aspect": aspect})
+    return cams
