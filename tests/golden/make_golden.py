@@ -96,7 +96,7 @@ def make_image(case):
 # two 128^2 and two 256^2 scenes of 22k-175k triangles with Disney, Lambert and
 # dielectric materials.
 BATCH_CASES = [16, 26, 39, 43]
-BATCH_SPP, BATCH_SEED, BATCH_TILE = 2048, 9, 48
+BATCH_SPP, BATCH_SEED, BATCH_TILE = 1024, 9, 32
 
 
 def batch_tile(spec):
@@ -123,11 +123,11 @@ def make_batch(s):
 
 
 # The single-mesh configuration (1.31 M-triangle displaced icosphere with per-vertex
-# Disney parameters, thin lens, 2048x1024 sky with a sharp sun) at 480x270: 48x48 tiles
-# at the centre of the sphere and across its silhouette, double build, 4096 spp.
+# Disney parameters, thin lens, 2048x1024 sky with a sharp sun) at 480x270: 32x32 tiles
+# at the centre of the sphere and across its silhouette, double build, 1024 spp.
 SINGLE_RES = (480, 270)
-SINGLE_TILES = [(216, 111, 48, 48), (315, 111, 48, 48)]
-SINGLE_SPP, SINGLE_SEED = 4096, 11
+SINGLE_TILES = [(224, 119, 32, 32), (323, 119, 32, 32)]
+SINGLE_SPP, SINGLE_SEED = 1024, 11
 
 
 def single_scene():

@@ -108,7 +108,8 @@ def test_wavefront_matches_megakernel_on_same_random_streams(ctx):
 def test_batched_scenes_match_reference(ctx, mode):
     """Four scenes of the batched workload rendered together through fm_render_batch
     (one graph-captured wavefront, or the megakernel view after view), 16 x 256 spp, against
-    64x64 tiles of the reference's double build at 4096 spp (tests/golden/batch_s*.npz)."""
+    tiles of the reference's double build (tests/golden/batch_s*.npz; each fixture records
+    its tile and spp)."""
     cases = [s for s in BATCH_CASES if (GOLDEN_DIR / f"batch_s{s}.npz").exists()]
     if not cases:
         pytest.skip("no batched-scene fixtures (tests/golden/make_golden.py batch)")
@@ -145,8 +146,9 @@ def test_batched_scenes_match_reference(ctx, mode):
 @pytest.mark.parametrize("mode", [fb.FM_MODE_MEGAKERNEL, fb.FM_MODE_WAVEFRONT], ids=["megakernel", "wavefront"])
 def test_single_mesh_scene_matches_reference(ctx, mode):
     """The single-mesh configuration (1.31 M triangles, per-vertex Disney parameters,
-    thin lens, 2048x1024 sky with a sharp sun) at 480x270, 16 x 256 spp, against 48x48
-    tiles of the reference's double build at 4096 spp (tests/golden/single_t*.npz)."""
+    thin lens, 2048x1024 sky with a sharp sun) at 480x270, 16 x 256 spp, against 32x32
+    tiles of the reference's double build (tests/golden/single_t*.npz; each fixture
+    records its tile and spp)."""
     tiles = [k for k in range(len(SINGLE_TILES)) if (GOLDEN_DIR / f"single_t{k}.npz").exists()]
     if not tiles:
         pytest.skip("no single-mesh fixtures (tests/golden/make_golden.py single)")
