@@ -43,7 +43,9 @@ typedef struct fm_scene fm_scene;
 
 enum {
     FM_FLAG_DEVICE_PTRS = 1, /* buffers are device pointers */
-    FM_FLAG_PROFILE = 2      /* time the wavefront's trace and shade kernels (CUDA events) */
+    FM_FLAG_PROFILE = 2      /* time the wavefront's kernels with CUDA events: the render then runs
+                                as a host loop over graphs of iters_per_graph iterations instead of
+                                one conditional graph launch (slower; profilers see its kernels) */
 };
 
 /* ---- textures ------------------------------------------------------------------ */
@@ -178,8 +180,10 @@ typedef struct {
     int64_t bounces;          /* shading events */
     int64_t nan_samples;      /* samples whose radiance was not finite */
     double kernel_ms;         /* device time of the render kernels */
-    double trace_ms;          /* wavefront trace kernels (with FM_FLAG_PROFILE), else 0 */
-    double shade_ms;          /* wavefront shade kernels (with FM_FLAG_PROFILE), else 0 */
+    double trace_ms;          /* wavefront trace kernels: CUDA events with FM_FLAG_PROFILE, else the
+                                 GPU global timer (first block start to last block end per launch) */
+    double shade_ms;          /* wavefront kernels after the trace (resolve, shading, logic): CUDA
+                                 events with FM_FLAG_PROFILE, else kernel_ms minus trace_ms */
     int64_t launches;         /* kernels launched (graph nodes included) */
 } fm_render_stats;
 
