@@ -126,6 +126,22 @@ FM_D int64_t wagg_append(unsigned* counter, bool want)
     return (int64_t)base + __popc(b & lanemask_lt());
 }
 
+// wagg_append for call sites where lanes of one warp may reach the append with
+// different counters at once (divergent jobs whose appends the compiler may merge):
+// lanes are grouped by counter before the ballot.
+FM_D int64_t wagg_append_grouped(unsigned* counter, bool want)
+{
+    const unsigned mask = __activemask();
+    const unsigned peers = __match_any_sync(mask, (unsigned long long)counter);
+    const unsigned b = __ballot_sync(mask, want) & peers;
+    if (!want) return -1;
+    const int leader = __ffs(b) - 1;
+    unsigned base = 0;
+    if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(counter, (unsigned)__popc(b));
+    base = __shfl_sync(b, base, leader);
+    return (int64_t)base + __popc(b & lanemask_lt());
+}
+
 FM_D void acc_add(float4* a, f3 c)
 {
     atomicAdd(&a->x, c.x);
@@ -709,6 +725,15 @@ FM_D void start_sample(const WfState& st, int slot, const WfView& V, int64_t ite
     if (extra_flags & kReplay) st.dfr[5 * (size_t)slot + 3] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
 }
 
+// One sampling step of a vertex in k_wf_shade, and what the step's gradient needs.
+struct ShadeJob {
+    int kind = 0;   // 1: shadow ray queued, 2: MIS ray queued, 3: continuation queued
+    int64_t q = -1;
+    f3 wi, gw, ge, f, base;
+    float mis = 1.0f, dc = 0.0f;
+    bool sdelta = false, env = false;
+};
+
 // Shading of the slots whose continuation ray hit a surface of material class CLS (the
 // trace kernel queued them): AOVs at the first bounce, next-event estimation (shadow
 // rays), the MIS BSDF samples (MIS rays) and the continuation sample with Russian
@@ -775,151 +800,180 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfState st)
                 st.asum[slot] = as;
                 st.nsum[slot] = ns;
             }
+            // The vertex's sampling steps, in the forward render's random-number order: for
+            // each of direct_loop rounds, NEE of every light and one MIS-BSDF sample; then
+            // the continuation.  Replayed vertices of adjoint renders run the steps as one
+            // flat loop of jobs and evaluate the BSDF's derivatives for each job's direction
+            // at the end of the loop body: one call site keeps the dual-number code in the
+            // instruction caches once instead of three times.
             const float inv_dl = 1.0f / (float)V.cfg.direct_loop;
-            for (int kk = 0; kk < V.cfg.direct_loop; ++kk) {
-                for (int l = 0; l < S.num_lights; ++l) {
-                    const DevLight& L = S.lights[l];
-                    LightSample ls;
-                    bool ok = light_sample(S, L, h.pos, rng_3d(rng), ls);
-                    ok = ok && ls.pdf >= kEpsPdf && length(ls.radiance) >= kEpsPdf;
-                    f3 f = mk(0.0f);
-                    float pb = 0.0f;
-                    if (ok) {
-                        f = bsdf_f<CLS>(b, h.wo, ls.wi);
-                        ok = length(f) >= kEpsPdf;
-                    }
-                    if (ok) {
-                        pb = bsdf_pdf<CLS>(b, h.wo, ls.wi);
-                        ok = pb >= kEpsPdf;
-                    }
-                    const int64_t q = wagg_append(&st.qc[kQcShadow], ok);
-                    if (ok) {
-                        f3 c = beta * (f * ls.radiance * absdot(ls.wi, h.ng)) / ls.pdf;
-                        if (!ls.delta) c *= power_heuristic(ls.pdf, pb);
-                        c *= inv_dl;
-                        if (q < st.cap_sh) {
-                            st.sh_o[q] = make_float4(h.pos.x, h.pos.y, h.pos.z, ls.dist - kEps);
-                            st.sh_d[q] = make_float4(ls.wi.x, ls.wi.y, ls.wi.z, __int_as_float(slot));
-                            st.sh_c[q] = make_float4(c.x, c.y, c.z, __int_as_float(vid));
-                            if (ADJ) {
-                                float4* P = st.sh_g + 3 * q;
-                                if (replay) {
-                                    const float mis = ls.delta ? 1.0f : power_heuristic(ls.pdf, pb);
-                                    const f3 base = beta * (absdot(ls.wi, h.ng) / ls.pdf * mis * inv_dl);
-                                    const float dc = dot(delta, c);   // sum_c dLoss/dc_c * c_c
-                                    float g[kGradParams] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-                                    if (tgt >= 0) {
-                                        BsdfGrads bg;
-                                        bsdf_grads<CLS>(b, h.wo, ls.wi, bg);
-                                        contract(bg.f, delta * base * ls.radiance, g);
-                                        if (!ls.delta)
-                                            for (int i = 0; i < kGradParams; ++i) g[i] -= 2.0f * (1.0f - mis) * dc * bg.dlogp[i];
-                                    }
-                                    const bool env = L.kind == LK_ENV;
-                                    const f3 e = env ? delta * base * f : mk(0.0f);
-                                    const float senv = env ? 2.0f * (1.0f - mis) * dc : 0.0f;
-                                    P[0] = make_float4(g[0], g[1], g[2], g[3]);
-                                    P[1] = make_float4(g[4], h.u, h.v, __int_as_float(tgt));
-                                    P[2] = make_float4(e.x, e.y, e.z, senv);
-                                }
-                            }
-                            flags |= kPending;
-                        } else {
-                            atomicOr(st.status, 2u);
-                        }
-                    }
+            const int nl = S.num_lights;
+            auto nee_job = [&](int r, ShadeJob& J) {
+                const DevLight& L = S.lights[r];
+                LightSample ls;
+                bool ok = light_sample(S, L, h.pos, rng_3d(rng), ls);
+                ok = ok && ls.pdf >= kEpsPdf && length(ls.radiance) >= kEpsPdf;
+                float pb = 0.0f;
+                f3 f = mk(0.0f);
+                if (ok) {
+                    f = bsdf_f<CLS>(b, h.wo, ls.wi);
+                    ok = length(f) >= kEpsPdf;
                 }
+                if (ok) {
+                    pb = bsdf_pdf<CLS>(b, h.wo, ls.wi);
+                    ok = pb >= kEpsPdf;
+                }
+                const int64_t q = ADJ ? wagg_append_grouped(&st.qc[kQcShadow], ok) : wagg_append(&st.qc[kQcShadow], ok);
+                if (!ok) return;
+                f3 c = beta * (f * ls.radiance * absdot(ls.wi, h.ng)) / ls.pdf;
+                if (!ls.delta) c *= power_heuristic(ls.pdf, pb);
+                c *= inv_dl;
+                if (q >= st.cap_sh) {
+                    atomicOr(st.status, 2u);
+                    return;
+                }
+                st.sh_o[q] = make_float4(h.pos.x, h.pos.y, h.pos.z, ls.dist - kEps);
+                st.sh_d[q] = make_float4(ls.wi.x, ls.wi.y, ls.wi.z, __int_as_float(slot));
+                st.sh_c[q] = make_float4(c.x, c.y, c.z, __int_as_float(vid));
+                flags |= kPending;
+                if (ADJ) {
+                    J.kind = 1;
+                    J.q = q;
+                    J.wi = ls.wi;
+                    J.f = f;
+                    J.mis = ls.delta ? 1.0f : power_heuristic(ls.pdf, pb);
+                    J.base = beta * (absdot(ls.wi, h.ng) / ls.pdf * J.mis * inv_dl);
+                    J.dc = dot(delta, c);   // sum_c dLoss/dc_c * c_c
+                    J.gw = delta * J.base * ls.radiance;
+                    J.sdelta = ls.delta;
+                    J.env = L.kind == LK_ENV;
+                }
+            };
+            auto mis_job = [&](ShadeJob& J) {
                 const BsdfSample ms = bsdf_sample<CLS>(b, h.wo, rng_3d(rng));
                 const bool ok = length(ms.f) >= kEpsPdf && ms.pdf >= kEpsPdf;
-                const int64_t q = wagg_append(&st.qc[kQcMis], ok);
-                if (ok) {
-                    const f3 wi = normalize(ms.wi);
-                    const f3 ro = spawn_origin(h, wi);
-                    const f3 A = beta * ms.f * absdot(h.ng, wi) / ms.pdf * inv_dl;
-                    if (q < st.cap_mis) {
-                        st.mis_o[q] = make_float4(ro.x, ro.y, ro.z, __int_as_float(slot));
-                        st.mis_d[q] = make_float4(wi.x, wi.y, wi.z, ms.delta ? -1.0f : ms.pdf);
-                        st.mis_a[q] = make_float4(A.x, A.y, A.z, __int_as_float(vid));
-                        if (ADJ) {
-                            float4* P = st.mis_g + 8 * q;
-                            if (replay) {
-                                float B[15], a[kGradParams], bb[kGradParams];
-                                for (int k = 0; k < 15; ++k) B[k] = 0.0f;
-                                for (int k = 0; k < kGradParams; ++k) a[k] = bb[k] = 0.0f;
-                                if (tgt >= 0) {
-                                    BsdfGrads bg;
-                                    bsdf_grads<CLS>(b, h.wo, ms.wi, bg);
-                                    const f3 base = delta * beta * (absdot(h.ng, wi) / ms.pdf * inv_dl);
-                                    for (int i = 0; i < kGradParams; ++i) {
-                                        B[i] = base.x * bg.f.x.d[i];
-                                        B[5 + i] = base.y * bg.f.y.d[i];
-                                        B[10 + i] = base.z * bg.f.z.d[i];
-                                    }
-                                    if (!ms.delta)
-                                        for (int i = 0; i < kGradParams; ++i) {
-                                            a[i] = bg.dscore[i];
-                                            bb[i] = 2.0f * bg.dlogp[i];
-                                        }
-                                }
-                                const f3 e = delta * A;
-                                P[0] = make_float4(B[0], B[1], B[2], B[3]);
-                                P[1] = make_float4(B[4], B[5], B[6], B[7]);
-                                P[2] = make_float4(B[8], B[9], B[10], B[11]);
-                                P[3] = make_float4(B[12], B[13], B[14], __int_as_float(tgt));
-                                P[4] = make_float4(h.u, h.v, e.x, e.y);
-                                P[5] = make_float4(e.z, a[0], a[1], a[2]);
-                                P[6] = make_float4(a[3], a[4], bb[0], bb[1]);
-                                P[7] = make_float4(bb[2], bb[3], bb[4], 0.0f);
-                            }
-                        }
-                        flags |= kPending;
-                    } else {
-                        atomicOr(st.status, 2u);
-                    }
+                const int64_t q = ADJ ? wagg_append_grouped(&st.qc[kQcMis], ok) : wagg_append(&st.qc[kQcMis], ok);
+                if (!ok) return;
+                const f3 wn = normalize(ms.wi);
+                const f3 ro = spawn_origin(h, wn);
+                const f3 A = beta * ms.f * absdot(h.ng, wn) / ms.pdf * inv_dl;
+                if (q >= st.cap_mis) {
+                    atomicOr(st.status, 2u);
+                    return;
                 }
-            }
-            const BsdfSample sc = bsdf_sample<CLS>(b, h.wo, rng_3d(rng));
-            if (length(sc.f) >= kEpsPdf && sc.pdf >= kEpsPdf) {
+                st.mis_o[q] = make_float4(ro.x, ro.y, ro.z, __int_as_float(slot));
+                st.mis_d[q] = make_float4(wn.x, wn.y, wn.z, ms.delta ? -1.0f : ms.pdf);
+                st.mis_a[q] = make_float4(A.x, A.y, A.z, __int_as_float(vid));
+                flags |= kPending;
+                if (ADJ) {
+                    J.kind = 2;
+                    J.q = q;
+                    J.wi = ms.wi;
+                    J.gw = delta * beta * (absdot(h.ng, wn) / ms.pdf * inv_dl);
+                    J.ge = delta * A;
+                    J.sdelta = ms.delta;
+                }
+            };
+            auto cont_job = [&](ShadeJob& J) {
+                const BsdfSample sc = bsdf_sample<CLS>(b, h.wo, rng_3d(rng));
+                if (!(length(sc.f) >= kEpsPdf && sc.pdf >= kEpsPdf)) return;
                 beta *= sc.f * absdot(h.ng, sc.wi) / sc.pdf;
-                if (depth < V.cfg.depth) {
-                    bool go = true;
-                    if (V.cfg.rr_enabled) {
-                        if (rng_1d(rng) > V.cfg.rr_coef)
-                            go = false;
-                        else
-                            beta /= V.cfg.rr_coef;
-                    }
-                    if (go) {
-                        const f3 no = spawn_origin(h, sc.wi);
-                        st.ro[slot] = make_float4(no.x, no.y, no.z, 0.0f);
-                        st.rd[slot] = make_float4(sc.wi.x, sc.wi.y, sc.wi.z, 0.0f);
-                        st.beta[slot] = make_float4(beta.x, beta.y, beta.z, 0.0f);
-                        flags = kNextCont | (flags & (kPending | kReplay)) | ((depth + 1) << 8);
-                        enqueue_cont = true;
-                        if (ADJ && replay) {
-                            // d log (f / pdf_b) / dp at the continuation direction (and the
-                            // score of the sampler's density), used when the vertex's
-                            // record is flushed
-                            float4* D = st.dfr + 5 * (size_t)slot;
-                            if (tgt >= 0) {
-                                BsdfGrads bg;
-                                bsdf_grads<CLS>(b, h.wo, sc.wi, bg);
-                                const DV3& fd = bg.f;
-                                const float* dscore = bg.dscore;
-                                float dl[15];
-                                for (int i = 0; i < kGradParams; ++i) {
-                                    dl[i] = fd.x.v > 0.0f ? fd.x.d[i] / fd.x.v + dscore[i] : 0.0f;
-                                    dl[5 + i] = fd.y.v > 0.0f ? fd.y.d[i] / fd.y.v + dscore[i] : 0.0f;
-                                    dl[10 + i] = fd.z.v > 0.0f ? fd.z.d[i] / fd.z.v + dscore[i] : 0.0f;
-                                }
-                                D[0] = make_float4(dl[0], dl[1], dl[2], dl[3]);
-                                D[1] = make_float4(dl[4], dl[5], dl[6], dl[7]);
-                                D[2] = make_float4(dl[8], dl[9], dl[10], dl[11]);
-                                D[3] = make_float4(dl[12], dl[13], dl[14], __int_as_float(tgt));
-                            }
+                if (depth >= V.cfg.depth) return;
+                if (V.cfg.rr_enabled) {
+                    if (rng_1d(rng) > V.cfg.rr_coef) return;
+                    beta /= V.cfg.rr_coef;
+                }
+                const f3 no = spawn_origin(h, sc.wi);
+                st.ro[slot] = make_float4(no.x, no.y, no.z, 0.0f);
+                st.rd[slot] = make_float4(sc.wi.x, sc.wi.y, sc.wi.z, 0.0f);
+                st.beta[slot] = make_float4(beta.x, beta.y, beta.z, 0.0f);
+                flags = kNextCont | (flags & (kPending | kReplay)) | ((depth + 1) << 8);
+                enqueue_cont = true;
+                if (ADJ) {
+                    J.kind = 3;
+                    J.wi = sc.wi;
+                }
+            };
+            if constexpr (ADJ) {
+                const int njobs = V.cfg.direct_loop * (nl + 1) + 1;
+                for (int j = 0; j < njobs; ++j) {
+                    const int r = j == njobs - 1 ? -1 : j % (nl + 1);
+                    ShadeJob J;
+                    if (r < 0)
+                        cont_job(J);
+                    else if (r == nl)
+                        mis_job(J);
+                    else
+                        nee_job(r, J);
+                    if (J.kind == 0) continue;
+                    BsdfGrads bg;
+                    const bool grads = tgt >= 0 && !(J.kind == 2 && J.sdelta && CLS == kClsSimple);
+                    if (grads) bsdf_grads<CLS>(b, h.wo, J.wi, bg);
+                    if (J.kind == 1) {
+                        // NEE: df/dp weighted by dLoss/dI beta Le cos w_l / pdf_l, and the MIS
+                        // weight's dependence on pdf_b
+                        float g[kGradParams] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+                        if (grads) {
+                            contract(bg.f, J.gw, g);
+                            if (!J.sdelta)
+                                for (int i = 0; i < kGradParams; ++i) g[i] -= 2.0f * (1.0f - J.mis) * J.dc * bg.dlogp[i];
                         }
+                        const f3 e = J.env ? delta * J.base * J.f : mk(0.0f);
+                        const float senv = J.env ? 2.0f * (1.0f - J.mis) * J.dc : 0.0f;
+                        float4* P = st.sh_g + 3 * J.q;
+                        P[0] = make_float4(g[0], g[1], g[2], g[3]);
+                        P[1] = make_float4(g[4], h.u, h.v, __int_as_float(tgt));
+                        P[2] = make_float4(e.x, e.y, e.z, senv);
+                    } else if (J.kind == 2) {
+                        // MIS: df/dp per channel (Le and the MIS weight are known only
+                        // after the trace), the density terms, and the env weight
+                        float B[15], a[kGradParams], bb[kGradParams];
+                        for (int k = 0; k < 15; ++k) B[k] = 0.0f;
+                        for (int k = 0; k < kGradParams; ++k) a[k] = bb[k] = 0.0f;
+                        if (grads) {
+                            for (int i = 0; i < kGradParams; ++i) {
+                                B[i] = J.gw.x * bg.f.x.d[i];
+                                B[5 + i] = J.gw.y * bg.f.y.d[i];
+                                B[10 + i] = J.gw.z * bg.f.z.d[i];
+                            }
+                            if (!J.sdelta)
+                                for (int i = 0; i < kGradParams; ++i) {
+                                    a[i] = bg.dscore[i];
+                                    bb[i] = 2.0f * bg.dlogp[i];
+                                }
+                        }
+                        float4* P = st.mis_g + 8 * J.q;
+                        P[0] = make_float4(B[0], B[1], B[2], B[3]);
+                        P[1] = make_float4(B[4], B[5], B[6], B[7]);
+                        P[2] = make_float4(B[8], B[9], B[10], B[11]);
+                        P[3] = make_float4(B[12], B[13], B[14], __int_as_float(tgt));
+                        P[4] = make_float4(h.u, h.v, J.ge.x, J.ge.y);
+                        P[5] = make_float4(J.ge.z, a[0], a[1], a[2]);
+                        P[6] = make_float4(a[3], a[4], bb[0], bb[1]);
+                        P[7] = make_float4(bb[2], bb[3], bb[4], 0.0f);
+                    } else if (grads) {
+                        // continuation: d log (f / pdf_b) / dp and the score of the
+                        // sampler's density, used when the vertex's record is flushed
+                        float dl[15];
+                        for (int i = 0; i < kGradParams; ++i) {
+                            dl[i] = bg.f.x.v > 0.0f ? bg.f.x.d[i] / bg.f.x.v + bg.dscore[i] : 0.0f;
+                            dl[5 + i] = bg.f.y.v > 0.0f ? bg.f.y.d[i] / bg.f.y.v + bg.dscore[i] : 0.0f;
+                            dl[10 + i] = bg.f.z.v > 0.0f ? bg.f.z.d[i] / bg.f.z.v + bg.dscore[i] : 0.0f;
+                        }
+                        float4* D = st.dfr + 5 * (size_t)slot;
+                        D[0] = make_float4(dl[0], dl[1], dl[2], dl[3]);
+                        D[1] = make_float4(dl[4], dl[5], dl[6], dl[7]);
+                        D[2] = make_float4(dl[8], dl[9], dl[10], dl[11]);
+                        D[3] = make_float4(dl[12], dl[13], dl[14], __int_as_float(tgt));
                     }
                 }
+            } else {
+                ShadeJob J;
+                for (int kk = 0; kk < V.cfg.direct_loop; ++kk) {
+                    for (int r = 0; r < nl; ++r) nee_job(r, J);
+                    mis_job(J);
+                }
+                cont_job(J);
             }
             st.rng[slot] = rng.state;
             st.flags[slot] = flags;

@@ -6,9 +6,12 @@ variance of those means.  The golden fixture holds the reference's per-pixel mea
 single-sample variance at 4096 spp (tests/golden/make_golden.py).  Checks:
   * per-pixel 3-sigma agreement: |mu_gpu - mu_ref| <= 3 sqrt(var_gpu/N + var_ref/N);
     about 0.27% of pixel channels fail under pure noise, the bound is 1%;
-  * relMSE = mean((mu_gpu - mu_ref)^2 / (mu_ref^2 + 1e-2)); with both estimators at 4096
-    spp it contains their noise, so the test bounds relMSE minus its expected noise part
-    (the squared bias) by 1e-3 and reports both;
+  * relMSE = mean((mu_gpu - mu_ref)^2 / (mu_ref^2 + 1e-2)); it contains both estimators'
+    noise, so the test bounds relMSE minus its expected noise part (the squared bias) by
+    1e-3 plus three standard errors of the relMSE estimate itself (the sample standard
+    deviation of the per-channel terms over sqrt(n)): on noisy tiles (caustics, a sharp
+    sun) the noise term is large and the mean of n heavy-tailed terms scatters around it;
+    on converged ones the standard error is small and 1e-3 is the bound;
   * albedo and normal AOVs (first-hit averages) agree to 2e-2 mean absolute difference.
 """
 import json
@@ -51,11 +54,18 @@ def compare(rgb_batches, g):
     r = g["mean"].astype(np.float64)
     var_r = g["var"].astype(np.float64) / float(g["spp"])
     den = r * r + 1e-2
-    relmse = float(np.mean((mu - r) ** 2 / den))
+    terms = (mu - r) ** 2 / den
+    relmse = float(np.mean(terms))
+    se = float(np.std(terms, ddof=1) / np.sqrt(terms.size))
     noise = float(np.mean((var_mu + var_r) / den))
     z = np.abs(mu - r) / np.sqrt(var_mu + var_r + 1e-12)
-    return {"relmse": relmse, "relmse_noise": noise, "relmse_bias": relmse - noise,
+    return {"relmse": relmse, "relmse_noise": noise, "relmse_bias": relmse - noise, "relmse_se": se,
             "frac_3sigma": float(np.mean(z > 3.0)), "pixels": int(np.prod(r.shape[:2]))}
+
+
+def assert_parity(res):
+    assert res["frac_3sigma"] < 0.01, res
+    assert res["relmse_bias"] < 1e-3 + 3.0 * res["relmse_se"], res
 
 
 @pytest.mark.gpu
@@ -76,8 +86,7 @@ def test_converged_image_matches_reference(ctx, case, mode):
         with open(RESULTS / "image_parity.jsonl", "a") as f:
             f.write(json.dumps(res) + "\n")
     assert np.all(np.isfinite(rgb))
-    assert res["frac_3sigma"] < 0.01, res
-    assert res["relmse_bias"] < 1e-3, res
+    assert_parity(res)
     assert res["albedo_mad"] < 2e-2 and res["normal_mad"] < 2e-2, res
 
 
@@ -138,8 +147,7 @@ def test_batched_scenes_match_reference(ctx, mode):
         if RESULTS.is_dir():
             with open(RESULTS / "image_parity.jsonl", "a") as f:
                 f.write(json.dumps(res) + "\n")
-        assert res["frac_3sigma"] < 0.01, res
-        assert res["relmse_bias"] < 1e-3, res
+        assert_parity(res)
 
 
 @pytest.mark.gpu
@@ -164,5 +172,4 @@ def test_single_mesh_scene_matches_reference(ctx, mode):
         if RESULTS.is_dir():
             with open(RESULTS / "image_parity.jsonl", "a") as f:
                 f.write(json.dumps(res) + "\n")
-        assert res["frac_3sigma"] < 0.01, res
-        assert res["relmse_bias"] < 1e-3, res
+        assert_parity(res)
