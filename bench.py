@@ -460,9 +460,9 @@ def main():
     achieved = alg_bytes / (totals["trace_ms"] / 1e3) / 1e9 if totals["trace_ms"] > 0 else None
     # six launches per wavefront iteration (prep, trace, resolve, two shade kernels,
     # logic), one loop-condition kernel per graph body of iters_per_graph iterations,
-    # and one init and one reduce per view per step
+    # and per step one init, one counter copy and one reduce per view
     it = tuning.iters_per_graph
-    launches_trace = max(1, (totals["launches"] - args.steps * (1 + len(specs))) * it // (6 * it + 1))
+    launches_trace = max(1, (totals["launches"] - args.steps * (2 + len(specs))) * it // (6 * it + 1))
     traffic = None
     if TRACE_DRAM_BYTES_PER_RAY is not None:
         traffic = TRACE_DRAM_BYTES_PER_RAY * (totals["closest"] + totals["shadow"]) / launches_trace

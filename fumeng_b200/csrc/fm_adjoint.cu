@@ -205,6 +205,7 @@ extern "C" fm_status fm_render_adjoint(fm_ctx* ctx, const fm_scene* scene, int32
             WfView& v = views[i];
             v = WfView{};
             v.scene = scene->d_dev;
+            v.num_lights = scene->dev.num_lights;
             v.cam = make_camera(cams[i]);
             v.cfg = make_cfg(params[i]);
             v.rgb = rgb_out[i];

@@ -48,6 +48,7 @@ std::vector<WfView> make_views(int n, const fm_scene* const* scenes, const fm_ca
         WfView& w = v[i];
         w = WfView{};
         w.scene = scenes[i]->d_dev;
+        w.num_lights = scenes[i]->dev.num_lights;
         w.cam = make_camera(cams[i]);
         fm_render_params p = params[i];
         if (spp_override > 0) p.spp = std::min(p.spp, spp_override);

@@ -218,6 +218,7 @@ void fm_ctx_destroy(fm_ctx* ctx)
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    fm::wf_cache_release(ctx);
     cudaFree(ctx->d_status);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;

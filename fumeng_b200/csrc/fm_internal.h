@@ -9,6 +9,11 @@
 #include "fm_bvh_build.h"
 #include "fm_scene.cuh"
 
+namespace fm {
+struct WfCache;   // wavefront workspace (fm_wavefront.cu)
+void wf_cache_release(fm_ctx* ctx);
+}  // namespace fm
+
 struct fm_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -17,6 +22,9 @@ struct fm_ctx {
     int num_sms = 148;
     // autotuned wavefront settings per batch shape class (views, log2 samples, max lights)
     std::map<std::tuple<int, int, int>, fm_tuning> tune_cache;
+    // wavefront workspaces (forward, adjoint): state buffers, pinned staging and the
+    // instantiated graph, kept between renders
+    fm::WfCache* wf_cache[2] = {nullptr, nullptr};
 };
 
 struct fm_scene {

@@ -22,6 +22,7 @@ struct WfView {
     float* alb;
     float* nrm;
     const float* drgb;       // adjoint renders: dLoss/dI per pixel (device, w*h*3)
+    int32_t num_lights;      // the scene's light count (host copy, sizes the shadow queue)
 };
 
 // Gradient accumulators of an adjoint render (device buffers, zeroed by the caller).

@@ -25,6 +25,7 @@
 // partial sums once; a final kernel sums the chunks of each pixel in chunk order.  When
 // a path ends, its slot immediately starts the next sample (path regeneration).
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "fm_bsdf_grad.cuh"
@@ -1157,9 +1158,186 @@ __global__ void k_wf_reduce(WfView V)
     }
 }
 
+// Adds the counters of one render (workspace-owned, so that the cached graph's launch
+// state does not depend on the caller's buffer) to the caller's.
+__global__ void k_counters_add(Counters* dst, const Counters* src)
+{
+    dst->paths += src->paths;
+    dst->closest += src->closest;
+    dst->shadow += src->shadow;
+    dst->bounces += src->bounces;
+    dst->nans += src->nans;
+}
+
 }  // namespace
 
+// The wavefront workspace of a context: the path-state and queue buffers (sized by the
+// largest pool and queue capacities seen so far), the per-view partial sums, pinned
+// host staging, events, and the instantiated graph with the launch state it was built
+// for.  Renders of one batch shape class reuse all of it, so a render costs the host
+// a views upload, a few memsets and one graph launch.
+struct WfCache {
+    bool adj = false;
+    int64_t pool = 0, cap_mis = 0, cap_sh = 0, partial_f4 = 0;
+    int32_t nviews = 0;
+    std::vector<void*> allocs;   // state buffers
+    WfState bufs;                // their pointers
+    float4* partial = nullptr;
+    WfView* d_views = nullptr;
+    Counters* cnt = nullptr;
+    WfView* h_views = nullptr;   // pinned
+    void* h_block = nullptr;     // pinned: queue counters, status word, trace spans
+    unsigned* h_qc = nullptr;
+    uint32_t* h_status = nullptr;
+    unsigned long long* h_span = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::vector<cudaEvent_t> pev;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    WfState g_st;
+    int64_t g_pool = 0, g_max_launches = 0;
+    int g_trace_block = 0, g_shade_block = 0, g_iters = 0;
+    bool g_profile = false;
+    WfCache()
+    {
+        std::memset(&bufs, 0, sizeof(bufs));
+        std::memset(&g_st, 0, sizeof(g_st));
+    }
+};
+
 namespace {
+
+void wf_cache_drop_graph(WfCache& c)
+{
+    if (c.exec) cudaGraphExecDestroy(c.exec);
+    if (c.graph) cudaGraphDestroy(c.graph);
+    c.exec = nullptr;
+    c.graph = nullptr;
+}
+
+void wf_cache_free_state(WfCache& c, cudaStream_t s)
+{
+    for (void* p : c.allocs) cudaFreeAsync(p, s);
+    c.allocs.clear();
+    std::memset(&c.bufs, 0, sizeof(c.bufs));
+    c.pool = c.cap_mis = c.cap_sh = 0;
+}
+
+// Makes the workspace of `ctx` (forward or adjoint) hold at least the given capacities.
+fm_status wf_cache_reserve(fm_ctx* ctx, bool adj, int64_t pool, int64_t cap_mis, int64_t cap_sh, int64_t partial_f4,
+                           int32_t nviews, WfCache*& out)
+{
+    cudaStream_t s = ctx->stream;
+    WfCache*& c = ctx->wf_cache[adj ? 1 : 0];
+    if (!c) {
+        c = new WfCache();
+        c->adj = adj;
+        const size_t hb = sizeof(unsigned) * kQcCount + sizeof(uint32_t) * 4 + sizeof(unsigned long long) * 4;
+        if (cudaEventCreate(&c->e0) != cudaSuccess || cudaEventCreate(&c->e1) != cudaSuccess ||
+            cudaMallocHost(&c->h_block, hb) != cudaSuccess || cudaMallocAsync((void**)&c->cnt, sizeof(Counters), s) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(ctx, FM_ERR_OOM, "wavefront: workspace allocation failed");
+        }
+        char* hp = static_cast<char*>(c->h_block);
+        c->h_span = reinterpret_cast<unsigned long long*>(hp);
+        c->h_qc = reinterpret_cast<unsigned*>(hp + sizeof(unsigned long long) * 4);
+        c->h_status = reinterpret_cast<uint32_t*>(hp + sizeof(unsigned long long) * 4 + sizeof(unsigned) * kQcCount);
+    }
+    if (nviews > c->nviews) {
+        wf_cache_drop_graph(*c);
+        if (c->d_views) cudaFreeAsync(c->d_views, s);
+        if (c->h_views) {
+            cudaStreamSynchronize(s);
+            cudaFreeHost(c->h_views);
+        }
+        c->d_views = nullptr;
+        c->h_views = nullptr;
+        c->nviews = 0;
+        if (cudaMallocAsync((void**)&c->d_views, sizeof(WfView) * (size_t)nviews, s) != cudaSuccess ||
+            cudaMallocHost((void**)&c->h_views, sizeof(WfView) * (size_t)nviews) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(ctx, FM_ERR_OOM, "wavefront: view table allocation failed");
+        }
+        c->nviews = nviews;
+    }
+    if (partial_f4 > c->partial_f4) {
+        if (c->partial) cudaFreeAsync(c->partial, s);
+        c->partial = nullptr;
+        c->partial_f4 = 0;
+        if (cudaMallocAsync((void**)&c->partial, sizeof(float4) * (size_t)partial_f4, s) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(ctx, FM_ERR_OOM, "wavefront: partial buffer allocation failed");
+        }
+        c->partial_f4 = partial_f4;
+    }
+    if (pool > c->pool || cap_mis > c->cap_mis || cap_sh > c->cap_sh) {
+        wf_cache_drop_graph(*c);
+        pool = std::max(pool, c->pool);
+        cap_mis = std::max(cap_mis, c->cap_mis);
+        cap_sh = std::max(cap_sh, c->cap_sh);
+        wf_cache_free_state(*c, s);
+        WfState& b = c->bufs;
+        bool ok = true;
+        auto A = [&](auto*& p, size_t count) {
+            void* q = nullptr;
+            if (ok && cudaMallocAsync(&q, sizeof(*p) * count, s) == cudaSuccess) {
+                c->allocs.push_back(q);
+                p = static_cast<std::remove_reference_t<decltype(p)>>(q);
+            } else {
+                ok = false;
+            }
+        };
+        A(b.next_item, 1);
+        A(b.item, pool);
+        A(b.k, pool);
+        A(b.view, pool);
+        A(b.flags, pool);
+        A(b.rng, pool);
+        A(b.beta, pool);
+        A(b.col, pool);
+        A(b.ro, pool);
+        A(b.rd, pool);
+        A(b.hit, pool);
+        A(b.acc, pool);
+        A(b.isum, pool);
+        A(b.icomp, pool);
+        A(b.asum, pool);
+        A(b.nsum, pool);
+        A(b.cont_q, pool);
+        A(b.disney_q, pool);
+        A(b.simple_q, pool);
+        A(b.mis_o, cap_mis);
+        A(b.mis_d, cap_mis);
+        A(b.mis_a, cap_mis);
+        A(b.mis_h, cap_mis);
+        A(b.sh_o, cap_sh);
+        A(b.sh_d, cap_sh);
+        A(b.sh_c, cap_sh);
+        A(b.sh_h, cap_sh);
+        A(b.qc, kQcCount);
+        A(b.tspan, 4);
+        if (adj) {
+            A(b.disney_r, pool);
+            A(b.simple_r, pool);
+            A(b.lp, pool);
+            A(b.dfr, 5 * (size_t)pool);
+            A(b.vg, 2 * (size_t)pool);
+            A(b.gq, 3 * 2 * (size_t)pool);
+            A(b.sh_g, 3 * (size_t)cap_sh);
+            A(b.mis_g, 8 * (size_t)cap_mis);
+        }
+        if (!ok) {
+            cudaGetLastError();
+            wf_cache_free_state(*c, s);
+            return set_error(ctx, FM_ERR_OOM, "wavefront: state allocation failed");
+        }
+        c->pool = pool;
+        c->cap_mis = cap_mis;
+        c->cap_sh = cap_sh;
+    }
+    out = c;
+    return FM_OK;
+}
 
 template <bool ADJ>
 fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const WfTuning& tune, const WfAdjoint* adj,
@@ -1173,26 +1351,11 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
     for (const auto& v : views) {
         total_samples += (double)v.cfg.width * v.cfg.height * v.cfg.spp;
         max_dl = std::max(max_dl, v.cfg.direct_loop);
-    }
-    for (const auto& v : views) {
-        DevScene hs;
-        FM_CUDA_TRY(ctx, cudaMemcpy(&hs, v.scene, sizeof(DevScene), cudaMemcpyDeviceToHost), "wavefront scene");
-        max_lights = std::max(max_lights, hs.num_lights);
+        max_lights = std::max(max_lights, v.num_lights);
     }
     const int64_t pool = std::max<int64_t>(1024, std::min<int64_t>(tune.pool, (int64_t)total_samples));
     const double per_item = total_samples / (4.0 * (double)pool);
-    int64_t item_base = 0;
-    std::vector<void*> allocs;
-    auto alloc = [&](size_t bytes) -> void* {
-        void* p = nullptr;
-        if (cudaMallocAsync(&p, bytes, s) != cudaSuccess) return nullptr;
-        allocs.push_back(p);
-        return p;
-    };
-    auto free_all = [&]() {
-        for (void* p : allocs) cudaFreeAsync(p, s);
-        allocs.clear();
-    };
+    int64_t item_base = 0, partial_f4 = 0;
     for (auto& v : views) {
         int chunk = (int)std::floor(per_item);
         chunk = std::max(1, std::min(chunk, v.cfg.spp));
@@ -1201,100 +1364,56 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
         v.item_base = item_base;
         const int64_t npix = (int64_t)v.cfg.width * v.cfg.height;
         item_base += npix * v.nchunks;
-        v.partial = static_cast<float4*>(alloc(sizeof(float4) * 3 * (size_t)(npix * v.nchunks)));
-        if (!v.partial) {
-            free_all();
-            return set_error(ctx, FM_ERR_OOM, "wavefront: partial buffer allocation failed");
+        partial_f4 += 3 * npix * v.nchunks;
+    }
+    WfCache* c = nullptr;
+    fm_status result = wf_cache_reserve(ctx, ADJ, pool, pool * max_dl, pool * max_dl * (int64_t)max_lights, partial_f4,
+                                        (int32_t)views.size(), c);
+    if (result != FM_OK) return result;
+    {
+        float4* p = c->partial;
+        for (auto& v : views) {
+            v.partial = p;
+            p += 3 * (int64_t)v.cfg.width * v.cfg.height * v.nchunks;
         }
     }
-    WfState st{};
+    // the launch state: the workspace's buffers, this call's sizes
+    WfState st;
+    std::memcpy(&st, &c->bufs, sizeof(st));
     st.pool = pool;
     st.nviews = (int32_t)views.size();
     st.total_items = item_base;
     st.cap_cont = pool;
     st.cap_mis = pool * max_dl;
     st.cap_sh = pool * max_dl * (int64_t)max_lights;
-    bool ok = true;
-    auto A = [&](auto*& p, size_t count) {
-        p = static_cast<std::remove_reference_t<decltype(p)>>(alloc(sizeof(*p) * count));
-        ok = ok && p != nullptr;
-    };
-    WfView* d_views = nullptr;
-    A(d_views, views.size());
-    A(st.next_item, 1);
-    A(st.item, pool);
-    A(st.k, pool);
-    A(st.view, pool);
-    A(st.flags, pool);
-    A(st.rng, pool);
-    A(st.beta, pool);
-    A(st.col, pool);
-    A(st.ro, pool);
-    A(st.rd, pool);
-    A(st.hit, pool);
-    A(st.acc, pool);
-    A(st.isum, pool);
-    A(st.icomp, pool);
-    A(st.asum, pool);
-    A(st.nsum, pool);
-    A(st.cont_q, st.cap_cont);
-    A(st.disney_q, pool);
-    A(st.simple_q, pool);
+    st.views = c->d_views;
+    st.cnt = c->cnt;
+    st.status = ctx->d_status;
     if (ADJ) {
-        A(st.disney_r, pool);
-        A(st.simple_r, pool);
-    }
-    A(st.mis_o, st.cap_mis);
-    A(st.mis_d, st.cap_mis);
-    A(st.mis_a, st.cap_mis);
-    A(st.sh_o, st.cap_sh);
-    A(st.sh_d, st.cap_sh);
-    A(st.sh_c, st.cap_sh);
-    A(st.mis_h, st.cap_mis);
-    A(st.sh_h, st.cap_sh);
-    A(st.qc, kQcCount);
-    A(st.tspan, 4);
-    if (ADJ) {
-        A(st.lp, pool);
-        A(st.dfr, 5 * (size_t)pool);
-        A(st.vg, 2 * (size_t)pool);
         st.cap_grad = 2 * pool;   // a slot can finish two vertices in one iteration
-        A(st.gq, 3 * (size_t)st.cap_grad);
-        A(st.sh_g, 3 * (size_t)st.cap_sh);
-        A(st.mis_g, 8 * (size_t)st.cap_mis);
         st.tex_acc = adj->tex_acc;
         st.tex_copies = adj->tex_copies;
         st.mat_acc = adj->mat_acc;
         st.env_row = adj->env_row;
         st.env_total = adj->env_total;
     }
-    if (!ok) {
-        free_all();
-        return set_error(ctx, FM_ERR_OOM, "wavefront: state allocation failed");
-    }
-    st.views = d_views;
-    st.cnt = cnt;
-    st.status = ctx->d_status;
-    FM_CUDA_TRY(ctx, cudaMemcpyAsync(d_views, views.data(), sizeof(WfView) * views.size(), cudaMemcpyHostToDevice, s),
+    // the previous call ended with a stream synchronisation, so the pinned staging is free
+    std::memcpy(c->h_views, views.data(), sizeof(WfView) * views.size());
+    FM_CUDA_TRY(ctx, cudaMemcpyAsync(c->d_views, c->h_views, sizeof(WfView) * views.size(), cudaMemcpyHostToDevice, s),
                 "wavefront views");
     FM_CUDA_TRY(ctx, cudaMemsetAsync(st.next_item, 0, sizeof(unsigned long long), s), "wavefront");
     FM_CUDA_TRY(ctx, cudaMemsetAsync(st.qc, 0, sizeof(unsigned) * kQcCount, s), "wavefront");
     FM_CUDA_TRY(ctx, cudaMemsetAsync(st.tspan, 0, sizeof(unsigned long long) * 4, s), "wavefront");
+    FM_CUDA_TRY(ctx, cudaMemsetAsync(c->cnt, 0, sizeof(Counters), s), "wavefront");
     const int sms = ctx->num_sms;
     k_wf_init<<<sms * 8, 256, 0, s>>>(st);
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0, s);
+    cudaEventRecord(c->e0, s);
     // one graph body = `iters_per_graph` iterations of prep -> trace -> resolve -> shade
     // (Disney) -> shade (other materials) [-> replay shading] -> logic [-> gradient scatter]
     const int trace_grid = sms * 16;
     const int shade_grid = (int)std::min<int64_t>((pool + tune.shade_block - 1) / tune.shade_block, (int64_t)sms * 32);
     const int logic_grid = (int)std::min<int64_t>((pool + 255) / 256, (int64_t)sms * 32);
     const int resolve_grid = sms * 16;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    fm_status result = FM_OK;
     // Bound on iterations: every sample takes at most depth + 1 iterations and a slot
     // runs its samples one after another.
     int max_depth = 1, max_chunk = 1;
@@ -1306,10 +1425,13 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
         (total_samples / (double)pool + 4.0 * max_chunk + 8.0) * (max_depth + 2) * 4.0 * (ADJ ? 2.0 : 1.0) + 1000.0;
     const int64_t max_launches = (int64_t)(iter_bound / tune.iters_per_graph) + 16;
     // optional per-kernel timing: event-record nodes around every trace and shade launch
-    std::vector<cudaEvent_t> pev;
+    std::vector<cudaEvent_t>& pev = c->pev;
     if (tune.profile) {
-        pev.resize(3 * (size_t)tune.iters_per_graph);
-        for (auto& ev : pev) cudaEventCreate(&ev);
+        while (pev.size() < 3 * (size_t)tune.iters_per_graph) {
+            cudaEvent_t ev = nullptr;
+            cudaEventCreate(&ev);
+            pev.push_back(ev);
+        }
     }
     double trace_ms = 0.0, shade_ms = 0.0;
     auto capture_iterations = [&]() {
@@ -1331,71 +1453,87 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
         }
     };
     cudaError_t e = cudaSuccess;
-    if (!tune.profile) {
-        // The whole render is one launch: a conditional WHILE node repeats the body
-        // (iters_per_graph iterations and k_wf_continue) on the device until no slot
-        // holds work, so the host never waits between iterations.
-        e = cudaGraphCreate(&graph, 0);
-        cudaGraphConditionalHandle handle{};
-        if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&handle, graph, 1u, cudaGraphCondAssignDefault);
-        cudaGraphNodeParams cp{};
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = handle;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        cudaGraphNode_t cnode = nullptr;
-        if (e == cudaSuccess) e = cudaGraphAddNode(&cnode, graph, nullptr, 0, &cp);
-        cudaGraph_t body = e == cudaSuccess ? cp.conditional.phGraph_out[0] : nullptr;
-        if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-        if (e == cudaSuccess) {
-            capture_iterations();
-            k_wf_continue<<<1, 1, 0, s>>>(st, handle, (unsigned)std::min<int64_t>(max_launches, 0x7fffffff));
-            e = cudaStreamEndCapture(s, &body);
+    // The instantiated graph is kept in the workspace and launched again while the
+    // launch state (buffers, sizes, tuning, iteration bound) is the same; a batch of the
+    // same shape class re-uploads only its views.
+    const bool reuse = c->exec && std::memcmp(&c->g_st, &st, sizeof(st)) == 0 && c->g_pool == tune.pool &&
+                       c->g_trace_block == tune.trace_block && c->g_shade_block == tune.shade_block &&
+                       c->g_iters == tune.iters_per_graph && c->g_profile == tune.profile &&
+                       c->g_max_launches == max_launches;
+    if (!reuse) {
+        wf_cache_drop_graph(*c);
+        cudaGraph_t graph = nullptr;
+        if (!tune.profile) {
+            // The whole render is one launch: a conditional WHILE node repeats the body
+            // (iters_per_graph iterations and k_wf_continue) on the device until no slot
+            // holds work, so the host never waits between iterations.
+            e = cudaGraphCreate(&graph, 0);
+            cudaGraphConditionalHandle handle{};
+            if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&handle, graph, 1u, cudaGraphCondAssignDefault);
+            cudaGraphNodeParams cp{};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = handle;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t cnode = nullptr;
+            if (e == cudaSuccess) e = cudaGraphAddNode(&cnode, graph, nullptr, 0, &cp);
+            cudaGraph_t body = e == cudaSuccess ? cp.conditional.phGraph_out[0] : nullptr;
+            if (e == cudaSuccess)
+                e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                capture_iterations();
+                k_wf_continue<<<1, 1, 0, s>>>(st, handle, (unsigned)std::min<int64_t>(max_launches, 0x7fffffff));
+                e = cudaStreamEndCapture(s, &body);
+            }
+        } else {
+            e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                capture_iterations();
+                e = cudaStreamEndCapture(s, &graph);
+            }
         }
-    } else {
-        e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
-        if (e == cudaSuccess) {
-            capture_iterations();
-            e = cudaStreamEndCapture(s, &graph);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&c->exec, graph, 0);
+        c->graph = graph;
+        if (e != cudaSuccess) {
+            wf_cache_drop_graph(*c);
+            cudaStreamSynchronize(s);
+            return cuda_error(ctx, e, "wavefront graph");
         }
+        std::memcpy(&c->g_st, &st, sizeof(st));
+        c->g_pool = tune.pool;
+        c->g_trace_block = tune.trace_block;
+        c->g_shade_block = tune.shade_block;
+        c->g_iters = tune.iters_per_graph;
+        c->g_profile = tune.profile;
+        c->g_max_launches = max_launches;
     }
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-    if (e != cudaSuccess) {
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        for (auto& ev : pev) cudaEventDestroy(ev);
-        if (graph) cudaGraphDestroy(graph);
-        free_all();
-        return cuda_error(ctx, e, "wavefront graph");
-    }
-    unsigned* h_qc = nullptr;
-    cudaMallocHost(&h_qc, sizeof(unsigned) * kQcCount);
+    unsigned* h_qc = c->h_qc;
     int64_t graph_launches = 0;
     if (!tune.profile) {
-        uint32_t hs = 0;
-        unsigned long long span[4] = {0, 0, 0, 0};
-        e = cudaGraphLaunch(exec, s);
+        uint32_t* hs = c->h_status;
+        unsigned long long* span = c->h_span;
+        e = cudaGraphLaunch(c->exec, s);
         if (e == cudaSuccess) e = cudaMemcpyAsync(h_qc, st.qc, sizeof(unsigned) * kQcCount, cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(&hs, st.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(span, st.tspan, sizeof(span), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hs, st.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(span, st.tspan, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e == cudaSuccess) {
             graph_launches = h_qc[kQcBodies];
             // the resolve launch after each trace launch adds that launch's span
             trace_ms = 1e-6 * (double)span[2];
-            if (hs & 4u) result = set_error(ctx, FM_ERR_TIMEOUT, "wavefront: iteration limit reached");
+            if (*hs & 4u) result = set_error(ctx, FM_ERR_TIMEOUT, "wavefront: iteration limit reached");
         }
     } else {
         int64_t guard = 0;
         for (;;) {
-            e = cudaGraphLaunch(exec, s);
+            e = cudaGraphLaunch(c->exec, s);
             if (e != cudaSuccess) break;
             ++graph_launches;
             e = cudaMemcpyAsync(h_qc, st.qc, sizeof(unsigned) * kQcCount, cudaMemcpyDeviceToHost, s);
             if (e != cudaSuccess) break;
             e = cudaStreamSynchronize(s);
             if (e != cudaSuccess) break;
-            for (int it = 0; it < (int)pev.size() / 3; ++it) {
+            for (int it = 0; it < tune.iters_per_graph; ++it) {
                 float a = 0.0f, b = 0.0f;
                 cudaEventElapsedTime(&a, pev[3 * it], pev[3 * it + 1]);
                 cudaEventElapsedTime(&b, pev[3 * it + 1], pev[3 * it + 2]);
@@ -1416,29 +1554,24 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
             const int npix = v.cfg.width * v.cfg.height;
             k_wf_reduce<<<std::min((npix + 255) / 256, sms * 16), 256, 0, s>>>(v);
         }
+        k_counters_add<<<1, 1, 0, s>>>(cnt, c->cnt);
         e = cudaGetLastError();
         if (e != cudaSuccess) result = cuda_error(ctx, e, "wavefront reduce");
     }
-    cudaEventRecord(e1, s);
+    cudaEventRecord(c->e1, s);
     cudaStreamSynchronize(s);
     float ms = 0.0f;
-    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventElapsedTime(&ms, c->e0, c->e1);
     if (times) {
-        times->launches = 1 + graph_launches * ((ADJ ? 9 : 6) * tune.iters_per_graph + (tune.profile ? 0 : 1)) +
+        times->launches = 2 + graph_launches * ((ADJ ? 9 : 6) * tune.iters_per_graph + (tune.profile ? 0 : 1)) +
                           (int64_t)views.size();
         times->total_ms = ms;
         times->trace_ms = trace_ms;
         // without event timing, everything but the trace kernel counts as shading
         times->shade_ms = tune.profile ? shade_ms : std::max(0.0, (double)ms - trace_ms);
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    for (auto& ev : pev) cudaEventDestroy(ev);
-    cudaFreeHost(h_qc);
-    cudaGraphExecDestroy(exec);
-    cudaGraphDestroy(graph);
-    free_all();
-    cudaStreamSynchronize(s);
+    // a failed render leaves the graph in an unknown state: build it again next time
+    if (result != FM_OK) wf_cache_drop_graph(*c);
     return result;
 }
 
@@ -1456,11 +1589,32 @@ fm_status wavefront_adjoint(fm_ctx* ctx, const std::vector<WfView>& views, const
     return run_wavefront<true>(ctx, views, tune, &adj, cnt, times);
 }
 
+void wf_cache_release(fm_ctx* ctx)
+{
+    for (WfCache*& c : ctx->wf_cache) {
+        if (!c) continue;
+        wf_cache_drop_graph(*c);
+        wf_cache_free_state(*c, ctx->stream);
+        if (c->partial) cudaFreeAsync(c->partial, ctx->stream);
+        if (c->d_views) cudaFreeAsync(c->d_views, ctx->stream);
+        if (c->cnt) cudaFreeAsync(c->cnt, ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
+        if (c->h_views) cudaFreeHost(c->h_views);
+        if (c->h_block) cudaFreeHost(c->h_block);
+        if (c->e0) cudaEventDestroy(c->e0);
+        if (c->e1) cudaEventDestroy(c->e1);
+        for (cudaEvent_t ev : c->pev) cudaEventDestroy(ev);
+        delete c;
+        c = nullptr;
+    }
+}
+
 fm_status launch_wavefront(fm_ctx* ctx, const fm_scene* scene, const DevCamera& cam, const RenderCfg& cfg, float* rgb,
                            float* alb, float* nrm, Counters* cnt)
 {
     WfView v{};
     v.scene = scene->d_dev;
+    v.num_lights = scene->dev.num_lights;
     v.cam = cam;
     v.cfg = cfg;
     v.rgb = rgb;
