@@ -14,6 +14,7 @@
 // varies between builds, which changes no query result.
 #include "fm_bvh_build.h"
 
+#include <algorithm>
 #include <vector>
 
 namespace fm {
@@ -65,24 +66,28 @@ FM_HD float half_area(const float* lo, const float* hi)
     return dx * dy + dy * dz + dz * dx;
 }
 
-__global__ void k_init_bins(Bins* bins, int ntasks)
+// The level loops run on the device (see bvh_build): kernels whose work depends on a
+// level's task or frontier count read that count from device memory and stride over
+// it with a fixed grid.
+__global__ void k_init_bins(Bins* bins, const int32_t* ntasks_p)
 {
-    const int t = blockIdx.x;
-    if (t >= ntasks) return;
-    uint32_t* w = reinterpret_cast<uint32_t*>(bins + t);
+    const int ntasks = *ntasks_p;
     const int nw = sizeof(Bins) / 4;
     const int ncnt = 3 * kBins;
     const int nlo = ncnt + 3 * kBins * 3;
     const int nhi = nlo + 3 * kBins * 3;
     const int nclo = nhi + 3 * kBins * 3;
-    for (int i = threadIdx.x; i < nw; i += blockDim.x) {
-        uint32_t v;
-        if (i < ncnt) v = 0u;
-        else if (i < nlo) v = 0xffffffffu;   // min slots start at +max
-        else if (i < nhi) v = 0u;            // max slots start at -max
-        else if (i < nclo) v = 0xffffffffu;
-        else v = 0u;
-        w[i] = v;
+    for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
+        uint32_t* w = reinterpret_cast<uint32_t*>(bins + t);
+        for (int i = threadIdx.x; i < nw; i += blockDim.x) {
+            uint32_t v;
+            if (i < ncnt) v = 0u;
+            else if (i < nlo) v = 0xffffffffu;   // min slots start at +max
+            else if (i < nhi) v = 0u;            // max slots start at -max
+            else if (i < nclo) v = 0xffffffffu;
+            else v = 0u;
+            w[i] = v;
+        }
     }
 }
 
@@ -235,13 +240,12 @@ __global__ void k_bin(const float4* __restrict__ plo, const float4* __restrict__
     }
 }
 
-// One thread per task: choose the SAH split from the bins, create the two child nodes
+// SAH split of task ti: choose the split from the bins, create the two child nodes
 // (exact boxes from the bins) and either a next-level task or a small cluster for each.
-__global__ void k_sah(const Task* __restrict__ tasks, int ntasks, const Bins* __restrict__ bins, Split* splits,
-                      BNode* nodes, Task* next_tasks, int32_t* small_list, int32_t* counters, int32_t* pending_bounds)
+FM_D void sah_split(const Task* __restrict__ tasks, int ti, const Bins* __restrict__ bins, Split* splits,
+                    BNode* nodes, Task* next_tasks, int32_t* small_list, int32_t* counters, int32_t* pending_bounds,
+                    int max_tasks)
 {
-    const int ti = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ti >= ntasks) return;
     const Task tk = tasks[ti];
     const Bins& B = bins[ti];
     float best = kRealMax;
@@ -341,6 +345,13 @@ __global__ void k_sah(const Task* __restrict__ tasks, int ntasks, const Bins* __
             sp.child_task[s] = -1;
         } else {
             const int q = atomicAdd(&counters[1], 1);
+            if (q >= max_tasks) {
+                // cannot happen (tasks hold > kSmall primitives each); recorded, and the
+                // primitives are left out so that the build reports a leaf-count error
+                atomicOr(&counters[5], 1);
+                sp.child_task[s] = -1;
+                continue;
+            }
             Task nt;
             nt.node = c0 + s;
             nt.begin = beg[s];
@@ -356,6 +367,16 @@ __global__ void k_sah(const Task* __restrict__ tasks, int ntasks, const Bins* __
     }
     if (!child_bounds_known) atomicAdd(pending_bounds, 1);
     splits[ti] = sp;
+}
+
+// One thread per task of the level.
+__global__ void k_sah(const Task* __restrict__ tasks, const int32_t* ntasks_p, const Bins* __restrict__ bins,
+                      Split* splits, BNode* nodes, Task* next_tasks, int32_t* small_list, int32_t* counters,
+                      int32_t* pending_bounds, int max_tasks)
+{
+    const int ntasks = *ntasks_p;
+    for (int ti = blockIdx.x * blockDim.x + threadIdx.x; ti < ntasks; ti += gridDim.x * blockDim.x)
+        sah_split(tasks, ti, bins, splits, nodes, next_tasks, small_list, counters, pending_bounds, max_tasks);
 }
 
 __global__ void k_flags(const float4* __restrict__ plo, const float4* __restrict__ phi, const int32_t* __restrict__ pidx,
@@ -474,75 +495,69 @@ __global__ void k_scatter(const int32_t* __restrict__ pidx, const int32_t* __res
 // Boxes of children created by a median split are accumulated here after the scatter.
 __global__ void k_pending_bounds(const float4* __restrict__ plo, const float4* __restrict__ phi,
                                  const int32_t* __restrict__ pidx, const Task* __restrict__ tasks, const Split* splits,
-                                 int ntasks, BNode* nodes, Task* next_tasks, const int32_t* small_list, int nsmall_before,
-                                 int nsmall_after)
+                                 const int32_t* ntasks_p, const int32_t* pending_p, BNode* nodes, Task* next_tasks)
 {
     // One block per task of the previous level whose split was a median split.
-    const int ti = blockIdx.x;
-    if (ti >= ntasks) return;
-    const Split sp = splits[ti];
-    if (sp.axis >= 0) return;
-    const Task tk = tasks[ti];
-    for (int s = 0; s < 2; ++s) {
-        const int beg = s == 0 ? tk.begin : tk.begin + sp.nl;
-        const int cnt = s == 0 ? sp.nl : tk.count - sp.nl;
-        const int node = nodes[tk.node].a + s;
-        uint32_t* nb = reinterpret_cast<uint32_t*>(&nodes[node]);
-        for (int i = beg + threadIdx.x; i < beg + cnt; i += blockDim.x) {
-            const int p = pidx[i];
-            const float4 l = plo[p], h = phi[p];
-            const float lv[3] = {l.x, l.y, l.z}, hv[3] = {h.x, h.y, h.z};
-            for (int k = 0; k < 3; ++k) {
-                // nodes hold floats; use a CAS loop through the ordered encoding
-                float* lo = &nodes[node].lo[k];
-                float* hi = &nodes[node].hi[k];
-                int* li = reinterpret_cast<int*>(lo);
-                int* hiI = reinterpret_cast<int*>(hi);
-                int old = *li;
-                while (lv[k] < __int_as_float(old)) {
-                    const int prev = atomicCAS(li, old, __float_as_int(lv[k]));
-                    if (prev == old) break;
-                    old = prev;
-                }
-                old = *hiI;
-                while (hv[k] > __int_as_float(old)) {
-                    const int prev = atomicCAS(hiI, old, __float_as_int(hv[k]));
-                    if (prev == old) break;
-                    old = prev;
-                }
-                if (sp.child_task[s] >= 0) {
-                    const float c = 0.5f * (lv[k] + hv[k]);
-                    Task& nt = next_tasks[sp.child_task[s]];
-                    int* cl = reinterpret_cast<int*>(&nt.cmin[k]);
-                    int* ch = reinterpret_cast<int*>(&nt.cmax[k]);
-                    old = *cl;
-                    while (c < __int_as_float(old)) {
-                        const int prev = atomicCAS(cl, old, __float_as_int(c));
+    if (*pending_p == 0) return;
+    const int ntasks = *ntasks_p;
+    for (int ti = blockIdx.x; ti < ntasks; ti += gridDim.x) {
+        const Split sp = splits[ti];
+        if (sp.axis >= 0) continue;
+        const Task tk = tasks[ti];
+        for (int s = 0; s < 2; ++s) {
+            const int beg = s == 0 ? tk.begin : tk.begin + sp.nl;
+            const int cnt = s == 0 ? sp.nl : tk.count - sp.nl;
+            const int node = nodes[tk.node].a + s;
+            for (int i = beg + threadIdx.x; i < beg + cnt; i += blockDim.x) {
+                const int p = pidx[i];
+                const float4 l = plo[p], h = phi[p];
+                const float lv[3] = {l.x, l.y, l.z}, hv[3] = {h.x, h.y, h.z};
+                for (int k = 0; k < 3; ++k) {
+                    // nodes hold floats; use a CAS loop through the ordered encoding
+                    float* lo = &nodes[node].lo[k];
+                    float* hi = &nodes[node].hi[k];
+                    int* li = reinterpret_cast<int*>(lo);
+                    int* hiI = reinterpret_cast<int*>(hi);
+                    int old = *li;
+                    while (lv[k] < __int_as_float(old)) {
+                        const int prev = atomicCAS(li, old, __float_as_int(lv[k]));
                         if (prev == old) break;
                         old = prev;
                     }
-                    old = *ch;
-                    while (c > __int_as_float(old)) {
-                        const int prev = atomicCAS(ch, old, __float_as_int(c));
+                    old = *hiI;
+                    while (hv[k] > __int_as_float(old)) {
+                        const int prev = atomicCAS(hiI, old, __float_as_int(hv[k]));
                         if (prev == old) break;
                         old = prev;
+                    }
+                    if (sp.child_task[s] >= 0) {
+                        const float c = 0.5f * (lv[k] + hv[k]);
+                        Task& nt = next_tasks[sp.child_task[s]];
+                        int* cl = reinterpret_cast<int*>(&nt.cmin[k]);
+                        int* ch = reinterpret_cast<int*>(&nt.cmax[k]);
+                        old = *cl;
+                        while (c < __int_as_float(old)) {
+                            const int prev = atomicCAS(cl, old, __float_as_int(c));
+                            if (prev == old) break;
+                            old = prev;
+                        }
+                        old = *ch;
+                        while (c > __int_as_float(old)) {
+                            const int prev = atomicCAS(ch, old, __float_as_int(c));
+                            if (prev == old) break;
+                            old = prev;
+                        }
                     }
                 }
             }
         }
-        (void)nb;
     }
-    (void)small_list;
-    (void)nsmall_before;
-    (void)nsmall_after;
 }
 
-// Sequential exact-SAH builder for one cluster of <= kSmall primitives per thread.
-__global__ void k_small(const float4* __restrict__ plo, const float4* __restrict__ phi, int32_t* pidx,
-                        const int32_t* __restrict__ small_list, int nsmall, BNode* nodes, int32_t* counters)
+// Sequential exact-SAH build of cluster ci (<= kSmall primitives) by one thread.
+FM_D void small_build(const float4* __restrict__ plo, const float4* __restrict__ phi, int32_t* pidx,
+                      const int32_t* __restrict__ small_list, int ci, BNode* nodes, int32_t* counters)
 {
-    const int ci = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ci >= nsmall) return;
     const int root = small_list[3 * ci], begin = small_list[3 * ci + 1], count = small_list[3 * ci + 2];
     int ids[kSmall];
     for (int k = 0; k < count; ++k) ids[k] = pidx[begin + k];
@@ -671,17 +686,24 @@ __global__ void k_small(const float4* __restrict__ plo, const float4* __restrict
     }
 }
 
+// Sequential exact-SAH builder for one cluster of <= kSmall primitives per thread.
+__global__ void k_small(const float4* __restrict__ plo, const float4* __restrict__ phi, int32_t* pidx,
+                        const int32_t* __restrict__ small_list, const int32_t* nsmall_p, BNode* nodes, int32_t* counters)
+{
+    const int nsmall = *nsmall_p;
+    for (int ci = blockIdx.x * blockDim.x + threadIdx.x; ci < nsmall; ci += gridDim.x * blockDim.x)
+        small_build(plo, phi, pidx, small_list, ci, nodes, counters);
+}
+
 // ---- collapse to 8-wide nodes --------------------------------------------------
 
 FM_D float node_area(const BNode& b) { return half_area(b.lo, b.hi); }
 
-__global__ void k_collapse(const BNode* __restrict__ bnodes, const int32_t* __restrict__ pidx,
-                           const int2* __restrict__ frontier, int nfront, int2* next_frontier, int32_t* counters,
-                           uint4* wnodes, int32_t* leaf_prim)
+// Collapses the binary subtree under frontier entry fi into one 8-wide node.
+FM_D void collapse_node(const BNode* __restrict__ bnodes, const int32_t* __restrict__ pidx,
+                        const int2* __restrict__ frontier, int fi, int2* next_frontier, int32_t* counters,
+                        uint4* wnodes, int32_t* leaf_prim)
 {
-    // counters: [0] wide node count, [1] leaf slot count, [2] next frontier count
-    const int fi = blockIdx.x * blockDim.x + threadIdx.x;
-    if (fi >= nfront) return;
     const int bn = frontier[fi].x, wslot = frontier[fi].y;
     const BNode root = bnodes[bn];
     int ch[8];
@@ -827,12 +849,26 @@ __global__ void k_collapse(const BNode* __restrict__ bnodes, const int32_t* __re
     np[4] = make_uint4(pack4(qh[1]), pack4(qh[1] + 4), pack4(qh[2]), pack4(qh[2] + 4));
 }
 
+__global__ void k_collapse(const BNode* __restrict__ bnodes, const int32_t* __restrict__ pidx,
+                           const int2* __restrict__ frontier, const int32_t* nfront_p, int2* next_frontier,
+                           int32_t* counters, uint4* wnodes, int32_t* leaf_prim)
+{
+    // counters: [0] wide node count, [1] leaf slot count, [2] next frontier count
+    const int nfront = *nfront_p;
+    for (int fi = blockIdx.x * blockDim.x + threadIdx.x; fi < nfront; fi += gridDim.x * blockDim.x)
+        collapse_node(bnodes, pidx, frontier, fi, next_frontier, counters, wnodes, leaf_prim);
+}
+
 __global__ void k_fill_leaf(const int32_t* __restrict__ leaf_prim, int nleaf, PrimSource src, float4* leaf)
 {
+    const int nprim = src.num_tris + 2 * src.num_rects + src.num_spheres;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nleaf; i += gridDim.x * blockDim.x) {
         const int p = leaf_prim[i];
         float4 a, b, c;
-        if (p < src.num_tris) {
+        if (p < 0 || p >= nprim) {
+            // a slot the collapse did not fill (the build then reports a leaf-count error)
+            a = b = c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        } else if (p < src.num_tris) {
             const float* v = src.tri_pos + 9 * (size_t)p;
             a = make_float4(v[0], v[1], v[2], __uint_as_float((uint32_t)p));
             b = make_float4(v[3], v[4], v[5], 0.0f);
@@ -894,6 +930,60 @@ __global__ void k_prim_bounds(PrimSource src, float4* plo, float4* phi)
     }
 }
 
+// Level-loop control.  Split phase counters: [0] binary nodes, [1] tasks of the next
+// level, [2] small clusters, [3] median splits awaiting child bounds, [4] tasks of the
+// current level, [5] error bits, [6] loop bodies run.
+__global__ void k_level_begin(int32_t* counters)
+{
+    counters[4] = counters[1];
+    counters[1] = 0;
+    counters[3] = 0;
+}
+
+__global__ void k_split_continue(int32_t* counters, cudaGraphConditionalHandle handle, int max_bodies)
+{
+    const int bodies = ++counters[6];
+    bool more = counters[1] > 0;
+    if (more && bodies >= max_bodies) {
+        counters[5] |= 2;
+        more = false;
+    }
+    cudaGraphSetConditional(handle, more ? 1u : 0u);
+}
+
+// Collapse phase counters: [0] wide nodes, [1] leaf slots, [2] next frontier, [3]
+// current frontier, [4] levels, [5] loop bodies run, [6] error bits.
+__global__ void k_collapse_init(int2* front, int32_t* ccnt)
+{
+    front[0] = make_int2(0, 0);
+    ccnt[0] = 1;
+    ccnt[1] = 0;
+    ccnt[2] = 1;
+    ccnt[3] = 0;
+    ccnt[4] = 0;
+    ccnt[5] = 0;
+    ccnt[6] = 0;
+}
+
+__global__ void k_collapse_begin(int32_t* ccnt)
+{
+    const int cur = ccnt[2];
+    ccnt[2] = 0;
+    ccnt[3] = cur;
+    if (cur > 0) ++ccnt[4];
+}
+
+__global__ void k_collapse_continue(int32_t* ccnt, cudaGraphConditionalHandle handle, int max_bodies)
+{
+    const int bodies = ++ccnt[5];
+    bool more = ccnt[2] > 0;
+    if (more && bodies >= max_bodies) {
+        ccnt[6] |= 1;
+        more = false;
+    }
+    cudaGraphSetConditional(handle, more ? 1u : 0u);
+}
+
 inline int grid_for(int64_t n, int block)
 {
     int64_t g = (n + block - 1) / block;
@@ -913,119 +1003,210 @@ inline int grid_for(int64_t n, int block)
         }                                                                        \
     } while (0)
 
+namespace {
+
+// Buffers of one build.
+struct BuildBufs {
+    int n, max_tasks, ntiles, sms;
+    PrimSource src;
+    float4 *plo, *phi;
+    int32_t *pidx, *pidx2, *pos_task, *pos_task2, *flags, *scan, *tile_sums, *small_list, *counters, *ccnt, *leaf_prim;
+    uint32_t* rb;
+    BNode* bnodes;
+    Task *tasks, *tasks2;
+    Split* splits;
+    Bins* bins;
+    int2 *front, *front2;
+    uint4* wnodes;
+    float4* leaf;
+};
+
+// One split level: bins, SAH splits, stable partition of the level's primitives (in ->
+// out), and the bounds of children made by median splits.
+void split_level(cudaStream_t s, const BuildBufs& b, const int32_t* pidx_in, const int32_t* pos_in,
+                 const Task* tasks_in, int32_t* pidx_out, int32_t* pos_out, Task* tasks_out)
+{
+    const int n = b.n;
+    const int task_blocks = std::min(b.max_tasks, b.sms * 16);
+    k_level_begin<<<1, 1, 0, s>>>(b.counters);
+    k_init_bins<<<task_blocks, 256, 0, s>>>(b.bins, b.counters + 4);
+    k_bin<<<(n + 1023) / 1024, 256, 0, s>>>(b.plo, b.phi, pidx_in, pos_in, tasks_in, b.bins, n);
+    k_sah<<<grid_for(b.max_tasks, 128), 128, 0, s>>>(tasks_in, b.counters + 4, b.bins, b.splits, b.bnodes, tasks_out,
+                                                    b.small_list, b.counters, b.counters + 3, b.max_tasks);
+    k_flags<<<grid_for(n, 256), 256, 0, s>>>(b.plo, b.phi, pidx_in, pos_in, tasks_in, b.splits, b.flags, n);
+    k_scan_tiles<<<b.ntiles, kScanBlock, 0, s>>>(b.flags, b.scan, b.tile_sums, n);
+    k_scan_sums<<<1, kScanBlock, 0, s>>>(b.tile_sums, b.ntiles, b.scan + n);
+    k_scan_add<<<b.ntiles, 256, 0, s>>>(b.scan, b.tile_sums, n);
+    k_scatter<<<grid_for(n, 256), 256, 0, s>>>(pidx_in, pos_in, tasks_in, b.splits, b.flags, b.scan, pidx_out, pos_out,
+                                               n);
+    k_pending_bounds<<<task_blocks, 256, 0, s>>>(b.plo, b.phi, pidx_out, tasks_in, b.splits, b.counters + 4,
+                                                 b.counters + 3, b.bnodes, tasks_out);
+}
+
+void collapse_level(cudaStream_t s, const BuildBufs& b, const int2* front_in, int2* front_out)
+{
+    k_collapse_begin<<<1, 1, 0, s>>>(b.ccnt);
+    k_collapse<<<grid_for((int64_t)b.n + 1, 128), 128, 0, s>>>(b.bnodes, b.pidx, front_in, b.ccnt + 3, front_out,
+                                                               b.ccnt, b.wnodes, b.leaf_prim);
+}
+
+// Adds a WHILE node after `dep` whose body is what `body_fn` launches on `s`.
+template <class F>
+cudaError_t add_while(cudaGraph_t graph, cudaGraphNode_t dep, cudaStream_t s, cudaGraphConditionalHandle& handle,
+                      cudaGraphNode_t& node, F&& body_fn)
+{
+    cudaError_t e = cudaGraphConditionalHandleCreate(&handle, graph, 1u, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return e;
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    e = cudaGraphAddNode(&node, graph, &dep, 1, &cp);
+    if (e != cudaSuccess) return e;
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    body_fn(handle);
+    return cudaStreamEndCapture(s, &body);
+}
+
+// Adds a child-graph node after `dep` (none when dep is null) holding what `fn` launches.
+template <class F>
+cudaError_t add_captured(cudaGraph_t graph, const cudaGraphNode_t* dep, cudaStream_t s, cudaGraphNode_t& node, F&& fn)
+{
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    fn();
+    e = cudaStreamEndCapture(s, &g);
+    if (e != cudaSuccess) return e;
+    e = cudaGraphAddChildGraphNode(&node, graph, dep, dep ? 1 : 0, g);
+    cudaGraphDestroy(g);
+    return e;
+}
+
+// The whole build as one graph: root set-up, a WHILE loop of split levels (two per
+// body, so that the ping-pong buffers are fixed: after every body the partition is back
+// in pidx — a level without tasks copies it through), the small clusters, a WHILE loop
+// of collapse levels, and the leaf records.  The host waits once, at the end.
+cudaError_t build_graph(cudaStream_t s, const BuildBufs& b, cudaGraph_t& graph)
+{
+    cudaError_t e = cudaGraphCreate(&graph, 0);
+    if (e != cudaSuccess) return e;
+    const int n = b.n;
+    cudaGraphNode_t n_pre = nullptr, n_split = nullptr, n_mid = nullptr, n_collapse = nullptr, n_post = nullptr;
+    cudaGraphConditionalHandle h_split{}, h_collapse{};
+    e = add_captured(graph, nullptr, s, n_pre, [&]() {
+        k_prim_bounds<<<grid_for(n, 256), 256, 0, s>>>(b.src, b.plo, b.phi);
+        k_root_bounds<<<grid_for(n, 256), 256, 0, s>>>(b.plo, b.phi, n, b.rb);
+        k_make_root<<<1, 1, 0, s>>>(b.rb, n, b.bnodes, b.tasks, b.pos_task, b.small_list, b.counters);
+        k_fill_pos_task<<<grid_for(n, 256), 256, 0, s>>>(b.pos_task, b.pidx, n, n <= kSmall ? -1 : 0);
+    });
+    if (e != cudaSuccess) return e;
+    e = add_while(graph, n_pre, s, h_split, n_split, [&](cudaGraphConditionalHandle h) {
+        split_level(s, b, b.pidx, b.pos_task, b.tasks, b.pidx2, b.pos_task2, b.tasks2);
+        split_level(s, b, b.pidx2, b.pos_task2, b.tasks2, b.pidx, b.pos_task, b.tasks);
+        k_split_continue<<<1, 1, 0, s>>>(b.counters, h, 1024);
+    });
+    if (e != cudaSuccess) return e;
+    e = add_captured(graph, &n_split, s, n_mid, [&]() {
+        k_small<<<grid_for(n, 64), 64, 0, s>>>(b.plo, b.phi, b.pidx, b.small_list, b.counters + 2, b.bnodes,
+                                               b.counters);
+        k_collapse_init<<<1, 1, 0, s>>>(b.front, b.ccnt);
+    });
+    if (e != cudaSuccess) return e;
+    e = add_while(graph, n_mid, s, h_collapse, n_collapse, [&](cudaGraphConditionalHandle h) {
+        collapse_level(s, b, b.front, b.front2);
+        collapse_level(s, b, b.front2, b.front);
+        k_collapse_continue<<<1, 1, 0, s>>>(b.ccnt, h, 64);
+    });
+    if (e != cudaSuccess) return e;
+    return add_captured(graph, &n_collapse, s, n_post, [&]() {
+        k_fill_leaf<<<grid_for(n, 256), 256, 0, s>>>(b.leaf_prim, n, b.src, b.leaf);
+    });
+}
+
+}  // namespace
+
 int bvh_build(cudaStream_t stream, const PrimSource& src, BvhResult& out, std::string& err)
 {
     const int n = src.num_tris + 2 * src.num_rects + src.num_spheres;
     out = BvhResult{};
     if (n == 0) return 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    float4 *plo = nullptr, *phi = nullptr;
-    int32_t *pidx = nullptr, *pidx2 = nullptr, *pos_task = nullptr, *pos_task2 = nullptr, *flags = nullptr,
-            *scan = nullptr, *tile_sums = nullptr, *small_list = nullptr, *counters = nullptr, *leaf_prim = nullptr;
-    uint32_t* rb = nullptr;
-    BNode* bnodes = nullptr;
-    Task *tasks = nullptr, *tasks2 = nullptr;
-    Split* splits = nullptr;
-    Bins* bins = nullptr;
-    int2 *front = nullptr, *front2 = nullptr;
-    const int max_tasks = n / (kSmall + 1) + 2;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    BuildBufs b{};
+    b.n = n;
+    b.src = src;
+    b.max_tasks = n / (kSmall + 1) + 2;
+    b.ntiles = (n + kScanTile - 1) / kScanTile;
+    {
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        b.sms = sms;
+    }
     const int max_nodes = 2 * n + 2;
-    const int ntiles = (n + kScanTile - 1) / kScanTile;
-    int h_counters[4];
-    int ntasks = 0, nsmall = 0, depth = 0, nwide = 0, nleaf = 0;
+    int32_t h_cnt[16];
+    int nwide = 0, nleaf = 0, depth = 0;
     FM_BUILD_CHECK(cudaEventCreate(&ev0));
     FM_BUILD_CHECK(cudaEventCreate(&ev1));
     FM_BUILD_CHECK(cudaEventRecord(ev0, stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&plo, sizeof(float4) * n, stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&phi, sizeof(float4) * n, stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&pidx, sizeof(int32_t) * n, stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&pidx2, sizeof(int32_t) * n, stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&pos_task, sizeof(int32_t) * n, stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&pos_task2, sizeof(int32_t) * n, stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&flags, sizeof(int32_t) * n, stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&scan, sizeof(int32_t) * (n + 1), stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&tile_sums, sizeof(int32_t) * (ntiles + 1), stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&small_list, sizeof(int32_t) * 3 * (n + 1), stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&counters, sizeof(int32_t) * 8, stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&rb, sizeof(uint32_t) * 12, stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&bnodes, sizeof(BNode) * max_nodes, stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&tasks, sizeof(Task) * max_tasks, stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&tasks2, sizeof(Task) * max_tasks, stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&splits, sizeof(Split) * max_tasks, stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&bins, sizeof(Bins) * max_tasks, stream));
-
-    k_prim_bounds<<<grid_for(n, 256), 256, 0, stream>>>(src, plo, phi);
+    FM_BUILD_CHECK(cudaMallocAsync(&b.plo, sizeof(float4) * n, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.phi, sizeof(float4) * n, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.pidx, sizeof(int32_t) * n, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.pidx2, sizeof(int32_t) * n, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.pos_task, sizeof(int32_t) * n, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.pos_task2, sizeof(int32_t) * n, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.flags, sizeof(int32_t) * n, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.scan, sizeof(int32_t) * (n + 1), stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.tile_sums, sizeof(int32_t) * (b.ntiles + 1), stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.small_list, sizeof(int32_t) * 3 * (n + 1), stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.counters, sizeof(int32_t) * 16, stream));
+    b.ccnt = b.counters + 8;
+    FM_BUILD_CHECK(cudaMallocAsync(&b.rb, sizeof(uint32_t) * 12, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.bnodes, sizeof(BNode) * max_nodes, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.tasks, sizeof(Task) * b.max_tasks, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.tasks2, sizeof(Task) * b.max_tasks, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.splits, sizeof(Split) * b.max_tasks, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.bins, sizeof(Bins) * b.max_tasks, stream));
+    // wide nodes <= binary internal nodes; leaf slots == n
+    FM_BUILD_CHECK(cudaMallocAsync(&out.nodes, sizeof(uint4) * 5 * (size_t)(n + 1), stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.leaf_prim, sizeof(int32_t) * n, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.front, sizeof(int2) * (n + 1), stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.front2, sizeof(int2) * (n + 1), stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&out.leaf, sizeof(float4) * 3 * (size_t)n, stream));
+    b.wnodes = out.nodes;
+    b.leaf = out.leaf;
     {
         const uint32_t init[12] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u,
                                    0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
-        FM_BUILD_CHECK(cudaMemcpyAsync(rb, init, sizeof(init), cudaMemcpyHostToDevice, stream));
+        FM_BUILD_CHECK(cudaMemcpyAsync(b.rb, init, sizeof(init), cudaMemcpyHostToDevice, stream));
     }
-    k_root_bounds<<<grid_for(n, 256), 256, 0, stream>>>(plo, phi, n, rb);
-    FM_BUILD_CHECK(cudaMemsetAsync(counters, 0, sizeof(int32_t) * 8, stream));
-    k_make_root<<<1, 1, 0, stream>>>(rb, n, bnodes, tasks, pos_task, small_list, counters);
-    k_fill_pos_task<<<grid_for(n, 256), 256, 0, stream>>>(pos_task, pidx, n, n <= kSmall ? -1 : 0);
-    FM_BUILD_CHECK(cudaMemcpyAsync(h_counters, counters, sizeof(int32_t) * 4, cudaMemcpyDeviceToHost, stream));
-    FM_BUILD_CHECK(cudaStreamSynchronize(stream));
-    ntasks = h_counters[1];
-    nsmall = h_counters[2];
-
-    while (ntasks > 0) {
-        k_init_bins<<<ntasks, 256, 0, stream>>>(bins, ntasks);
-        k_bin<<<(n + 1023) / 1024, 256, 0, stream>>>(plo, phi, pidx, pos_task, tasks, bins, n);
-        FM_BUILD_CHECK(cudaMemsetAsync(counters + 1, 0, sizeof(int32_t), stream));
-        FM_BUILD_CHECK(cudaMemsetAsync(counters + 3, 0, sizeof(int32_t), stream));
-        k_sah<<<(ntasks + 127) / 128, 128, 0, stream>>>(tasks, ntasks, bins, splits, bnodes, tasks2, small_list,
-                                                         counters, counters + 3);
-        k_flags<<<grid_for(n, 256), 256, 0, stream>>>(plo, phi, pidx, pos_task, tasks, splits, flags, n);
-        k_scan_tiles<<<ntiles, kScanBlock, 0, stream>>>(flags, scan, tile_sums, n);
-        k_scan_sums<<<1, kScanBlock, 0, stream>>>(tile_sums, ntiles, scan + n);
-        k_scan_add<<<ntiles, 256, 0, stream>>>(scan, tile_sums, n);
-        k_scatter<<<grid_for(n, 256), 256, 0, stream>>>(pidx, pos_task, tasks, splits, flags, scan, pidx2, pos_task2,
-                                                         n);
-        FM_BUILD_CHECK(cudaMemcpyAsync(h_counters, counters, sizeof(int32_t) * 4, cudaMemcpyDeviceToHost, stream));
-        FM_BUILD_CHECK(cudaStreamSynchronize(stream));
-        if (h_counters[3] > 0)
-            k_pending_bounds<<<ntasks, 256, 0, stream>>>(plo, phi, pidx2, tasks, splits, ntasks, bnodes, tasks2,
-                                                          small_list, 0, 0);
-        std::swap(pidx, pidx2);
-        std::swap(pos_task, pos_task2);
-        std::swap(tasks, tasks2);
-        ntasks = h_counters[1];
-        nsmall = h_counters[2];
-        if (ntasks > max_tasks) {
-            err = "bvh build: task list overflow";
-            goto fail;
-        }
+    FM_BUILD_CHECK(cudaMemsetAsync(b.counters, 0, sizeof(int32_t) * 16, stream));
+    FM_BUILD_CHECK(cudaMemsetAsync(b.leaf_prim, 0xff, sizeof(int32_t) * n, stream));
+    FM_BUILD_CHECK(build_graph(stream, b, graph));
+    FM_BUILD_CHECK(cudaGraphInstantiate(&exec, graph, 0));
+    FM_BUILD_CHECK(cudaGraphLaunch(exec, stream));
+    FM_BUILD_CHECK(cudaMemcpyAsync(h_cnt, b.counters, sizeof(h_cnt), cudaMemcpyDeviceToHost, stream));
+    FM_BUILD_CHECK(cudaEventRecord(ev1, stream));
+    FM_BUILD_CHECK(cudaEventSynchronize(ev1));
+    if (h_cnt[5] & 1) {
+        err = "bvh build: task list overflow";
+        goto fail;
     }
-    if (nsmall > 0) k_small<<<(nsmall + 63) / 64, 64, 0, stream>>>(plo, phi, pidx, small_list, nsmall, bnodes, counters);
-    FM_BUILD_CHECK(cudaGetLastError());
-
-    // Collapse.  Wide node count <= binary internal nodes; leaf slots == n.
-    FM_BUILD_CHECK(cudaMallocAsync(&out.nodes, sizeof(uint4) * 5 * (size_t)(n + 1), stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&leaf_prim, sizeof(int32_t) * n, stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&front, sizeof(int2) * (n + 1), stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&front2, sizeof(int2) * (n + 1), stream));
-    {
-        const int2 r0 = make_int2(0, 0);
-        FM_BUILD_CHECK(cudaMemcpyAsync(front, &r0, sizeof(int2), cudaMemcpyHostToDevice, stream));
-        const int32_t c0[4] = {1, 0, 0, 0};
-        FM_BUILD_CHECK(cudaMemcpyAsync(counters, c0, sizeof(c0), cudaMemcpyHostToDevice, stream));
+    if (h_cnt[5] & 2) {
+        err = "bvh build: too many split levels";
+        goto fail;
     }
-    {
-        int nfront = 1;
-        while (nfront > 0) {
-            ++depth;
-            FM_BUILD_CHECK(cudaMemsetAsync(counters + 2, 0, sizeof(int32_t), stream));
-            k_collapse<<<(nfront + 127) / 128, 128, 0, stream>>>(bnodes, pidx, front, nfront, front2, counters,
-                                                                  out.nodes, leaf_prim);
-            FM_BUILD_CHECK(cudaMemcpyAsync(h_counters, counters, sizeof(int32_t) * 4, cudaMemcpyDeviceToHost, stream));
-            FM_BUILD_CHECK(cudaStreamSynchronize(stream));
-            nfront = h_counters[2];
-            std::swap(front, front2);
-        }
-        nwide = h_counters[0];
-        nleaf = h_counters[1];
+    if (h_cnt[8 + 6] & 1) {
+        err = "bvh build: too many collapse levels";
+        goto fail;
     }
+    nwide = h_cnt[8 + 0];
+    nleaf = h_cnt[8 + 1];
+    depth = h_cnt[8 + 4];
     if (nleaf != n) {
         err = "bvh build: leaf count mismatch";
         goto fail;
@@ -1034,11 +1215,6 @@ int bvh_build(cudaStream_t stream, const PrimSource& src, BvhResult& out, std::s
         err = "bvh build: tree deeper than the traversal stack";
         goto fail;
     }
-    FM_BUILD_CHECK(cudaMallocAsync(&out.leaf, sizeof(float4) * 3 * (size_t)n, stream));
-    k_fill_leaf<<<grid_for(n, 256), 256, 0, stream>>>(leaf_prim, n, src, out.leaf);
-    FM_BUILD_CHECK(cudaGetLastError());
-    FM_BUILD_CHECK(cudaEventRecord(ev1, stream));
-    FM_BUILD_CHECK(cudaEventSynchronize(ev1));
     {
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, ev0, ev1);
@@ -1047,53 +1223,59 @@ int bvh_build(cudaStream_t stream, const PrimSource& src, BvhResult& out, std::s
     out.num_nodes = nwide;
     out.num_leaf = nleaf;
     out.depth = depth;
-    cudaFreeAsync(plo, stream);
-    cudaFreeAsync(phi, stream);
-    cudaFreeAsync(pidx, stream);
-    cudaFreeAsync(pidx2, stream);
-    cudaFreeAsync(pos_task, stream);
-    cudaFreeAsync(pos_task2, stream);
-    cudaFreeAsync(flags, stream);
-    cudaFreeAsync(scan, stream);
-    cudaFreeAsync(tile_sums, stream);
-    cudaFreeAsync(small_list, stream);
-    cudaFreeAsync(counters, stream);
-    cudaFreeAsync(rb, stream);
-    cudaFreeAsync(bnodes, stream);
-    cudaFreeAsync(tasks, stream);
-    cudaFreeAsync(tasks2, stream);
-    cudaFreeAsync(splits, stream);
-    cudaFreeAsync(bins, stream);
-    cudaFreeAsync(front, stream);
-    cudaFreeAsync(front2, stream);
-    cudaFreeAsync(leaf_prim, stream);
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    cudaFreeAsync(b.plo, stream);
+    cudaFreeAsync(b.phi, stream);
+    cudaFreeAsync(b.pidx, stream);
+    cudaFreeAsync(b.pidx2, stream);
+    cudaFreeAsync(b.pos_task, stream);
+    cudaFreeAsync(b.pos_task2, stream);
+    cudaFreeAsync(b.flags, stream);
+    cudaFreeAsync(b.scan, stream);
+    cudaFreeAsync(b.tile_sums, stream);
+    cudaFreeAsync(b.small_list, stream);
+    cudaFreeAsync(b.counters, stream);
+    cudaFreeAsync(b.rb, stream);
+    cudaFreeAsync(b.bnodes, stream);
+    cudaFreeAsync(b.tasks, stream);
+    cudaFreeAsync(b.tasks2, stream);
+    cudaFreeAsync(b.splits, stream);
+    cudaFreeAsync(b.bins, stream);
+    cudaFreeAsync(b.front, stream);
+    cudaFreeAsync(b.front2, stream);
+    cudaFreeAsync(b.leaf_prim, stream);
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
     return 0;
 fail:
+    cudaGetLastError();
     cudaStreamSynchronize(stream);
-    cudaFreeAsync(plo, stream);
-    cudaFreeAsync(phi, stream);
-    cudaFreeAsync(pidx, stream);
-    cudaFreeAsync(pidx2, stream);
-    cudaFreeAsync(pos_task, stream);
-    cudaFreeAsync(pos_task2, stream);
-    cudaFreeAsync(flags, stream);
-    cudaFreeAsync(scan, stream);
-    cudaFreeAsync(tile_sums, stream);
-    cudaFreeAsync(small_list, stream);
-    cudaFreeAsync(counters, stream);
-    cudaFreeAsync(rb, stream);
-    cudaFreeAsync(bnodes, stream);
-    cudaFreeAsync(tasks, stream);
-    cudaFreeAsync(tasks2, stream);
-    cudaFreeAsync(splits, stream);
-    cudaFreeAsync(bins, stream);
-    cudaFreeAsync(front, stream);
-    cudaFreeAsync(front2, stream);
-    cudaFreeAsync(leaf_prim, stream);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaFreeAsync(b.plo, stream);
+    cudaFreeAsync(b.phi, stream);
+    cudaFreeAsync(b.pidx, stream);
+    cudaFreeAsync(b.pidx2, stream);
+    cudaFreeAsync(b.pos_task, stream);
+    cudaFreeAsync(b.pos_task2, stream);
+    cudaFreeAsync(b.flags, stream);
+    cudaFreeAsync(b.scan, stream);
+    cudaFreeAsync(b.tile_sums, stream);
+    cudaFreeAsync(b.small_list, stream);
+    cudaFreeAsync(b.counters, stream);
+    cudaFreeAsync(b.rb, stream);
+    cudaFreeAsync(b.bnodes, stream);
+    cudaFreeAsync(b.tasks, stream);
+    cudaFreeAsync(b.tasks2, stream);
+    cudaFreeAsync(b.splits, stream);
+    cudaFreeAsync(b.bins, stream);
+    cudaFreeAsync(b.front, stream);
+    cudaFreeAsync(b.front2, stream);
+    cudaFreeAsync(b.leaf_prim, stream);
     cudaFreeAsync(out.nodes, stream);
     cudaFreeAsync(out.leaf, stream);
+    cudaStreamSynchronize(stream);
     out = BvhResult{};
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
