@@ -341,6 +341,9 @@ def main():
     ap.add_argument("--scenes", type=int, default=NSCENES, help="batch size (profiling runs use fewer)")
     ap.add_argument("--adjoint-steps", type=int, default=2, help="timed adjoint/forward pairs (0 skips)")
     ap.add_argument("--no-autotune", action="store_true", help="default tuning instead of the autotuner's")
+    ap.add_argument("--tuning", default=None, metavar="POOL,TRACE_BLOCK,SHADE_BLOCK,ITERS",
+                    help="fixed wavefront tuning instead of the autotuner's (profiling runs pass the "
+                         "autotuned values, so that ncu sees the timed step without the trial renders)")
     ap.add_argument("--event-timing", action="store_true",
                     help="time renders with CUDA event nodes and a host loop over ordinary graphs "
                          "(FM_FLAG_PROFILE) instead of the one-launch conditional graph; ncu lists and "
@@ -403,7 +406,12 @@ def main():
     outs = [torch.empty((p.height, p.width, 3), device="cuda", dtype=torch.float32) for p in params_wf]
     out_ptrs = [o.data_ptr() for o in outs]
 
-    tuning = fb.Tuning(1 << 21, 128, 128, 8) if args.no_autotune else ctx.autotune_batch(scenes, cams, params_wf)
+    if args.tuning:
+        tuning = fb.Tuning(*(int(x) for x in args.tuning.split(",")))
+    elif args.no_autotune:
+        tuning = fb.Tuning(1 << 21, 128, 128, 8)
+    else:
+        tuning = ctx.autotune_batch(scenes, cams, params_wf)
 
     def step_wf(profile=False):
         return ctx.render_batch(scenes, cams, params_wf, tuning=tuning, device_outputs=out_ptrs, profile=profile)[3]
