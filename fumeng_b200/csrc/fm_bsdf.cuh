@@ -277,11 +277,6 @@ FM_D void disney_setup(Disney& d, float wo_z)
     }
 }
 
-// Material classes for specialised shading kernels: kClsDisney holds only Disney,
-// kClsSimple holds Lambert / conductor / dielectric, kClsAny holds every type.  A kernel
-// instantiated for one class contains only that class's code.
-constexpr int kClsAny = -1, kClsDisney = 0, kClsSimple = 1;
-FM_HD int material_class(int type) { return type == 3 ? kClsDisney : kClsSimple; }
 
 template <int CLS = kClsAny>
 FM_D Bsdf make_bsdf(const DevScene& S, const HitInfo& h)

@@ -449,6 +449,15 @@ fm_status fm_scene_create(fm_ctx* ctx, const fm_scene_desc* d, fm_scene** out)
             lights.push_back(L);
         }
         sc->lights = lights;
+        {
+            // what the wavefront's hit resolution needs of a primitive, in one load
+            std::vector<int32_t> prim_info((size_t)nprim);
+            for (int64_t p = 0; p < nprim; ++p) {
+                const int32_t o = prim_obj[p];
+                prim_info[p] = ((obj_light[o] + 1) << 2) | (material_class(mats[d->obj_material[o]].type) + 1);
+            }
+            FM_TRY(upload(ctx, sc, prim_info.data(), prim_info.size(), &S.prim_info));
+        }
         FM_TRY(upload(ctx, sc, obj_light.data(), obj_light.size(), &S.obj_light));
         FM_TRY(upload(ctx, sc, d->obj_material, (size_t)d->num_objects, &S.obj_material));
         FM_TRY(upload(ctx, sc, lights.data(), lights.size(), &S.lights));

@@ -141,6 +141,66 @@ __global__ void k_env_alias_marg(const double* rowsum, int h, float* prob, int32
     vose(nullptr, rowsum, h, prob, alias, scratch, scratch + h);
 }
 
+// The same tables with one row per block (one warp): the row's weights, outputs and
+// stacks live in shared memory while lane 0 runs Vose's method (its sequential loop is
+// bound by memory latency), and the warp moves the row in and out.  Dynamic shared
+// memory: 5 w 4-byte words.
+__global__ void k_env_alias_rows_smem(const float* lum, int w, float* prob, int32_t* alias)
+{
+    extern __shared__ float4 smem_f4[];
+    float* wt = reinterpret_cast<float*>(smem_f4);
+    float* p = wt + w;
+    int32_t* a = reinterpret_cast<int32_t*>(p + w);
+    int32_t* stk = a + w;
+    const size_t row = (size_t)blockIdx.x * w;
+    for (int i = threadIdx.x; i < w; i += blockDim.x) wt[i] = lum[row + i];
+    __syncwarp();
+    if (threadIdx.x == 0) vose(wt, nullptr, w, p, a, stk, stk + w);
+    __syncwarp();
+    for (int i = threadIdx.x; i < w; i += blockDim.x) {
+        prob[row + i] = p[i];
+        alias[row + i] = a[i];
+    }
+}
+
+// Marginal table in shared memory (24 h bytes: weights, probabilities, aliases, stacks).
+__global__ void k_env_alias_marg_smem(const double* rowsum, int h, float* prob, int32_t* alias)
+{
+    extern __shared__ float4 smem_f4[];
+    double* wt = reinterpret_cast<double*>(smem_f4);
+    float* p = reinterpret_cast<float*>(wt + h);
+    int32_t* a = reinterpret_cast<int32_t*>(p + h);
+    int32_t* stk = a + h;
+    for (int i = threadIdx.x; i < h; i += blockDim.x) wt[i] = rowsum[i];
+    __syncwarp();
+    if (threadIdx.x == 0) vose(nullptr, wt, h, p, a, stk, stk + h);
+    __syncwarp();
+    for (int i = threadIdx.x; i < h; i += blockDim.x) {
+        prob[i] = p[i];
+        alias[i] = a[i];
+    }
+}
+
+// Dynamic shared memory a kernel may use: the default 48 KB, or up to the device's
+// opt-in limit once requested.
+template <class K>
+bool smem_fits(K kernel, size_t bytes)
+{
+    if (bytes <= 48 * 1024) return true;
+    int dev = 0, limit = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+        bytes > (size_t)limit) {
+        cudaGetLastError();
+        return false;
+    }
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return true;
+}
+
 // grad[k][l][c] -= total_score * d log(sum lum)/d texel + row_score[k] * d log(rowsum_k)/d texel,
 // with d lum[k][l] / d texel[k][l][c] = L_c * sin_k (lum as in k_env_lum).
 __global__ void k_env_grad_spread(const float* lum, const double* rowsum, const double* totals, const double* row_score,
@@ -225,8 +285,15 @@ fm_status env_build_tables(fm_ctx* ctx, fm_scene* scene, const DevTexture& tex, 
     k_env_totals<<<1, 256, 0, st>>>(rowsum, w, h, totals);
     k_env_pdfs<<<(int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096), 256, 0, st>>>(lum, rowsum, totals, w, h,
                                                                                        pdf_sample, pdf_eval);
-    k_env_alias_rows<<<(h + 63) / 64, 64, 0, st>>>(lum, w, h, row_prob, row_alias, scratch);
-    k_env_alias_marg<<<1, 1, 0, st>>>(rowsum, h, marg_prob, marg_alias, scratch);
+    const size_t row_smem = 5 * sizeof(float) * (size_t)w, marg_smem = 24 * (size_t)h;
+    if (smem_fits(k_env_alias_rows_smem, row_smem))
+        k_env_alias_rows_smem<<<h, 32, row_smem, st>>>(lum, w, row_prob, row_alias);
+    else
+        k_env_alias_rows<<<(h + 63) / 64, 64, 0, st>>>(lum, w, h, row_prob, row_alias, scratch);
+    if (smem_fits(k_env_alias_marg_smem, marg_smem))
+        k_env_alias_marg_smem<<<1, 32, marg_smem, st>>>(rowsum, h, marg_prob, marg_alias);
+    else
+        k_env_alias_marg<<<1, 1, 0, st>>>(rowsum, h, marg_prob, marg_alias, scratch);
     cudaFreeAsync(lum, st);
     cudaFreeAsync(scratch, st);
     cudaFreeAsync(rowsum, st);

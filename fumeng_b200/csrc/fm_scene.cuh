@@ -78,6 +78,12 @@ struct DevEnv {
     const int32_t* marg_alias;    // [h]
 };
 
+// Material classes for specialised shading kernels: kClsDisney holds only Disney,
+// kClsSimple holds Lambert / conductor / dielectric, kClsAny holds every type.  A kernel
+// instantiated for one class contains only that class's code.
+constexpr int kClsAny = -1, kClsDisney = 0, kClsSimple = 1;
+FM_HD int material_class(int type) { return type == 3 ? kClsDisney : kClsSimple; }
+
 struct DevScene {
     // BVH: 5 x uint4 (80 B) per wide node; 3 x float4 per leaf primitive slot
     const uint4* nodes;
@@ -86,6 +92,7 @@ struct DevScene {
     int32_t num_tris, num_rects, num_spheres, num_prims;
 
     const int32_t* prim_obj;      // [num_prims] object of each primitive
+    const int32_t* prim_info;     // [num_prims] (object's area light + 1) << 2 | (material class + 1)
     // shading data in original order
     const float* tri_pos;         // [T*9]
     const float* tri_normal;      // [T*9] or null

@@ -466,13 +466,13 @@ FM_D void finish_cont(const WfState& st, int64_t idx, const DevScene& S, const H
             if (ADJ && (cflags & kReplay)) scatter_env(st, S, d, pixel_delta(st, cslot, st.views[st.view[cslot]]));
         }
     } else {
-        const int obj = __ldg(S.prim_obj + h.prim);
-        const int li = depth == 1 ? __ldg(S.obj_light + obj) : -1;
+        const int info = __ldg(S.prim_info + h.prim);
+        const int li = depth == 1 ? (info >> 2) - 1 : -1;
         if (li >= 0) {
             const HitInfo lh = make_hit(S, o, d, h);
             if (dot(lh.ng, lh.wo) > 0) acc_add(&st.acc[cslot], ld3(S.lights[li].radiance));
         } else {
-            cls = material_class(S.materials[__ldg(S.obj_material + obj)].type);
+            cls = (info & 3) - 1;
         }
     }
     // replayed vertices of an adjoint render go to their own queues, so that primal
@@ -513,8 +513,7 @@ FM_D void finish_mis(const WfState& st, int64_t q, const DevScene& S, const Hit&
             env_hit = true;
         }
     } else {
-        const int obj = __ldg(S.prim_obj + h.prim);
-        const int li = __ldg(S.obj_light + obj);
+        const int li = (__ldg(S.prim_info + h.prim) >> 2) - 1;
         if (li >= 0) {
             const HitInfo lh = make_hit(S, o, d, h);
             const f3 l2s = normalize(o - lh.pos);
