@@ -454,14 +454,18 @@ template <bool ADJ>
 FM_D void finish_cont(const WfState& st, int64_t idx, const DevScene& S, const Hit& h)
 {
     const int cslot = st.cont_q[idx];
-    const float4 o4 = st.ro[cslot], d4 = st.rd[cslot];
-    const f3 o = f3{o4.x, o4.y, o4.z}, d = f3{d4.x, d4.y, d4.z};
     const int cflags = st.flags[cslot];
     const int depth = cflags >> 8;
     int cls = -1;
+    // the ray itself is needed only for a first-bounce miss or emitter hit
+    auto ray_dir = [&]() {
+        const float4 d4 = st.rd[cslot];
+        return f3{d4.x, d4.y, d4.z};
+    };
     if (h.prim < 0) {
         // the camera ray's beta is 1
         if (depth == 1 && S.env_light >= 0) {
+            const f3 d = ray_dir();
             acc_add(&st.acc[cslot], env_radiance(S, d));
             if (ADJ && (cflags & kReplay)) scatter_env(st, S, d, pixel_delta(st, cslot, st.views[st.view[cslot]]));
         }
@@ -469,7 +473,8 @@ FM_D void finish_cont(const WfState& st, int64_t idx, const DevScene& S, const H
         const int info = __ldg(S.prim_info + h.prim);
         const int li = depth == 1 ? (info >> 2) - 1 : -1;
         if (li >= 0) {
-            const HitInfo lh = make_hit(S, o, d, h);
+            const float4 o4 = st.ro[cslot];
+            const HitInfo lh = make_hit(S, f3{o4.x, o4.y, o4.z}, ray_dir(), h);
             if (dot(lh.ng, lh.wo) > 0) acc_add(&st.acc[cslot], ld3(S.lights[li].radiance));
         } else {
             cls = (info & 3) - 1;
@@ -741,7 +746,7 @@ struct ShadeJob {
 // sample open.  Each class runs its own kernel, so a warp holds one kind of BSDF and
 // the kernel's code holds only that kind's lobes.
 template <int CLS, bool ADJ>
-__global__ void __launch_bounds__(256) k_wf_shade(WfState st)
+FM_D void shade_vertices(const WfState& st)
 {
     // ADJ: the replayed vertices of an adjoint render; otherwise forward (or primal) ones
     const int64_t n = st.qc[CLS == kClsDisney ? (ADJ ? kQcDisneyR : kQcDisney) : (ADJ ? kQcSimpleR : kQcSimple)];
@@ -990,6 +995,22 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfState st)
     if ((threadIdx.x & 31) == 0 && n_bounces) atomicAdd(&st.cnt->bounces, n_bounces);
 }
 
+// The shading kernels.  Forward ones are capped at 80 registers (three 256-thread blocks
+// per SM): the extra occupancy outweighs the spills of the Disney kernel.  The replay
+// kernels of adjoint renders keep the compiler's allocation (their dual-number code
+// spills heavily under a cap).
+template <int CLS>
+__global__ void __launch_bounds__(256, 3) k_wf_shade(WfState st)
+{
+    shade_vertices<CLS, false>(st);
+}
+
+template <int CLS>
+__global__ void __launch_bounds__(256) k_wf_shade_replay(WfState st)
+{
+    shade_vertices<CLS, true>(st);
+}
+
 // Per slot, after the shading kernels: fold the contributions the trace kernel added
 // (shadow and MIS rays of the previous bounce, emission seen by the continuation ray)
 // into the sample's color; a sample with neither a continuation ray nor rays in flight
@@ -1008,6 +1029,10 @@ __global__ void __launch_bounds__(256) k_wf_logic(WfState st)
         bool need_new = item == kNeedItem;
         bool enqueue_cont = false;
         bool alive = false;
+        // the sample to start (one start_sample call for every case below, so that the
+        // lanes of a warp generate their camera rays together)
+        int s_vid = 0, s_k = 0, s_flags = 0;
+        int64_t s_local = 0;
         if (item >= 0) {
             const float4 a4 = st.acc[slot];
             const float4 c4 = st.col[slot];
@@ -1027,7 +1052,10 @@ __global__ void __launch_bounds__(256) k_wf_logic(WfState st)
                 kahan_add4(sum, cmp, col);
                 st.isum[slot] = sum;
                 st.icomp[slot] = cmp;
-                start_sample(st, slot, V, item - V.item_base, st.k[slot], kReplay);
+                s_vid = vid;
+                s_local = item - V.item_base;
+                s_k = st.k[slot];
+                s_flags = kReplay;
                 enqueue_cont = true;
             } else {
                 const int vid = st.view[slot];
@@ -1056,7 +1084,9 @@ __global__ void __launch_bounds__(256) k_wf_logic(WfState st)
                     st.isum[slot] = sum;
                     st.icomp[slot] = cmp;
                     st.k[slot] = kdone;
-                    start_sample(st, slot, V, local, kdone);
+                    s_vid = vid;
+                    s_local = local;
+                    s_k = kdone;
                     enqueue_cont = true;
                 }
             }
@@ -1084,11 +1114,14 @@ __global__ void __launch_bounds__(256) k_wf_logic(WfState st)
                     st.icomp[slot] = z;
                     st.asum[slot] = z;
                     st.nsum[slot] = z;
-                    start_sample(st, slot, V, it - V.item_base, 0);
+                    s_vid = vid;
+                    s_local = it - V.item_base;
+                    s_k = 0;
                     enqueue_cont = true;
                 }
             }
         }
+        if (enqueue_cont) start_sample(st, slot, st.views[s_vid], s_local, s_k, s_flags);
         const int64_t q = wagg_append(&st.qc[kQcCont], enqueue_cont);
         if (enqueue_cont) {
             if (q < st.cap_cont)
@@ -1440,11 +1473,11 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
             k_wf_trace<<<trace_grid, tune.trace_block, 0, s>>>(st);
             if (tune.profile) cudaEventRecordWithFlags(pev[3 * it + 1], s, cudaEventRecordExternal);
             k_wf_resolve<ADJ><<<resolve_grid, 256, 0, s>>>(st);
-            k_wf_shade<kClsDisney, false><<<shade_grid, tune.shade_block, 0, s>>>(st);
-            k_wf_shade<kClsSimple, false><<<shade_grid, tune.shade_block, 0, s>>>(st);
+            k_wf_shade<kClsDisney><<<shade_grid, tune.shade_block, 0, s>>>(st);
+            k_wf_shade<kClsSimple><<<shade_grid, tune.shade_block, 0, s>>>(st);
             if (ADJ) {
-                k_wf_shade<kClsDisney, true><<<shade_grid, tune.shade_block, 0, s>>>(st);
-                k_wf_shade<kClsSimple, true><<<shade_grid, tune.shade_block, 0, s>>>(st);
+                k_wf_shade_replay<kClsDisney><<<shade_grid, tune.shade_block, 0, s>>>(st);
+                k_wf_shade_replay<kClsSimple><<<shade_grid, tune.shade_block, 0, s>>>(st);
             }
             k_wf_logic<ADJ><<<logic_grid, 256, 0, s>>>(st);
             if (ADJ) k_wf_grad_scatter<<<sms * 8, 256, 0, s>>>(st);
