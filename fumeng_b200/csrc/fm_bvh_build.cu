@@ -21,7 +21,9 @@ namespace fm {
 
 namespace {
 
-constexpr int kBins = 16;
+// 8 bins: on the batched workload (64 scenes of displaced meshes) the trees traced
+// faster than with 4, 16 or 32 (trace kernel 248 ms per step against 255 ms at 16).
+constexpr int kBins = 8;
 constexpr int kSmall = 32;     // clusters of <= kSmall primitives are built by one thread
 constexpr int kLeafMax = 3;    // primitives per leaf (a wide-node leaf slot holds <= 3)
 constexpr int kScanBlock = 1024;
@@ -629,8 +631,11 @@ FM_D void small_build(const float4* __restrict__ plo, const float4* __restrict__
                 }
             }
         }
-        // SAH termination with unit costs (traversal step 1, primitive test 1).
-        const float split_cost = parent_area > 0.0f ? 1.0f + best / parent_area : kRealMax;
+        // SAH termination: a binary node costs half a primitive test.  The collapse into
+        // 8-wide nodes removes most binary levels, so splitting down to single-primitive
+        // leaves pays (trace kernel 270 -> 248 ms per step on the batched workload
+        // against unit costs; costs of 0.25 and 0 give the same trees).
+        const float split_cost = parent_area > 0.0f ? 0.5f + best / parent_area : kRealMax;
         const bool make_leaf = n <= 1 || (n <= kLeafMax && (float)n <= split_cost);
         if (make_leaf) {
             for (int k = 0; k < n; ++k) pidx[begin + lo0 + k] = ids[lo0 + k];
