@@ -48,7 +48,7 @@ NSCENES = 64
 # DRAM bytes the trace kernel moves per traced ray (read + write, cold L2 at each
 # launch), from ncu over every trace launch of the 8-scene case of this workload
 # (profiles/k_wf_trace_batched8.md); traffic grows with the rays a launch traces.
-TRACE_DRAM_BYTES_PER_RAY = 79.4
+TRACE_DRAM_BYTES_PER_RAY = 80.4
 
 
 def measured_peak_hbm():
