@@ -15,6 +15,7 @@ single-sample variance at 4096 spp (tests/golden/make_golden.py).  Checks:
   * albedo and normal AOVs (first-hit averages) agree to 2e-2 mean absolute difference.
 """
 import json
+import os
 from pathlib import Path
 
 import numpy as np
@@ -26,7 +27,15 @@ from golden.make_golden import BATCH_CASES, IMAGE_CASES, SINGLE_TILES, single_sc
 
 GOLDEN_DIR = Path(__file__).resolve().parent / "golden"
 BATCHES, BATCH_SPP = 16, 256
-RESULTS = Path(__file__).resolve().parents[1] / "gpurun_out"
+# Optional log of every comparison (one JSON line each): the file named by this variable.
+RESULTS_LOG = os.environ.get("FUMENG_B200_PARITY_LOG")
+
+
+def log_result(res: dict) -> None:
+    print(json.dumps(res))
+    if RESULTS_LOG:
+        with open(RESULTS_LOG, "a") as f:
+            f.write(json.dumps(res) + "\n")
 
 
 def render_batches(ctx, spec, mode, seed=1234, batches=BATCHES, spp=BATCH_SPP):
@@ -81,10 +90,7 @@ def test_converged_image_matches_reference(ctx, case, mode):
     res["albedo_mad"] = float(np.mean(np.abs(alb[::s, ::s] - g["albedo"])))
     res["normal_mad"] = float(np.mean(np.abs(nrm[::s, ::s] - g["normal"])))
     res.update(case=name, mode="megakernel" if mode == fb.FM_MODE_MEGAKERNEL else "wavefront")
-    print(json.dumps(res))
-    if RESULTS.is_dir():
-        with open(RESULTS / "image_parity.jsonl", "a") as f:
-            f.write(json.dumps(res) + "\n")
+    log_result(res)
     assert np.all(np.isfinite(rgb))
     assert_parity(res)
     assert res["albedo_mad"] < 2e-2 and res["normal_mad"] < 2e-2, res
@@ -143,10 +149,7 @@ def test_batched_scenes_match_reference(ctx, mode):
         assert np.all(np.isfinite(tiles))
         res = compare(tiles, g)
         res.update(case=f"batch_s{s}", mode="megakernel" if mode == fb.FM_MODE_MEGAKERNEL else "wavefront")
-        print(json.dumps(res))
-        if RESULTS.is_dir():
-            with open(RESULTS / "image_parity.jsonl", "a") as f:
-                f.write(json.dumps(res) + "\n")
+        log_result(res)
         assert_parity(res)
 
 
@@ -168,8 +171,5 @@ def test_single_mesh_scene_matches_reference(ctx, mode):
         assert np.all(np.isfinite(t))
         res = compare(t, g)
         res.update(case=f"single_t{k}", mode="megakernel" if mode == fb.FM_MODE_MEGAKERNEL else "wavefront")
-        print(json.dumps(res))
-        if RESULTS.is_dir():
-            with open(RESULTS / "image_parity.jsonl", "a") as f:
-                f.write(json.dumps(res) + "\n")
+        log_result(res)
         assert_parity(res)
