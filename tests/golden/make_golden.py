@@ -3,7 +3,7 @@
 Run on a machine that has the reference sources (the oracle libraries are built from
 them by oracle/Makefile):
 
-    python tests/golden/make_golden.py [hit] [images] [adjoint] [batch] [single]
+    python tests/golden/make_golden.py [hit] [images] [adjoint] [batch] [single] [large]
 
 Scenes and rays are regenerated from seeds by fumeng_b200.synth, so each fixture stores
 only the reference's answers plus a SHA-256 of the inputs, which the tests recompute to
@@ -149,6 +149,35 @@ def make_single():
         rs.close()
 
 
+# The large configuration's scene generator at a size the reference renders here in
+# minutes: 2x2 displaced meshes (1,728 triangles each) with the configuration's material
+# mix (glass-like Disney with specular transmission 1, diffuse Disney, general Disney),
+# the Lambert ground, four rectangle lights and a sky with a sharp sun, depth 16; a closer
+# camera; full 64x40 frame, double build, 4096 spp.
+LARGE_SMALL_SPP, LARGE_SMALL_SEED = 4096, 13
+
+
+def large_small_scene():
+    spec = synth.large_scene(grid=2, box_n=12, width=64, height=40, spp=16, depth=16, env_w=256, env_h=128)
+    spec.camera = {"type": "pin_hole", "pos": [4.5, -5.0, 3.5], "look_at": [0.0, 0.0, 0.8], "up": [0, 0, 1],
+                   "fov": 50.0, "aspect": 64 / 40}
+    return spec
+
+
+def make_large_small():
+    spec = large_small_scene()
+    with tempfile.TemporaryDirectory() as d:
+        rs = fmref.RefScene(spec.write(Path(d)), "double")
+        t0 = time.time()
+        r = rs.render(LARGE_SMALL_SPP, seed=LARGE_SMALL_SEED)
+        rs.close()
+    mean = r["sum"] / LARGE_SMALL_SPP
+    var = np.maximum(r["sumsq"] / LARGE_SMALL_SPP - mean * mean, 0.0) * LARGE_SMALL_SPP / (LARGE_SMALL_SPP - 1)
+    np.savez_compressed(GOLDEN / "large_small.npz", mean=mean.astype(np.float32), var=var.astype(np.float32),
+                        spp=LARGE_SMALL_SPP, stride=1)
+    print("large_small", "%.1fs" % (time.time() - t0), "mean", mean.mean(axis=(0, 1)))
+
+
 # Central differences of L = sum(w * image) from the reference's double build, for
 # constant material parameters of synth.gradient_scene (48x48), with common random
 # numbers across +-h: (material, JSON key, channel or None).
@@ -210,4 +239,6 @@ if __name__ == "__main__":
             make_batch(s)
     if "single" in what:
         make_single()
+    if "large" in what:
+        make_large_small()
     print("done in %.1fs" % (time.time() - t0))

@@ -23,7 +23,7 @@ import pytest
 
 import fumeng_b200 as fb
 from fumeng_b200 import synth
-from golden.make_golden import BATCH_CASES, IMAGE_CASES, SINGLE_TILES, single_scene
+from golden.make_golden import BATCH_CASES, IMAGE_CASES, SINGLE_TILES, large_small_scene, single_scene
 
 GOLDEN_DIR = Path(__file__).resolve().parent / "golden"
 BATCHES, BATCH_SPP = 16, 256
@@ -173,3 +173,24 @@ def test_single_mesh_scene_matches_reference(ctx, mode):
         res.update(case=f"single_t{k}", mode="megakernel" if mode == fb.FM_MODE_MEGAKERNEL else "wavefront")
         log_result(res)
         assert_parity(res)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", [fb.FM_MODE_MEGAKERNEL, fb.FM_MODE_WAVEFRONT], ids=["megakernel", "wavefront"])
+def test_large_config_generator_matches_reference(ctx, mode):
+    """The large configuration's scene generator at 2x2 meshes (glass-like Disney with
+    specular transmission 1, diffuse and general Disney, Lambert ground, four rectangle
+    lights, a sky with a sharp sun, depth 16), full 64x40 frame, 16 x 256 spp against the
+    reference's double build at 4096 spp (tests/golden/large_small.npz).  The only
+    fixture with specular transmission in Disney, whose lobe choice and reflect /
+    transmit choice share one random number in the reference."""
+    path = GOLDEN_DIR / "large_small.npz"
+    if not path.exists():
+        pytest.skip("no large-configuration fixture (tests/golden/make_golden.py large)")
+    g = np.load(path)
+    rgb, _, _ = render_batches(ctx, large_small_scene(), mode)
+    res = compare(rgb, g)
+    res.update(case="large_small", mode="megakernel" if mode == fb.FM_MODE_MEGAKERNEL else "wavefront")
+    log_result(res)
+    assert np.all(np.isfinite(rgb))
+    assert_parity(res)
