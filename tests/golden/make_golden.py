@@ -3,7 +3,7 @@
 Run on a machine that has the reference sources (the oracle libraries are built from
 them by oracle/Makefile):
 
-    python tests/golden/make_golden.py [hit] [images] [adjoint] [batch] [single] [large]
+    python tests/golden/make_golden.py [hit] [images] [adjoint] [batch] [single] [large] [digests]
 
 Scenes and rays are regenerated from seeds by fumeng_b200.synth, so each fixture stores
 only the reference's answers plus a SHA-256 of the inputs, which the tests recompute to
@@ -178,6 +178,45 @@ def make_large_small():
     print("large_small", "%.1fs" % (time.time() - t0), "mean", mean.mean(axis=(0, 1)))
 
 
+# SHA-256 of the scene inputs behind each image fixture (scene_digests.json), so that a
+# change of the scene generators that would invalidate a fixture is caught on the CPU.
+def scene_digest(spec) -> str:
+    import json as _json
+    from fumeng_b200.scene import Mesh, Rect, Sphere
+    h = hashlib.sha256()
+    h.update(_json.dumps([spec.camera, spec.renderer, spec.materials, spec.lights], sort_keys=True,
+                         default=float).encode())
+    for o in spec.objects:
+        if isinstance(o, Mesh):
+            h.update(np.ascontiguousarray(o.vertices, np.float32).tobytes())
+            h.update(np.ascontiguousarray(o.faces, np.int64).tobytes())
+            for extra in (o.uvs, o.normals, o.vattr):
+                if extra is not None:
+                    h.update(np.ascontiguousarray(extra, np.float32).tobytes())
+        elif isinstance(o, (Rect, Sphere)):
+            h.update(repr(o).encode())
+        h.update(str(getattr(o, "material", "")).encode())
+    for name in sorted(spec.textures):
+        h.update(name.encode())
+        h.update(np.ascontiguousarray(spec.textures[name], np.float32).tobytes())
+    return h.hexdigest()
+
+
+def image_fixture_scenes():
+    """(fixture name, scene builder) of every image fixture."""
+    out = [(name, builder) for name, builder, _, _, _ in IMAGE_CASES]
+    out += [(f"batch_s{s}", (lambda s=s: synth.batch_scene(s))) for s in BATCH_CASES]
+    out += [("single", single_scene), ("large_small", large_small_scene)]
+    return out
+
+
+def make_digests():
+    import json as _json
+    d = {name: scene_digest(builder()) for name, builder in image_fixture_scenes()}
+    (GOLDEN / "scene_digests.json").write_text(_json.dumps(d, indent=1, sort_keys=True) + "\n")
+    print("scene digests", len(d))
+
+
 # Central differences of L = sum(w * image) from the reference's double build, for
 # constant material parameters of synth.gradient_scene (48x48), with common random
 # numbers across +-h: (material, JSON key, channel or None).
@@ -241,4 +280,6 @@ if __name__ == "__main__":
         make_single()
     if "large" in what:
         make_large_small()
+    if "digests" in what:
+        make_digests()
     print("done in %.1fs" % (time.time() - t0))
