@@ -24,6 +24,10 @@
 // item's samples one after another with Kahan-compensated sums and writes the item's
 // partial sums once; a final kernel sums the chunks of each pixel in chunk order.  When
 // a path ends, its slot immediately starts the next sample (path regeneration).
+//
+// The buffers, pinned staging, events and the instantiated graph live in a per-context
+// workspace (WfCache) that later renders reuse; the graph is launched again as long as
+// the launch state (WfState, tuning, iteration bound) is byte-identical.
 #include <cmath>
 #include <cstring>
 #include <vector>
