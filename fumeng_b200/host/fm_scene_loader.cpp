@@ -1,6 +1,8 @@
 #include "fm_scene_loader.h"
 
+#include <algorithm>
 #include <array>
+#include <charconv>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -106,69 +108,132 @@ void normalize_f(float* v)
     v[2] *= inv;
 }
 
-struct ObjData {
-    std::vector<float> v, vt, vn;
-    struct Corner {
-        int v, vt, vn;
-    };
-    std::vector<std::array<Corner, 3>> faces;
-};
-
-int obj_index(const std::string& s, size_t count)
+// strtol(s, nullptr, 10) for the token characters [s, e): decimal digits with an
+// optional sign are converted here, anything else by strtol itself.
+long obj_long(const char* s, const char* e)
 {
-    if (s.empty()) return -1;
-    const long i = std::strtol(s.c_str(), nullptr, 10);
+    const char* q = s;
+    bool neg = false;
+    if (q < e && (*q == '-' || *q == '+')) neg = *q++ == '-';
+    long v = 0;
+    int nd = 0;
+    while (q < e && *q >= '0' && *q <= '9' && nd < 18) {
+        v = 10 * v + (*q++ - '0');
+        ++nd;
+    }
+    if (nd == 18 && q < e && *q >= '0' && *q <= '9') return std::strtol(s, nullptr, 10);
+    return neg ? -v : v;
+}
+
+int obj_index(const char* s, const char* e, size_t count)
+{
+    if (s == e) return -1;
+    const long i = obj_long(s, e);
     if (i > 0) return (int)(i - 1);
     if (i < 0) return (int)((long)count + i);
     return -1;
 }
 
+bool obj_space(char c) { return c == ' ' || c == '\t' || c == '\r' || c == '\v' || c == '\f'; }
+
+// Next whitespace-separated token of [p, e): returns its start and sets `end`; p is
+// advanced past it (start == e when the line has no more tokens).
+const char* obj_token(const char*& p, const char* e, const char*& end)
+{
+    while (p < e && obj_space(*p)) ++p;
+    const char* t = p;
+    while (p < e && !obj_space(*p)) ++p;
+    end = p;
+    return t;
+}
+
+// A token as a float: the value strtof gives for its characters (0 for a missing
+// token).  std::from_chars converts plain decimal tokens (correctly rounded, as strtof);
+// a token it does not take whole without error (a leading '+', hexadecimal, out of
+// range, trailing characters) goes to strtof.  Lines are NUL-terminated in the buffer,
+// so strtof cannot read past the line.
+float obj_float(const char*& p, const char* e)
+{
+    const char* end;
+    const char* t = obj_token(p, e, end);
+    if (t == end) return 0.0f;
+    float v = 0.0f;
+    const auto r = std::from_chars(t, end, v, std::chars_format::general);
+    if (r.ec == std::errc() && r.ptr == end) return v;
+    return std::strtof(t, nullptr);
+}
+
+}  // namespace
+
 // Wavefront OBJ (v / vt / vn / f); polygons are split into fans (0, k, k+1) in file order,
-// one object per triangle (triangle.cpp:312-329).
+// one object per triangle (triangle.cpp:312-329).  The file is read whole and scanned in
+// place (no per-line or per-token strings); numbers are converted with strtof / strtol
+// on each whitespace-separated token, as a token-by-token reader would.
 ObjData load_obj(const std::string& path)
 {
-    std::ifstream f(path);
-    if (!f) throw std::runtime_error("Loading model failed: " + path);
+    std::FILE* fp = std::fopen(path.c_str(), "rb");
+    if (!fp) throw std::runtime_error("Loading model failed: " + path);
+    std::string buf;
+    if (std::fseek(fp, 0, SEEK_END) == 0) {
+        const long size = std::ftell(fp);
+        if (size > 0) {
+            buf.resize((size_t)size);
+            std::rewind(fp);
+            buf.resize(std::fread(&buf[0], 1, (size_t)size, fp));
+        }
+    }
+    std::fclose(fp);
     ObjData o;
-    std::string line;
-    while (std::getline(f, line)) {
-        if (line.size() < 2) continue;
-        std::istringstream ss(line);
-        std::string tag;
-        ss >> tag;
-        if (tag == "v") {
-            std::string a, b, c;
-            ss >> a >> b >> c;
-            o.v.push_back(std::strtof(a.c_str(), nullptr));
-            o.v.push_back(std::strtof(b.c_str(), nullptr));
-            o.v.push_back(std::strtof(c.c_str(), nullptr));
-        } else if (tag == "vt") {
-            std::string a, b;
-            ss >> a >> b;
-            o.vt.push_back(std::strtof(a.c_str(), nullptr));
-            o.vt.push_back(b.empty() ? 0.0f : std::strtof(b.c_str(), nullptr));
-        } else if (tag == "vn") {
-            std::string a, b, c;
-            ss >> a >> b >> c;
-            o.vn.push_back(std::strtof(a.c_str(), nullptr));
-            o.vn.push_back(std::strtof(b.c_str(), nullptr));
-            o.vn.push_back(std::strtof(c.c_str(), nullptr));
-        } else if (tag == "f") {
-            std::vector<ObjData::Corner> poly;
-            std::string tok;
-            while (ss >> tok) {
+    // rough capacity from the file size (a vertex or face line is >= 20 bytes)
+    o.v.reserve(buf.size() / 40 * 3);
+    o.faces.reserve(buf.size() / 40);
+    std::vector<ObjData::Corner> poly;
+    char* p = buf.empty() ? nullptr : &buf[0];
+    char* const end_all = p + buf.size();
+    while (p && p < end_all) {
+        char* nl = static_cast<char*>(std::memchr(p, '\n', (size_t)(end_all - p)));
+        char* line_end = nl ? nl : end_all;
+        const size_t len = (size_t)(line_end - p);
+        if (nl) *nl = '\0';
+        const char* q = p;
+        p = nl ? nl + 1 : end_all;
+        if (len < 2) continue;
+        const char* e = q + len;
+        const char* tag_end;
+        const char* tag = obj_token(q, e, tag_end);
+        const size_t tl = (size_t)(tag_end - tag);
+        if (tl == 1 && tag[0] == 'v') {
+            const float x = obj_float(q, e), y = obj_float(q, e), z = obj_float(q, e);
+            o.v.push_back(x);
+            o.v.push_back(y);
+            o.v.push_back(z);
+        } else if (tl == 2 && tag[0] == 'v' && tag[1] == 't') {
+            const float u = obj_float(q, e), v = obj_float(q, e);
+            o.vt.push_back(u);
+            o.vt.push_back(v);
+        } else if (tl == 2 && tag[0] == 'v' && tag[1] == 'n') {
+            const float x = obj_float(q, e), y = obj_float(q, e), z = obj_float(q, e);
+            o.vn.push_back(x);
+            o.vn.push_back(y);
+            o.vn.push_back(z);
+        } else if (tl == 1 && tag[0] == 'f') {
+            poly.clear();
+            for (;;) {
+                const char* te;
+                const char* t = obj_token(q, e, te);
+                if (t == te) break;
                 ObjData::Corner c{-1, -1, -1};
-                const size_t s1 = tok.find('/');
-                if (s1 == std::string::npos) {
-                    c.v = obj_index(tok, o.v.size() / 3);
+                const char* s1 = static_cast<const char*>(std::memchr(t, '/', (size_t)(te - t)));
+                if (!s1) {
+                    c.v = obj_index(t, te, o.v.size() / 3);
                 } else {
-                    c.v = obj_index(tok.substr(0, s1), o.v.size() / 3);
-                    const size_t s2 = tok.find('/', s1 + 1);
-                    if (s2 == std::string::npos) {
-                        c.vt = obj_index(tok.substr(s1 + 1), o.vt.size() / 2);
+                    c.v = obj_index(t, s1, o.v.size() / 3);
+                    const char* s2 = static_cast<const char*>(std::memchr(s1 + 1, '/', (size_t)(te - s1 - 1)));
+                    if (!s2) {
+                        c.vt = obj_index(s1 + 1, te, o.vt.size() / 2);
                     } else {
-                        c.vt = obj_index(tok.substr(s1 + 1, s2 - s1 - 1), o.vt.size() / 2);
-                        c.vn = obj_index(tok.substr(s2 + 1), o.vn.size() / 3);
+                        c.vt = obj_index(s1 + 1, s2, o.vt.size() / 2);
+                        c.vn = obj_index(s2 + 1, te, o.vn.size() / 3);
                     }
                 }
                 if (c.v < 0 || (size_t)c.v >= o.v.size() / 3) throw std::runtime_error("bad OBJ vertex index: " + path);
@@ -179,8 +244,6 @@ ObjData load_obj(const std::string& path)
     }
     return o;
 }
-
-}  // namespace
 
 fm_scene_desc FlatScene::desc() const
 {
@@ -440,6 +503,16 @@ void SceneLoader::ParseRenderObject(const Json& j)
         double N[9];
         normal_matrix(M, N);
         const ObjData obj = load_obj(m_root + path);
+        // room for this mesh, growing geometrically across the scene's meshes
+        auto grow = [](auto& vec, size_t add) {
+            if (vec.capacity() < vec.size() + add) vec.reserve(std::max(vec.size() + add, 2 * vec.capacity()));
+        };
+        const size_t nf = obj.faces.size();
+        grow(F.tri_object, nf);
+        grow(F.tri_pos, 9 * nf);
+        grow(F.tri_has_normal, nf);
+        grow(F.tri_normal, 9 * nf);
+        grow(F.tri_uv, 6 * nf);
         for (const auto& f : obj.faces) {
             const int32_t o = add_object();
             F.tri_object.push_back(o);

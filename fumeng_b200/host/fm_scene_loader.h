@@ -11,6 +11,7 @@
 // "specular_reflection" {color, eta_i, eta_t, k}, and "renderer": {"mode":
 // "wavefront"|"megakernel", "seed"}.
 #pragma once
+#include <array>
 #include <map>
 #include <memory>
 #include <string>
@@ -40,6 +41,21 @@ struct FlatScene {
 
     fm_scene_desc desc() const;
 };
+
+// The triangles of a Wavefront OBJ file: positions, texture coordinates and normals as
+// read, and each face's corners (0-based indices, -1 where absent).
+struct ObjData {
+    std::vector<float> v, vt, vn;
+    struct Corner {
+        int v, vt, vn;
+    };
+    std::vector<std::array<Corner, 3>> faces;
+};
+
+// Reads an OBJ file (v, vt, vn, f; other lines ignored; polygons split into fans in file
+// order).  Throws std::runtime_error on an unreadable file or a face whose vertex index
+// is out of range.
+ObjData load_obj(const std::string& path);
 
 struct PostStep {
     std::string type;   // tonemapping | linear_to_srgb | srgb_to_linear | oidn_denoise
