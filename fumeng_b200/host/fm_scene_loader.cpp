@@ -2,6 +2,7 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <charconv>
 #include <cmath>
 #include <cstdio>
@@ -11,6 +12,7 @@
 #include <fstream>
 #include <sstream>
 #include <stdexcept>
+#include <thread>
 
 #include "fm_image_io.h"
 
@@ -468,6 +470,55 @@ void SceneLoader::ParseMaterial(const Json& j)
     m_flat.materials.push_back(m);
 }
 
+void SceneLoader::PreloadMeshes(const Json& objs)
+{
+    // the paths as ParseRenderObject reads them; an object whose fields do not parse is
+    // left to ParseRenderObject, which reports it in order
+    std::vector<std::string> paths;
+    for (const auto& o : objs.arr) {
+        try {
+            const Json* sh = o.find("shape");
+            if (!sh) continue;
+            std::string type, path;
+            load(*sh, "type", type);
+            if (type != "triangle_mesh") continue;
+            load(*sh, "path", path);
+            if (m_meshes.emplace(m_root + path, PreloadedMesh{}).second) paths.push_back(m_root + path);
+        } catch (const std::exception&) {
+        }
+    }
+    if (paths.empty()) return;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nthreads = std::min<size_t>(std::min<size_t>(paths.size(), hw), 16);
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+        for (size_t i = next++; i < paths.size(); i = next++) {
+            PreloadedMesh& m = m_meshes.at(paths[i]);
+            try {
+                m.data = load_obj(paths[i]);
+            } catch (...) {
+                m.error = std::current_exception();
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < nthreads; ++t) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+}
+
+const ObjData& SceneLoader::mesh_data(const std::string& path)
+{
+    auto it = m_meshes.find(path);
+    if (it == m_meshes.end()) {
+        PreloadedMesh m;
+        m.data = load_obj(path);
+        it = m_meshes.emplace(path, std::move(m)).first;
+    }
+    if (it->second.error) std::rethrow_exception(it->second.error);
+    return it->second.data;
+}
+
 void SceneLoader::ParseRenderObject(const Json& j)
 {
     float em[3] = {0, 0, 0};
@@ -502,7 +553,7 @@ void SceneLoader::ParseRenderObject(const Json& j)
         const bool ident = is_identity(M);
         double N[9];
         normal_matrix(M, N);
-        const ObjData obj = load_obj(m_root + path);
+        const ObjData& obj = mesh_data(m_root + path);
         // room for this mesh, growing geometrically across the scene's meshes
         auto grow = [](auto& vec, size_t add) {
             if (vec.capacity() < vec.size() + add) vec.reserve(std::max(vec.size() + add, 2 * vec.capacity()));
@@ -625,8 +676,11 @@ void SceneLoader::ParseScene(const Json& root)
         m_material_index["default_material"] = (int32_t)m_flat.materials.size();
         m_flat.materials.push_back(m);
     }
-    if (const Json* objs = c->find("render_objects"))
+    if (const Json* objs = c->find("render_objects")) {
+        PreloadMeshes(*objs);
         for (const auto& o : objs->arr) ParseRenderObject(o);
+        m_meshes.clear();
+    }
     if (const Json* ls = c->find("lights"))
         for (const auto& l : ls->arr) ParseLight(l);
 }

@@ -12,6 +12,7 @@
 // "wavefront"|"megakernel", "seed"}.
 #pragma once
 #include <array>
+#include <exception>
 #include <map>
 #include <memory>
 #include <string>
@@ -85,6 +86,10 @@ private:
     void ParseRenderObject(const Json& j);
     void ParseLight(const Json& j);
     void ParsePostProcess(const Json& j);
+    // Reads every OBJ file the render objects name, on several host threads, before the
+    // objects are flattened in order (mesh_data hands the results out).
+    void PreloadMeshes(const Json& objs);
+    const ObjData& mesh_data(const std::string& path);
     fm_tex_ref ParseTexture(const Json& j, float dflt[3]);
     int32_t LoadTexture(const std::string& path, const std::string& sampler, const std::string& wrap_u,
                         const std::string& wrap_v);
@@ -97,6 +102,11 @@ private:
     std::map<std::string, int32_t> m_material_index;
     std::vector<PostStep> m_post;
     std::map<std::string, int32_t> m_texture_cache;
+    struct PreloadedMesh {
+        ObjData data;
+        std::exception_ptr error;   // rethrown when the object that names the file is reached
+    };
+    std::map<std::string, PreloadedMesh> m_meshes;
 };
 
 // Post-process chain on a float RGB image (post/tonemapping.cpp, post/*_srgb.cpp).
