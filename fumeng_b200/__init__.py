@@ -77,7 +77,7 @@ class Camera(C.Structure):
 class RenderParams(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32), ("depth", C.c_int32),
                 ("direct_loop", C.c_int32), ("rr_depth", C.c_int32), ("rr_coef", C.c_float), ("seed", C.c_uint64),
-                ("mode", C.c_int32), ("sample_offset", C.c_int32)]
+                ("mode", C.c_int32), ("sample_offset", C.c_int32), ("max_sample_value", C.c_float)]
 
 
 class RenderStats(C.Structure):
@@ -88,7 +88,7 @@ class RenderStats(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("pool", C.c_int64), ("trace_block", C.c_int32), ("shade_block", C.c_int32),
-                ("iters_per_graph", C.c_int32)]
+                ("iters_per_graph", C.c_int32), ("max_iterations", C.c_int32), ("queue_limit", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {"pool": self.pool, "trace_block": self.trace_block, "shade_block": self.shade_block,

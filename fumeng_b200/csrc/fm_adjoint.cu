@@ -109,6 +109,8 @@ extern "C" fm_status fm_render_adjoint(fm_ctx* ctx, const fm_scene* scene, int32
         if (st != FM_OK) return st;
         if (params[i].mode != FM_MODE_WAVEFRONT)
             return set_error(ctx, FM_ERR_INVALID, "render_adjoint: views must use FM_MODE_WAVEFRONT");
+        if (params[i].max_sample_value != 0.0f)
+            return set_error(ctx, FM_ERR_INVALID, "render_adjoint: max_sample_value must be 0 (no clamp)");
         if (!d_rgb[i]) return set_error(ctx, FM_ERR_INVALID, "render_adjoint: d_rgb entry is null");
     }
     FM_CUDA_TRY(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");

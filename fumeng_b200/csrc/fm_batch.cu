@@ -27,6 +27,8 @@ WfTuning to_wf(const fm_tuning& t)
     w.trace_block = t.trace_block;
     w.shade_block = t.shade_block;
     w.iters_per_graph = t.iters_per_graph;
+    w.max_iterations = t.max_iterations;
+    w.queue_limit = t.queue_limit;
     return w;
 }
 
@@ -34,7 +36,7 @@ fm_status check_tuning(fm_ctx* ctx, const fm_tuning& t)
 {
     auto okb = [](int b) { return b == 32 || b == 64 || b == 128 || b == 256; };
     if (t.pool < 1024 || t.pool > ((int64_t)1 << 26) || !okb(t.trace_block) || !okb(t.shade_block) ||
-        t.iters_per_graph < 1 || t.iters_per_graph > 64)
+        t.iters_per_graph < 1 || t.iters_per_graph > 64 || t.max_iterations < 0 || t.queue_limit < 0)
         return set_error(ctx, FM_ERR_INVALID, "tuning out of range");
     return FM_OK;
 }
@@ -96,7 +98,7 @@ fm_status autotune(fm_ctx* ctx, int32_t n, const fm_scene* const* scenes, const 
     const std::vector<WfView> views = make_views(n, scenes, cams, params, imgs.data(), nullptr, nullptr, 8);
     double samples = 0.0;
     for (const auto& v : views) samples += (double)v.cfg.width * v.cfg.height * v.cfg.spp;
-    fm_tuning best{(int64_t)1 << 21, 128, 128, 8};
+    fm_tuning best{(int64_t)1 << 21, 128, 128, 8, 0, 0};
     double best_rate = -1.0;
     fm_status st = FM_OK;
     // each candidate's faster of two renders, so that one slow render does not decide
@@ -185,7 +187,7 @@ extern "C" fm_status fm_render_batch(fm_ctx* ctx, int32_t n, const fm_scene* con
     FM_CUDA_TRY(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
     const bool dev = (flags & FM_FLAG_DEVICE_PTRS) != 0;
     const bool wave = params[0].mode == FM_MODE_WAVEFRONT;
-    fm_tuning tune{(int64_t)1 << 21, 128, 128, 8};
+    fm_tuning tune{(int64_t)1 << 21, 128, 128, 8, 0, 0};
     if (wave) {
         if (tuning) {
             st = check_tuning(ctx, *tuning);

@@ -268,7 +268,20 @@ struct RenderCfg {
     uint64_t seed;
     int sample_offset;
     int rr_enabled;   // depth > rr_depth (path_tracing.cpp:107)
+    float clamp;      // > 0: per-channel limit of a sample's radiance (extension), 0: off
 };
+
+// A camera sample's radiance as it enters the pixel sum: each channel limited to
+// cfg.clamp when the clamp is on (a NaN channel stays NaN, so it is still counted).
+FM_HD f3 clamp_sample(const RenderCfg& cfg, f3 c)
+{
+    if (cfg.clamp > 0.0f) {
+        c.x = c.x > cfg.clamp ? cfg.clamp : c.x;
+        c.y = c.y > cfg.clamp ? cfg.clamp : c.y;
+        c.z = c.z > cfg.clamp ? cfg.clamp : c.z;
+    }
+    return c;
+}
 
 struct Counters {
     unsigned long long paths, closest, shadow, bounces, nans;

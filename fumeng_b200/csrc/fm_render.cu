@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(128) k_megakernel(const __grid_constant__ DevS
             camera_ray(cam, px, py, lx, ly, o, d);
             const PathOut po = trace_path(S, cfg, o, d, rng, status);
             if (!isfinite(po.color.x) || !isfinite(po.color.y) || !isfinite(po.color.z)) ++nn;
-            kahan_add(sum, comp, po.color);
+            kahan_add(sum, comp, clamp_sample(cfg, po.color));
             asum += po.albedo;
             nsum += po.normal;
             nc += po.closest;
@@ -124,6 +124,7 @@ RenderCfg make_cfg(const fm_render_params& p)
     r.seed = p.seed;
     r.sample_offset = p.sample_offset;
     r.rr_enabled = p.depth > p.rr_depth ? 1 : 0;
+    r.clamp = p.max_sample_value;
     return r;
 }
 
@@ -138,6 +139,7 @@ fm_status validate_render(fm_ctx* ctx, const fm_scene* scene, const fm_camera* c
     if (p->mode != FM_MODE_MEGAKERNEL && p->mode != FM_MODE_WAVEFRONT)
         return set_error(ctx, FM_ERR_INVALID, "render: bad mode");
     if (p->sample_offset < 0) return set_error(ctx, FM_ERR_INVALID, "render: negative sample_offset");
+    if (!(p->max_sample_value >= 0.0f)) return set_error(ctx, FM_ERR_INVALID, "render: max_sample_value must be >= 0");
     return FM_OK;
 }
 

@@ -46,6 +46,8 @@ struct WfTuning {
     int shade_block = 128;
     int iters_per_graph = 8;
     bool profile = false;     // record CUDA events around each trace / shade launch
+    int max_iterations = 0;   // > 0: iteration cap below the automatic bound (then FM_ERR_TIMEOUT)
+    int queue_limit = 0;      // > 0: ray-queue capacity cap (then FM_ERR_QUEUE_OVERFLOW)
 };
 
 struct WfTimes {

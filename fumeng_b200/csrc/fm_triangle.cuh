@@ -115,23 +115,30 @@ FM_D bool intersect_triangle(const RayPre& r, f3 v0, f3 v1, f3 v2, float tmin, f
     return true;
 }
 
-// Sphere::IntersectSphere (geometry/sphere.cpp:91-129): the ray is taken to object
-// space (not renormalized, so t is shared), the quadratic is solved without the robust
-// form, and the nearer root inside the inclusive range [tmin, tmax] is returned.
+// Sphere::IntersectSphere (geometry/sphere.cpp:91-129, GetCoef :206-212): the ray is
+// taken to object space (not renormalized, so t is shared), the quadratic is solved
+// without the robust form, and the nearer root inside the inclusive range [tmin, tmax]
+// is returned.  Every operation is explicitly rounded in the reference's order
+// (SquareSum and glm::dot left to right, b*b - (4a)*c, 0.5/a), so no multiply-add is
+// contracted and the result equals the reference's float build bit for bit whenever the
+// object-space ray does (always for translation-only transforms, whose world-to-object
+// step is one rounded subtraction per origin component and exact for the direction).
 FM_D bool intersect_sphere(const Xf& world_to_object, float radius, f3 o, f3 d, float tmin, float tmax,
                            float& t_out)
 {
     const f3 ol = xf_point(world_to_object, o);
     const f3 dl = xf_vec(world_to_object, d);
-    const float a = dl.x * dl.x + dl.y * dl.y + dl.z * dl.z;
-    const float b = 2.0f * dot(dl, ol);
-    const float c = (ol.x * ol.x + ol.y * ol.y + ol.z * ol.z) - radius * radius;
-    float delta = b * b - 4.0f * a * c;
+    const float a = __fadd_rn(__fadd_rn(__fmul_rn(dl.x, dl.x), __fmul_rn(dl.y, dl.y)), __fmul_rn(dl.z, dl.z));
+    const float b =
+        __fmul_rn(2.0f, __fadd_rn(__fadd_rn(__fmul_rn(dl.x, ol.x), __fmul_rn(dl.y, ol.y)), __fmul_rn(dl.z, ol.z)));
+    const float c = __fsub_rn(__fadd_rn(__fadd_rn(__fmul_rn(ol.x, ol.x), __fmul_rn(ol.y, ol.y)), __fmul_rn(ol.z, ol.z)),
+                              __fmul_rn(radius, radius));
+    float delta = __fsub_rn(__fmul_rn(b, b), __fmul_rn(__fmul_rn(4.0f, a), c));
     if (delta < 0) return false;
-    delta = sqrtf(delta);
-    const float inv2a = 0.5f / a;
-    const float t0 = (-b - delta) * inv2a;
-    const float t1 = (-b + delta) * inv2a;
+    delta = __fsqrt_rn(delta);
+    const float inv2a = __fdiv_rn(0.5f, a);
+    const float t0 = __fmul_rn(__fsub_rn(-b, delta), inv2a);
+    const float t1 = __fmul_rn(__fadd_rn(-b, delta), inv2a);
     if (t0 >= tmin && t0 <= tmax) {
         t_out = t0;
         return true;

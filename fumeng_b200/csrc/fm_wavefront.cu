@@ -389,21 +389,27 @@ FM_D void add_vertex_grad(const WfState& st, int slot, const float* g)
 }
 
 // Last kernel of a conditional graph body (iters_per_graph iterations): run the body
-// again while any slot holds work and the iteration bound is not reached (status bit 4
+// again while any slot holds work, no queue overflowed (status bit 2: work was dropped,
+// so the render has failed) and the iteration bound is not reached (status bit 4
 // reports that the bound stopped the loop).
 __global__ void k_wf_continue(WfState st, cudaGraphConditionalHandle handle, unsigned max_bodies)
 {
     const unsigned active = st.qc[kQcActive];
     const unsigned bodies = ++st.qc[kQcBodies];
-    if (active != 0u && bodies >= max_bodies) atomicOr(st.status, 4u);
-    cudaGraphSetConditional(handle, (active != 0u && bodies < max_bodies) ? 1u : 0u);
+    const bool overflow = (*(volatile uint32_t*)st.status & 2u) != 0u;
+    if (active != 0u && !overflow && bodies >= max_bodies) atomicOr(st.status, 4u);
+    cudaGraphSetConditional(handle, (active != 0u && !overflow && bodies < max_bodies) ? 1u : 0u);
 }
 
+// Swaps the filled ray queues into the trace slots.  A queue that overflowed counted
+// appends beyond its capacity (only the first cap entries were written, and status bit
+// 2 is set): the traced count is clamped to the capacity so that no kernel reads an
+// entry that was never written.
 __global__ void k_wf_prep(WfState st)
 {
-    st.qc[kQcTraceCont] = st.qc[kQcCont];
-    st.qc[kQcTraceMis] = st.qc[kQcMis];
-    st.qc[kQcTraceShadow] = st.qc[kQcShadow];
+    st.qc[kQcTraceCont] = (unsigned)min((int64_t)st.qc[kQcCont], st.cap_cont);
+    st.qc[kQcTraceMis] = (unsigned)min((int64_t)st.qc[kQcMis], st.cap_mis);
+    st.qc[kQcTraceShadow] = (unsigned)min((int64_t)st.qc[kQcShadow], st.cap_sh);
     st.qc[kQcCont] = 0;
     st.qc[kQcMis] = 0;
     st.qc[kQcShadow] = 0;
@@ -1073,7 +1079,7 @@ __global__ void __launch_bounds__(256) k_wf_logic(WfState st)
                 ++n_paths;
                 if (!isfinite(col.x) || !isfinite(col.y) || !isfinite(col.z)) ++n_nans;
                 float4 sum = st.isum[slot], cmp = st.icomp[slot];
-                if (!ADJ) kahan_add4(sum, cmp, col);
+                if (!ADJ) kahan_add4(sum, cmp, clamp_sample(V.cfg, col));
                 const int kdone = st.k[slot] + 1;
                 const int64_t local = item - V.item_base;
                 const int npix = V.cfg.width * V.cfg.height;
@@ -1422,6 +1428,12 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
     st.cap_cont = pool;
     st.cap_mis = pool * max_dl;
     st.cap_sh = pool * max_dl * (int64_t)max_lights;
+    if (tune.queue_limit > 0) {
+        // below the allocated capacities: appends beyond them are counted and dropped
+        st.cap_cont = std::min<int64_t>(st.cap_cont, tune.queue_limit);
+        st.cap_mis = std::min<int64_t>(st.cap_mis, tune.queue_limit);
+        st.cap_sh = std::min<int64_t>(st.cap_sh, tune.queue_limit);
+    }
     st.views = c->d_views;
     st.cnt = c->cnt;
     st.status = ctx->d_status;
@@ -1459,7 +1471,9 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
     }
     const double iter_bound =
         (total_samples / (double)pool + 4.0 * max_chunk + 8.0) * (max_depth + 2) * 4.0 * (ADJ ? 2.0 : 1.0) + 1000.0;
-    const int64_t max_launches = (int64_t)(iter_bound / tune.iters_per_graph) + 16;
+    int64_t max_launches = (int64_t)(iter_bound / tune.iters_per_graph) + 16;
+    if (tune.max_iterations > 0)
+        max_launches = std::min<int64_t>(max_launches, (tune.max_iterations + tune.iters_per_graph - 1) / tune.iters_per_graph);
     // optional per-kernel timing: event-record nodes around every trace and shade launch
     std::vector<cudaEvent_t>& pev = c->pev;
     if (tune.profile) {

@@ -284,7 +284,7 @@ class SceneSpec:
         return camera_struct(self.camera)
 
     def render_params(self, spp: int | None = None, seed: int = 0, mode: int = FM_MODE_WAVEFRONT,
-                      sample_offset: int = 0) -> RenderParams:
+                      sample_offset: int = 0, clamp: float = 0.0) -> RenderParams:
         r = self.renderer
         p = RenderParams()
         p.width = int(r.get("width", 1))
@@ -297,6 +297,7 @@ class SceneSpec:
         p.seed = seed
         p.mode = mode
         p.sample_offset = sample_offset
+        p.max_sample_value = clamp
         return p
 
 

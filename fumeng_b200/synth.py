@@ -213,8 +213,10 @@ def random_rays(rng: np.random.Generator, n: int, lo, hi, min_component: float =
     return r
 
 
-def hit_scene(seed: int, level: int = 4, boxes: int = 3) -> SceneSpec:
-    """Displaced icosphere + subdivided boxes + a few rectangles, identity transforms."""
+def hit_scene(seed: int, level: int = 4, boxes: int = 3, spheres: int = 0) -> SceneSpec:
+    """Displaced icosphere + subdivided boxes + a few rectangles, identity transforms,
+    and `spheres` analytic spheres with translation-only transforms (drawn after
+    everything else, so spheres=0 reproduces the earlier scenes exactly)."""
     rng = np.random.default_rng(seed)
     objs = []
     v, f = displaced_icosphere(level, seed)
@@ -226,10 +228,52 @@ def hit_scene(seed: int, level: int = 4, boxes: int = 3) -> SceneSpec:
         objs.append(Mesh((bv * s + c).astype(np.float32), bf, "m0"))
     objs.append(Rect((-2, -1.5, -2), (-2, -1.5, 2), (2, -1.5, 2), (2, -1.5, -2), "m0"))
     objs.append(Rect((-2, -2, 1.9), (2, -2, 1.9), (2, 2, 1.9), (-2, 2, 1.9), "m0"))
+    for _ in range(spheres):
+        r = float(np.float32(rng.uniform(0.1, 0.45)))
+        c = tuple(float(x) for x in rng.uniform(-1.4, 1.4, size=3).astype(np.float32))
+        objs.append(Sphere(r, translation=c, material="m0"))
     cam = {"type": "pin_hole", "pos": [0, 0, -4], "look_at": [0, 0, 0], "up": [0, 1, 0], "fov": 45.0, "aspect": 1.0}
     ren = {"width": 64, "height": 64, "spp": 1, "depth": 4}
     mats = [{"name": "m0", "type": "lambert_diffuse", "basecolor": [0.5, 0.5, 0.5]}]
     return SceneSpec(cam, ren, mats, objs)
+
+
+def single_mesh_hit_scene(level: int = 8) -> SceneSpec:
+    """The single-mesh configuration's geometry alone (the displaced icosphere of
+    single_mesh_scene, 1,310,720 triangles at level 8, mesh seed 1) with a Lambert
+    material, for closest-hit queries."""
+    v, f = displaced_icosphere(level, 1, amp=0.05)
+    cam = {"type": "pin_hole", "pos": [0.0, -4.0, 0.6], "look_at": [0.0, 0.0, 0.0], "up": [0, 0, 1], "fov": 40.0,
+           "aspect": 16 / 9}
+    ren = {"width": 64, "height": 36, "spp": 1, "depth": 4}
+    mats = [{"name": "m0", "type": "lambert_diffuse", "basecolor": [0.5, 0.5, 0.5]}]
+    return SceneSpec(cam, ren, mats, [Mesh(v.astype(np.float32), f, "m0")])
+
+
+def pinhole_rays(rng: np.random.Generator, camera: dict, nx: int, ny: int) -> np.ndarray:
+    """Primary rays of a pinhole camera: one jittered ray per cell of an nx x ny film
+    grid, direction = normalize(f + (2x-1) tan(fov/2) aspect s + (2y-1) tan(fov/2) u)
+    with the camera's forward f, side s and up u; computed in float64 and stored as
+    float32 (n x 8, tmin 0, tmax FLT_MAX).  Coherent rays for the closest-hit tests."""
+    pos = np.asarray(camera["pos"], np.float64)
+    f = np.asarray(camera["look_at"], np.float64) - pos
+    f /= np.linalg.norm(f)
+    up = np.asarray(camera.get("up", [0, 0, 1]), np.float64)
+    s = np.cross(up, f)
+    s /= np.linalg.norm(s)
+    u = np.cross(f, s)
+    th = np.tan(np.radians(float(camera.get("fov", 60.0))) / 2.0)
+    asp = float(camera.get("aspect", 1.0))
+    gx, gy = np.meshgrid(np.arange(nx), np.arange(ny), indexing="xy")
+    x = (gx.ravel() + rng.random(nx * ny)) / nx
+    y = (gy.ravel() + rng.random(nx * ny)) / ny
+    d = f[None] + ((2 * x - 1) * th * asp)[:, None] * s[None] + ((2 * y - 1) * th)[:, None] * u[None]
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r = np.zeros((nx * ny, 8), np.float32)
+    r[:, 0:3] = pos
+    r[:, 4:7] = d
+    r[:, 7] = np.finfo(np.float32).max
+    return r
 
 
 def material_scene(seed: int, res: int = 64, env_w: int = 128, env_h: int = 64, spp: int = 16, depth: int = 6) -> SceneSpec:

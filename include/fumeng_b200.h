@@ -170,6 +170,13 @@ typedef struct {
     uint64_t seed;
     int32_t mode;
     int32_t sample_offset;   /* first sample index (for split / decorrelated renders) */
+    /* Extension (the reference has no clamp): when > 0, each colour channel of every
+     * camera sample's radiance is limited to this value before it enters the pixel's
+     * sum (min(L, max_sample_value); NaN stays NaN).  0 renders the reference's
+     * estimator unchanged.  The clamped estimator is biased low; it exists for
+     * firefly-free previews and for comparisons whose variance must stay bounded.
+     * fm_render_adjoint requires 0. */
+    float max_sample_value;
 } fm_render_params;
 
 /* Counters of one render, read back after it completes. */
@@ -234,10 +241,17 @@ fm_status fm_render(fm_ctx* ctx, const fm_scene* scene, const fm_camera* camera,
                     int32_t flags, fm_render_stats* stats);
 
 /* Wavefront tuning: path-slot pool size (queue capacities scale with it), block sizes of
- * the trace and shade kernels, and iterations per captured CUDA graph. */
+ * the trace and shade kernels, and iterations per captured CUDA graph.  The last two
+ * fields bound a render below its automatic limits (0 = automatic): max_iterations caps
+ * the wavefront iterations (a render that still has work then stops and returns
+ * FM_ERR_TIMEOUT), queue_limit caps the entries of each ray queue (a render that needs
+ * more stops and returns FM_ERR_QUEUE_OVERFLOW).  Both leave the context usable; they
+ * exist to bound a render's time and to exercise those error paths. */
 typedef struct {
     int64_t pool;
     int32_t trace_block, shade_block, iters_per_graph;
+    int32_t max_iterations;
+    int32_t queue_limit;
 } fm_tuning;
 
 /* Replaces: running the reference once per scene (main.cpp:5-11, one SceneLoader and one

@@ -58,7 +58,8 @@ def lib(precision: str = "float") -> C.CDLL:
     L.fmref_trace_any.argtypes = [vp, _D, C.c_int64, C.POINTER(C.c_uint8), C.c_int]
     L.fmref_two_nearest.argtypes = [vp, _D, C.c_int64, _D, _D, C.c_int]
     L.fmref_camera_rays.argtypes = [vp, _D, _D, C.c_int64, _D]
-    L.fmref_render.argtypes = [vp, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _D, _D, _D, _D, C.c_int]
+    L.fmref_render.argtypes = [vp, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _D, _D, _D, _D, C.c_int,
+                               C.c_int, C.c_double, _D, _D]
     L.fmref_draw_frame.argtypes = [vp]
     L.fmref_draw_frame.restype = C.c_double
     L.fmref_load_image.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _D]
@@ -131,16 +132,24 @@ class RefScene:
         self.L.fmref_camera_rays(self.h, _dp(ndc), _dp(lens), len(ndc), _dp(out))
         return out
 
-    def render(self, spp: int, seed: int = 0, tile=None, threads: int = 0, aov: bool = False):
-        """Per-pixel sums over `spp` samples: returns dict of (h, w, 3) float64 arrays."""
+    def render(self, spp: int, seed: int = 0, tile=None, threads: int = 0, aov: bool = False, clamp: float = 0.0,
+               stride: int = 1):
+        """Per-pixel sums over `spp` samples: returns dict of (h, w, 3) float64 arrays
+        ("csum" / "csumsq": sums of the per-channel clamped sample colours when clamp > 0).
+        With stride > 1 only every stride-th pixel of the tile is rendered and the arrays
+        are (n, 3) over those pixels."""
         W, H, _ = self.image_size()
         x0, y0, w, h = tile if tile is not None else (0, 0, W, H)
-        s = np.zeros((h, w, 3))
-        s2 = np.zeros((h, w, 3))
-        a = np.zeros((h, w, 3)) if aov else None
-        nrm = np.zeros((h, w, 3)) if aov else None
-        self.L.fmref_render(self.h, seed, x0, y0, w, h, spp, _dp(s), _dp(s2), _dp(a), _dp(nrm), threads)
-        return {"sum": s, "sumsq": s2, "albedo": a, "normal": nrm, "spp": spp}
+        shape = (h, w, 3) if stride == 1 else ((w * h + stride - 1) // stride, 3)
+        s = np.zeros(shape)
+        s2 = np.zeros(shape)
+        a = np.zeros(shape) if aov else None
+        nrm = np.zeros(shape) if aov else None
+        cs = np.zeros(shape) if clamp > 0 else None
+        cs2 = np.zeros(shape) if clamp > 0 else None
+        self.L.fmref_render(self.h, seed, x0, y0, w, h, spp, _dp(s), _dp(s2), _dp(a), _dp(nrm), threads, stride,
+                            float(clamp), _dp(cs), _dp(cs2))
+        return {"sum": s, "sumsq": s2, "albedo": a, "normal": nrm, "csum": cs, "csumsq": cs2, "spp": spp}
 
     def draw_frame(self) -> float:
         return float(self.L.fmref_draw_frame(self.h))
@@ -220,6 +229,9 @@ def restate() -> C.CDLL:
     L.fmo_intersect_triangle.argtypes = [F, F, F, F]
     L.fmo_closest_bruteforce.argtypes = [F, C.c_int64, F, C.c_int64, C.POINTER(C.c_int32), F]
     L.fmo_closest_bruteforce.restype = None
+    L.fmo_intersect_sphere.argtypes = [F, F, C.c_float, F]
+    L.fmo_closest_bruteforce_spheres.argtypes = [F, C.c_int64, F, F, C.c_int64, F, C.c_int64, C.POINTER(C.c_int32), F]
+    L.fmo_closest_bruteforce_spheres.restype = None
     _cache["restate"] = L
     return L
 
@@ -233,4 +245,21 @@ def restate_closest(tri_pos: np.ndarray, rays: np.ndarray):
     F = C.POINTER(C.c_float)
     L.fmo_closest_bruteforce(tri.ctypes.data_as(F), len(tri), r.ctypes.data_as(F), len(r),
                              prim.ctypes.data_as(C.POINTER(C.c_int32)), t.ctypes.data_as(F))
+    return prim, t
+
+
+def restate_closest_spheres(tri_pos: np.ndarray, centers: np.ndarray, radii: np.ndarray, rays: np.ndarray):
+    """Exhaustive closest hit over triangles and translated spheres (prim >= n_tri: sphere
+    prim - n_tri)."""
+    L = restate()
+    tri = np.ascontiguousarray(tri_pos, np.float32).reshape(-1, 9)
+    cen = np.ascontiguousarray(centers, np.float32).reshape(-1, 3)
+    rad = np.ascontiguousarray(radii, np.float32).reshape(-1)
+    r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    prim = np.empty(len(r), np.int32)
+    t = np.empty(len(r), np.float32)
+    F = C.POINTER(C.c_float)
+    L.fmo_closest_bruteforce_spheres(tri.ctypes.data_as(F), len(tri), cen.ctypes.data_as(F), rad.ctypes.data_as(F),
+                                     len(rad), r.ctypes.data_as(F), len(r), prim.ctypes.data_as(C.POINTER(C.c_int32)),
+                                     t.ctypes.data_as(F))
     return prim, t

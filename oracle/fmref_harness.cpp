@@ -460,11 +460,15 @@ int fmref_camera_rays(void* h, const double* ndc, const double* lens, int64_t n,
 // (renderer.h:98-115) and integrator (path_tracing.cpp:34-117), over the image rows
 // [y0, y0+h) and columns [x0, x0+w) (row 0 = top, as Image stores it).  Each pixel's
 // mt19937_64 is seeded with splitmix64(seed ^ pixel); each thread owns a PathTracer.
-// Outputs (h x w x 3, double): per-pixel sums of color, color^2, albedo and normal
-// over `spp` samples.
+// With stride > 1 only every stride-th pixel of the tile (in row-major tile order) is
+// rendered.  Outputs (one row of 3 doubles per rendered pixel): per-pixel sums of color,
+// color^2, albedo and normal over `spp` samples; when clamp > 0 also the sums of the
+// sample colours limited per channel to clamp (min(c, clamp)) and of their squares.
 int fmref_render(void* hnd, uint64_t seed, int x0, int y0, int w, int h, int spp, double* sum,
-                 double* sumsq, double* albedo, double* normal, int nthreads)
+                 double* sumsq, double* albedo, double* normal, int nthreads, int stride, double clamp,
+                 double* csum, double* csumsq)
 {
+    if (stride < 1) stride = 1;
     auto* s = static_cast<RefScene*>(hnd);
     fe::Scene& scene = *s->loader.m_scene;
     const int W = s->width, H = s->height;
@@ -472,18 +476,20 @@ int fmref_render(void* hnd, uint64_t seed, int x0, int y0, int w, int h, int spp
     std::vector<std::shared_ptr<fe::PathTracer>> tracers(nthreads);
     for (auto& t : tracers) t = std::static_pointer_cast<fe::PathTracer>(fe::CreatePathTracer(s->pt_config));
     std::atomic<int64_t> next{0};
-    const int64_t npix = int64_t(w) * h;
+    const int64_t npix = (int64_t(w) * h + stride - 1) / stride;
     auto worker = [&](int tid) {
         fe::PathTracer& pt = *tracers[tid];
         const real res_x = real(W), res_y = real(H);
         for (;;) {
             const int64_t q = next.fetch_add(1);
             if (q >= npix) break;
-            const int row = y0 + int(q / w), i = x0 + int(q % w);
+            const int64_t tq = q * stride;
+            const int row = y0 + int(tq / w), i = x0 + int(tq % w);
             const int j = H - 1 - row;
             pt.m_sampler.rng.seed(splitmix64(seed ^ (uint64_t(row) * uint64_t(W) + uint64_t(i))));
             pt.m_sampler.udis.reset();
             double c[3] = {0, 0, 0}, c2[3] = {0, 0, 0}, a[3] = {0, 0, 0}, nn[3] = {0, 0, 0};
+            double cc[3] = {0, 0, 0}, cc2[3] = {0, 0, 0};
             for (int k = 0; k < spp; ++k) {
                 const vec2 film_sample = pt.m_sampler.Get2D();
                 const vec2 lens_sample = pt.m_sampler.Get2D();
@@ -495,6 +501,11 @@ int fmref_render(void* hnd, uint64_t seed, int x0, int y0, int w, int h, int spp
                     const double v = double(res.color[ch]);
                     c[ch] += v;
                     c2[ch] += v * v;
+                    if (clamp > 0.0) {
+                        const double vc = v > clamp ? clamp : v;
+                        cc[ch] += vc;
+                        cc2[ch] += vc * vc;
+                    }
                     a[ch] += double(res.albedo[ch]);
                     nn[ch] += double(res.normal[ch]);
                 }
@@ -504,6 +515,8 @@ int fmref_render(void* hnd, uint64_t seed, int x0, int y0, int w, int h, int spp
                 if (sumsq) sumsq[3 * q + ch] = c2[ch];
                 if (albedo) albedo[3 * q + ch] = a[ch];
                 if (normal) normal[3 * q + ch] = nn[ch];
+                if (csum) csum[3 * q + ch] = cc[ch];
+                if (csumsq) csumsq[3 * q + ch] = cc2[ch];
             }
         }
     };

@@ -102,3 +102,68 @@ void fmo_closest_bruteforce(const float* tri, int64_t ntri, const float* rays, i
         t_out[i] = bp >= 0 ? best : INFINITY;
     }
 }
+
+/* Sphere::IntersectSphere (src/engine/src/geometry/sphere.cpp:91-129, GetCoef :206-212)
+ * for a sphere whose object-to-world transform is the translation `center`: the
+ * object-space origin is o - center (Transform::ApplyToPoint of a translation is one
+ * rounded subtraction per component whatever the matrix-product order), the direction
+ * is unchanged; a = SquareSum(d), b = 2 dot(d, o), c = SquareSum(o) - r^2 (sums left to
+ * right), delta = b*b - 4*a*c, roots (-b -+ sqrt(delta)) * (0.5 / a); the nearer root in
+ * the inclusive range [tmin, tmax] (Ray::Contains) is returned.  Returns 1 on a hit. */
+int fmo_intersect_sphere(const float* ray, const float* center, float radius, float* t_out)
+{
+    const float o0 = ray[0] - center[0], o1 = ray[1] - center[1], o2 = ray[2] - center[2];
+    const float d0 = ray[4], d1 = ray[5], d2 = ray[6];
+    const float tmin = ray[3], tmax = ray[7];
+    const float a = d0 * d0 + d1 * d1 + d2 * d2;
+    const float b = 2.0f * (d0 * o0 + d1 * o1 + d2 * o2);
+    const float c = o0 * o0 + o1 * o1 + o2 * o2 - radius * radius;
+    float delta = b * b - 4.0f * a * c;
+    if (delta < 0) return 0;
+    delta = sqrtf(delta);
+    const float inv2a = 0.5f / a;
+    const float t0 = (-b - delta) * inv2a;
+    const float t1 = (-b + delta) * inv2a;
+    if (t0 >= tmin && t0 <= tmax) {
+        *t_out = t0;
+        return 1;
+    }
+    if (t1 >= tmin && t1 <= tmax) {
+        *t_out = t1;
+        return 1;
+    }
+    return 0;
+}
+
+/* Closest hit over triangles and translated spheres by exhaustive testing: triangles as
+ * fmo_closest_bruteforce; a sphere (Sphere::GetIntersect, sphere.cpp:40-55) is accepted
+ * when its root lies in [t_min, t_best] (BVHAggregate::GetIntersectImpl then shrinks
+ * t_max to it, bvh_aggregate.cpp:108-115).  Spheres are numbered after the triangles:
+ * prim[i] = ntri + sphere index for a sphere hit, -1 on a miss. */
+void fmo_closest_bruteforce_spheres(const float* tri, int64_t ntri, const float* centers, const float* radii,
+                                    int64_t nsph, const float* rays, int64_t nrays, int32_t* prim, float* t_out)
+{
+    for (int64_t i = 0; i < nrays; ++i) {
+        float r[8];
+        for (int k = 0; k < 8; ++k) r[k] = rays[8 * i + k];
+        float best = r[7];
+        int32_t bp = -1;
+        for (int64_t j = 0; j < ntri; ++j) {
+            float t;
+            r[7] = best;
+            if (!fmo_intersect_triangle(r, tri + 9 * j, &t, 0)) continue;
+            if (t > best || t <= 0.0f) continue;
+            best = t;
+            bp = (int32_t)j;
+        }
+        for (int64_t j = 0; j < nsph; ++j) {
+            float t;
+            r[7] = best;
+            if (!fmo_intersect_sphere(r, centers + 3 * j, radii[j], &t)) continue;
+            best = t;
+            bp = (int32_t)(ntri + j);
+        }
+        prim[i] = bp;
+        t_out[i] = bp >= 0 ? best : INFINITY;
+    }
+}

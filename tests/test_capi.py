@@ -39,3 +39,28 @@ def test_errors_without_device(fm_lib):
     assert st == fumeng_b200.FM_ERR_NO_DEVICE
     assert not h.value
     assert fm_lib.fm_last_error(None) == b"null context"
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    # the ctypes mirrors of the header's structs have the C compiler's sizes and offsets
+    import subprocess
+    structs = {"fm_texture_desc": fumeng_b200.TextureDesc, "fm_tex_ref": fumeng_b200.TexRef,
+               "fm_material_desc": fumeng_b200.MaterialDesc, "fm_light_desc": fumeng_b200.LightDesc,
+               "fm_scene_desc": fumeng_b200.SceneDesc, "fm_camera": fumeng_b200.Camera,
+               "fm_render_params": fumeng_b200.RenderParams, "fm_render_stats": fumeng_b200.RenderStats,
+               "fm_tuning": fumeng_b200.Tuning, "fm_grad_desc": fumeng_b200.GradDesc}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "fumeng_b200.h"', 'int main(void) {']
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname}.{fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("return 0; }")
+    src = tmp_path / "abi.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "abi"
+    subprocess.run(["gcc", "-std=c11", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(l.split() for l in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines())
+    for cname, py in structs.items():
+        assert int(got[cname]) == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert int(got[f"{cname}.{fname}"]) == getattr(py, fname).offset, f"{cname}.{fname}"

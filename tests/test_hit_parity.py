@@ -1,6 +1,8 @@
 """Closest-hit object IDs and distances of the CUDA BVH match the reference's built-in BVH
 bit for bit on seeded ray sets, excluding rays whose two nearest hits lie within 1e-6
-relative t; occlusion queries match exactly."""
+relative t; occlusion queries match exactly.  Ray sets: random rays among meshes and
+rectangles, among meshes, rectangles and analytic spheres, and random and camera rays on
+the single-mesh configuration's 1.31 M-triangle mesh."""
 import numpy as np
 import pytest
 
@@ -19,7 +21,7 @@ def test_closest_and_any_hit_bit_exact(ctx, case):
     scene = ctx.create_scene(holder)
     try:
         st = scene.bvh_stats()
-        assert st["prims"] == holder.desc.num_triangles + 2 * holder.desc.num_rects
+        assert st["prims"] == holder.desc.num_triangles + 2 * holder.desc.num_rects + holder.desc.num_spheres
         obj, t = scene.trace_closest(rays)
         occ = scene.trace_any(shadow)
     finally:
@@ -27,6 +29,9 @@ def test_closest_and_any_hit_bit_exact(ctx, case):
     gt1, gt2 = g["t"], g["t2"]
     tie = np.abs(gt2 - gt1) <= 1e-6 * np.abs(gt1)
     keep = ~tie
+    print(f"{case[0]}: {len(rays)} rays, {int((g['obj'] >= 0).sum())} hits, {int(tie.sum())} near ties excluded")
+    if holder.desc.num_spheres:
+        assert np.isin(g["obj"], holder.sphere_object).sum() > 1000
     mism = np.nonzero(obj[keep] != g["obj"][keep])[0]
     assert mism.size == 0, f"{mism.size} object-ID mismatches of {keep.sum()} (first {mism[:10]})"
     assert np.array_equal(t[keep], gt1[keep])

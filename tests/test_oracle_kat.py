@@ -82,7 +82,7 @@ def _golden(name):
     return spec, rays, shadow, digest, g
 
 
-@pytest.mark.parametrize("name", ["hit_s1_l4", "hit_s2_l6"])
+@pytest.mark.parametrize("name", [c[0] for c in __import__("golden.make_golden", fromlist=["HIT_CASES"]).HIT_CASES])
 def test_golden_inputs_reproduce(name):
     spec, rays, shadow, digest, g = _golden(name)
     assert str(g["sha256"]) == digest, "synthetic scene/ray generator drifted from the golden fixture"
@@ -108,8 +108,32 @@ def test_restatement_matches_golden_closest():
     assert np.array_equal(t[keep], gt1[keep])
 
 
+def test_restatement_matches_golden_spheres():
+    # The C restatement of Sphere::IntersectSphere, with the triangles and rectangles,
+    # reproduces the reference's closest hits on the scene with analytic spheres.
+    spec, rays, shadow, digest, g = _golden("hit_s3_spheres")
+    d = spec.to_desc()
+    assert d.desc.num_spheres == 10
+    xf = d.sphere_xform.reshape(-1, 4, 4)
+    assert np.array_equal(xf[:, :3, :3], np.broadcast_to(np.eye(3, dtype=np.float32), (10, 3, 3)))
+    centers = xf[:, :3, 3]
+    rp = d.rect_pts.reshape(-1, 4, 3)
+    rect_tris = np.concatenate([np.stack([rp[:, 0], rp[:, 1], rp[:, 2]], 1), np.stack([rp[:, 2], rp[:, 3], rp[:, 0]], 1)])
+    tri = np.concatenate([d.tri_pos.reshape(-1, 3, 3), rect_tris]).reshape(-1, 9)
+    tri_obj = np.concatenate([d.tri_object, d.rect_object, d.rect_object])
+    sel = np.arange(0, len(rays), 5)[:4000]
+    prim, t = fmref.restate_closest_spheres(tri, centers, d.sphere_radius, rays[sel])
+    obj = np.where(prim < 0, -1, np.where(prim < len(tri), tri_obj[np.minimum(np.maximum(prim, 0), len(tri) - 1)],
+                                           d.sphere_object[np.maximum(prim - len(tri), 0)]))
+    gt1, gt2 = g["t"][sel], g["t2"][sel]
+    keep = ~(np.abs(gt2 - gt1) <= 1e-6 * np.abs(gt1))
+    assert np.isin(g["obj"][sel], d.sphere_object).sum() > 200, "too few sphere hits to pin the sphere test"
+    assert np.array_equal(obj[keep], g["obj"][sel][keep])
+    assert np.array_equal(t[keep], gt1[keep])
+
+
 @needs_ref
-@pytest.mark.parametrize("name", ["hit_s1_l4"])
+@pytest.mark.parametrize("name", ["hit_s1_l4", "hit_s3_spheres"])
 def test_live_oracle_reproduces_golden(name, tmp_path):
     spec, rays, shadow, digest, g = _golden(name)
     rs = fmref.RefScene(spec.write(tmp_path), "float")
