@@ -77,7 +77,16 @@ class Camera(C.Structure):
 class RenderParams(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32), ("depth", C.c_int32),
                 ("direct_loop", C.c_int32), ("rr_depth", C.c_int32), ("rr_coef", C.c_float), ("seed", C.c_uint64),
-                ("mode", C.c_int32), ("sample_offset", C.c_int32), ("max_sample_value", C.c_float)]
+                ("mode", C.c_int32), ("sample_offset", C.c_int32), ("max_sample_value", C.c_float),
+                ("region_x", C.c_int32), ("region_y", C.c_int32), ("region_w", C.c_int32), ("region_h", C.c_int32)]
+
+    def out_shape(self) -> tuple:
+        """(rows, columns) of the rendered images: the region's, or the whole image's."""
+        return (self.region_h, self.region_w) if self.region_w > 0 else (self.height, self.width)
+
+    def out_pixels(self) -> int:
+        h, w = self.out_shape()
+        return h * w
 
 
 class RenderStats(C.Structure):
@@ -220,9 +229,9 @@ class Context:
             flags = FM_FLAG_DEVICE_PTRS | (FM_FLAG_PROFILE if profile else 0)
             self.check(self.lib.fm_render_batch(self.h, n, sc, ca, pa, rgb_p, None, None, flags, tp, C.byref(stats)))
             return None, None, None, stats
-        rgb = [np.empty((p.height, p.width, 3), np.float32) for p in params]
-        alb = [np.empty((p.height, p.width, 3), np.float32) for p in params] if want_aov else None
-        nrm = [np.empty((p.height, p.width, 3), np.float32) for p in params] if want_aov else None
+        rgb = [np.empty(p.out_shape() + (3,), np.float32) for p in params]
+        alb = [np.empty(p.out_shape() + (3,), np.float32) for p in params] if want_aov else None
+        nrm = [np.empty(p.out_shape() + (3,), np.float32) for p in params] if want_aov else None
         rgb_p = (C.c_void_p * n)(*[a.ctypes.data for a in rgb])
         alb_p = (C.c_void_p * n)(*[a.ctypes.data for a in alb]) if want_aov else None
         nrm_p = (C.c_void_p * n)(*[a.ctypes.data for a in nrm]) if want_aov else None
@@ -315,7 +324,7 @@ class Scene:
         pa = (RenderParams * n)(*params)
         d_rgb = [np.ascontiguousarray(d, dtype=np.float32) for d in d_rgb]
         dp = (C.c_void_p * n)(*[d.ctypes.data for d in d_rgb])
-        imgs = [np.empty((p.height, p.width, 3), np.float32) for p in params] if want_image else None
+        imgs = [np.empty(p.out_shape() + (3,), np.float32) for p in params] if want_image else None
         ip = (C.c_void_p * n)(*[a.ctypes.data for a in imgs]) if want_image else None
         info = self.info()
         nt = info["textures"]
@@ -335,7 +344,7 @@ class Scene:
 
     def render(self, camera: Camera, params: RenderParams, want_aov: bool = True):
         """Returns (rgb, albedo, normal, stats) as HxWx3 float32 arrays (row 0 = top)."""
-        h, w = params.height, params.width
+        h, w = params.out_shape()
         rgb = np.empty((h, w, 3), np.float32)
         alb = np.empty((h, w, 3), np.float32) if want_aov else None
         nrm = np.empty((h, w, 3), np.float32) if want_aov else None

@@ -187,7 +187,7 @@ extern "C" fm_status fm_render_adjoint(fm_ctx* ctx, const fm_scene* scene, int32
         // per-view dLoss/dI inputs and image outputs
         std::vector<WfView> views((size_t)n);
         for (int32_t i = 0; i < n; ++i) {
-            img_floats[i] = (size_t)params[i].width * params[i].height * 3;
+            img_floats[i] = (size_t)out_width(params[i]) * out_height(params[i]) * 3;
             const size_t bytes = img_floats[i] * sizeof(float);
             if (dev) {
                 drgb_in[i] = const_cast<float*>(d_rgb[i]);

@@ -14,7 +14,7 @@ std::tuple<int, int, int> shape_class(int n, const fm_render_params* params, con
     double samples = 0.0;
     int lights = 0;
     for (int i = 0; i < n; ++i) {
-        samples += (double)params[i].width * params[i].height * params[i].spp;
+        samples += (double)out_width(params[i]) * out_height(params[i]) * params[i].spp;
         lights = std::max(lights, scenes[i]->dev.num_lights);
     }
     return {n, (int)std::floor(std::log2(std::max(1.0, samples))), lights};
@@ -80,7 +80,7 @@ fm_status autotune(fm_ctx* ctx, int32_t n, const fm_scene* const* scenes, const 
     // scratch images for the trial renders
     std::vector<float*> imgs((size_t)n, nullptr);
     size_t total = 0;
-    for (int i = 0; i < n; ++i) total += (size_t)params[i].width * params[i].height * 3;
+    for (int i = 0; i < n; ++i) total += (size_t)out_width(params[i]) * out_height(params[i]) * 3;
     float* buf = nullptr;
     FM_CUDA_TRY(ctx, cudaMalloc(&buf, total * sizeof(float)), "autotune alloc");
     Counters* cnt = nullptr;
@@ -91,7 +91,7 @@ fm_status autotune(fm_ctx* ctx, int32_t n, const fm_scene* const* scenes, const 
     size_t off = 0;
     for (int i = 0; i < n; ++i) {
         imgs[i] = buf + off;
-        off += (size_t)params[i].width * params[i].height * 3;
+        off += (size_t)out_width(params[i]) * out_height(params[i]) * 3;
     }
     // trial renders at up to 8 spp: enough samples per view that the pool's refill tail
     // does not dominate the trial (at 2 spp it favoured small pools)
@@ -211,7 +211,7 @@ extern "C" fm_status fm_render_batch(fm_ctx* ctx, int32_t n, const fm_scene* con
     char* staging = nullptr;
     size_t total = 0;
     for (int i = 0; i < n; ++i) {
-        bytes[i] = (size_t)params[i].width * params[i].height * 3 * sizeof(float);
+        bytes[i] = (size_t)out_width(params[i]) * out_height(params[i]) * 3 * sizeof(float);
         if (!dev) total += bytes[i] * (1 + (albedo && albedo[i] ? 1 : 0) + (normal && normal[i] ? 1 : 0));
     }
     Counters* d_cnt = nullptr;
@@ -253,9 +253,8 @@ extern "C" fm_status fm_render_batch(fm_ctx* ctx, int32_t n, const fm_scene* con
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
         cudaEventRecord(e0, ctx->stream);
-        for (int i = 0; i < n && st == FM_OK; ++i)
-            st = launch_megakernel(ctx, scenes[i], make_camera(cameras[i]), make_cfg(params[i]), d_rgb[i], d_alb[i],
-                                   d_nrm[i], d_cnt);
+        st = megakernel_views(ctx, make_views(n, scenes, cameras, params, d_rgb.data(), d_alb.data(), d_nrm.data(), 0),
+                              d_cnt);
         cudaEventRecord(e1, ctx->stream);
         cudaEventSynchronize(e1);
         float f = 0.0f;
@@ -288,7 +287,7 @@ extern "C" fm_status fm_render_batch(fm_ctx* ctx, int32_t n, const fm_scene* con
         stats->kernel_ms = ms;
         stats->trace_ms = tm.trace_ms;
         stats->shade_ms = tm.shade_ms;
-        stats->launches = wave ? tm.launches : (int64_t)n;
+        stats->launches = wave ? tm.launches : 1 + (int64_t)n;
     }
     if (hs & 1u) return set_error(ctx, FM_ERR_QUEUE_OVERFLOW, "batch: traversal stack overflow");
     if (hs & 2u) return set_error(ctx, FM_ERR_QUEUE_OVERFLOW, "batch: wavefront queue overflow");

@@ -263,13 +263,30 @@ FM_D float power_heuristic(float f, float g)
 
 // ---- render configuration ----------------------------------------------------------
 struct RenderCfg {
+    // width x height: the rendered pixels (the region, or the whole image); the camera
+    // sees the img_w x img_h image, and rendered pixel (i, row) is image pixel
+    // (x0 + i, y0 + row)
     int width, height, spp, depth, direct_loop, rr_depth;
+    int img_w, img_h, x0, y0;
     float rr_coef;
     uint64_t seed;
     int sample_offset;
     int rr_enabled;   // depth > rr_depth (path_tracing.cpp:107)
     float clamp;      // > 0: per-channel limit of a sample's radiance (extension), 0: off
 };
+
+// Camera-film coordinates and random-stream key of rendered pixel p: film position
+// (i, j) with j counted from the bottom row (renderer.h:98,106) and the image pixel index.
+struct PixelRef {
+    int i, j;
+    uint64_t key;
+};
+FM_HD PixelRef pixel_ref(const RenderCfg& cfg, int p)
+{
+    const int row = cfg.y0 + p / cfg.width;
+    const int i = cfg.x0 + p % cfg.width;
+    return PixelRef{i, cfg.img_h - 1 - row, (uint64_t)row * (uint64_t)cfg.img_w + (uint64_t)i};
+}
 
 // A camera sample's radiance as it enters the pixel sum: each channel limited to
 // cfg.clamp when the clamp is on (a NaN channel stays NaN, so it is still counted).

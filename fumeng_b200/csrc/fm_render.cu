@@ -1,6 +1,8 @@
 // Rendering: the plain per-pixel megakernel and the fm_render entry point.
+#include <algorithm>
 #include <array>
 #include <cmath>
+#include <vector>
 
 #include "fm_internal.h"
 #include "fm_path.cuh"
@@ -38,27 +40,49 @@ FM_D void add_counters(Counters* cnt, unsigned long long paths, unsigned long lo
     }
 }
 
-// Plain megakernel: one thread owns one pixel and runs its samples one after another
-// (the reference's per-pixel task, renderer.h:97-116).
-__global__ void __launch_bounds__(128) k_megakernel(const __grid_constant__ DevScene S, DevCamera cam, RenderCfg cfg,
-                                                    float* rgb, float* alb, float* nrm, Counters* cnt,
-                                                    uint32_t* status)
+// Plain megakernel: each thread runs whole camera paths (the reference's per-sample
+// RenderPixel inside DrawFrame's pixel task, renderer.h:97-116), one sample after
+// another, with no queues.  Work items are (view, pixel, chunk of consecutive samples)
+// over every view of the call, numbered and laid out like the wavefront's items (chunk
+// index major, then pixel, so a warp's lanes take neighbouring pixels); threads are
+// persistent and each takes its next item from a global counter as soon as it finishes
+// one, so one launch covers a whole batch and no SM idles while others have work.  Each
+// item writes its Kahan-compensated colour sum and its albedo / normal sums once; the
+// per-pixel reduction (reduce_views) adds the chunks in order, so the image does not
+// depend on which thread ran which item.
+__global__ void __launch_bounds__(128) k_megakernel(const WfView* __restrict__ views, int nviews, int64_t total_items,
+                                                    unsigned long long* next, Counters* cnt, uint32_t* status)
 {
-    const int npix = cfg.width * cfg.height;
     unsigned long long np = 0, nc = 0, ns = 0, nb = 0, nn = 0;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
-        const int row = p / cfg.width, i = p % cfg.width;
-        const int j = cfg.height - 1 - row;
+    for (;;) {
+        const int64_t it = (int64_t)atomicAdd(next, 1ull);
+        if (it >= total_items) break;
+        int lo = 0, hi = nviews - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (views[mid].item_base <= it)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const WfView& V = views[lo];
+        const RenderCfg cfg = V.cfg;
+        const int npix = cfg.width * cfg.height;
+        const int64_t local = it - V.item_base;
+        const int c = (int)(local / npix);
+        const PixelRef pr = pixel_ref(cfg, (int)(local % npix));
+        const int first = c * V.chunk;
+        const int n = min(V.chunk, cfg.spp - first);
         f3 sum = mk(0.0f), comp = mk(0.0f), asum = mk(0.0f), nsum = mk(0.0f);
-        for (int k = 0; k < cfg.spp; ++k) {
-            Rng rng = rng_for(cfg.seed, (uint64_t)p, (uint64_t)(cfg.sample_offset + k));
+        for (int k = 0; k < n; ++k) {
+            Rng rng = rng_for(cfg.seed, pr.key, (uint64_t)(cfg.sample_offset + first + k));
             const float fx = rng_1d(rng), fy = rng_1d(rng);
             const float lx = rng_1d(rng), ly = rng_1d(rng);
-            const float px = ((float)i + fx) / (float)cfg.width;
-            const float py = ((float)j + fy) / (float)cfg.height;
+            const float px = ((float)pr.i + fx) / (float)cfg.img_w;
+            const float py = ((float)pr.j + fy) / (float)cfg.img_h;
             f3 o, d;
-            camera_ray(cam, px, py, lx, ly, o, d);
-            const PathOut po = trace_path(S, cfg, o, d, rng, status);
+            camera_ray(V.cam, px, py, lx, ly, o, d);
+            const PathOut po = trace_path(*V.scene, cfg, o, d, rng, status);
             if (!isfinite(po.color.x) || !isfinite(po.color.y) || !isfinite(po.color.z)) ++nn;
             kahan_add(sum, comp, clamp_sample(cfg, po.color));
             asum += po.albedo;
@@ -67,11 +91,11 @@ __global__ void __launch_bounds__(128) k_megakernel(const __grid_constant__ DevS
             ns += po.shadow;
             nb += po.bounces;
         }
-        const float inv = 1.0f / (float)cfg.spp;
-        st3(rgb + 3 * (size_t)p, sum * inv);
-        if (alb) st3(alb + 3 * (size_t)p, asum * inv);
-        if (nrm) st3(nrm + 3 * (size_t)p, nsum * inv);
-        np += (unsigned long long)cfg.spp;
+        float4* P = V.partial + 3 * (size_t)local;
+        P[0] = make_float4(sum.x, sum.y, sum.z, 0.0f);
+        P[1] = make_float4(asum.x, asum.y, asum.z, 0.0f);
+        P[2] = make_float4(nsum.x, nsum.y, nsum.z, 0.0f);
+        np += (unsigned long long)n;
     }
     add_counters(cnt, np, nc, ns, nb, nn);
 }
@@ -114,8 +138,12 @@ DevCamera make_camera(const fm_camera& c)
 RenderCfg make_cfg(const fm_render_params& p)
 {
     RenderCfg r;
-    r.width = p.width;
-    r.height = p.height;
+    r.img_w = p.width;
+    r.img_h = p.height;
+    r.width = out_width(p);
+    r.height = out_height(p);
+    r.x0 = p.region_w > 0 ? p.region_x : 0;
+    r.y0 = p.region_w > 0 ? p.region_y : 0;
     r.spp = p.spp;
     r.depth = p.depth;
     r.direct_loop = p.direct_loop;
@@ -140,18 +168,76 @@ fm_status validate_render(fm_ctx* ctx, const fm_scene* scene, const fm_camera* c
         return set_error(ctx, FM_ERR_INVALID, "render: bad mode");
     if (p->sample_offset < 0) return set_error(ctx, FM_ERR_INVALID, "render: negative sample_offset");
     if (!(p->max_sample_value >= 0.0f)) return set_error(ctx, FM_ERR_INVALID, "render: max_sample_value must be >= 0");
+    if (p->region_w != 0 || p->region_h != 0) {
+        if (p->region_w <= 0 || p->region_h <= 0 || p->region_x < 0 || p->region_y < 0 ||
+            (int64_t)p->region_x + p->region_w > p->width || (int64_t)p->region_y + p->region_h > p->height)
+            return set_error(ctx, FM_ERR_INVALID, "render: region outside the image");
+    }
     return FM_OK;
+}
+
+fm_status megakernel_views(fm_ctx* ctx, std::vector<WfView> views, Counters* cnt)
+{
+    cudaStream_t s = ctx->stream;
+    const int block = 128;
+    int per_sm = 0;
+    FM_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_megakernel, block, 0), "megakernel occupancy");
+    per_sm = std::max(per_sm, 1);
+    const int grid = ctx->num_sms * per_sm;
+    const double resident = (double)grid * block;
+    // samples per item: enough items (about 32 per resident thread) that the threads
+    // finishing last hold little work, and no more (each item writes 48 B of sums)
+    double total_samples = 0.0;
+    for (const auto& v : views) total_samples += (double)v.cfg.width * v.cfg.height * v.cfg.spp;
+    const int target = (int)std::max(1.0, std::floor(total_samples / (32.0 * resident)));
+    int64_t item_base = 0;
+    for (auto& v : views) {
+        v.chunk = std::max(1, std::min(target, v.cfg.spp));
+        v.nchunks = (v.cfg.spp + v.chunk - 1) / v.chunk;
+        v.item_base = item_base;
+        item_base += (int64_t)v.cfg.width * v.cfg.height * v.nchunks;
+    }
+    const size_t head = 256;
+    const size_t views_bytes = (sizeof(WfView) * views.size() + 255) / 256 * 256;
+    const size_t partial_bytes = (size_t)item_base * 3 * sizeof(float4);
+    char* buf = nullptr;
+    FM_CUDA_TRY(ctx, cudaMallocAsync((void**)&buf, head + views_bytes + partial_bytes, s), "megakernel alloc");
+    auto* next = reinterpret_cast<unsigned long long*>(buf);
+    auto* d_views = reinterpret_cast<WfView*>(buf + head);
+    float4* partial = reinterpret_cast<float4*>(buf + head + views_bytes);
+    for (auto& v : views) {
+        v.partial = partial;
+        partial += 3 * (size_t)v.cfg.width * v.cfg.height * v.nchunks;
+    }
+    fm_status st = FM_OK;
+    cudaError_t e = cudaMemsetAsync(next, 0, sizeof(unsigned long long), s);
+    // pageable source: the driver stages it before this call returns
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_views, views.data(), sizeof(WfView) * views.size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        k_megakernel<<<grid, block, 0, s>>>(d_views, (int)views.size(), item_base, next, cnt, ctx->d_status);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess)
+        st = cuda_error(ctx, e, "megakernel");
+    else
+        st = reduce_views(ctx, views);
+    cudaFreeAsync(buf, s);
+    return st;
 }
 
 fm_status launch_megakernel(fm_ctx* ctx, const fm_scene* scene, const DevCamera& cam, const RenderCfg& cfg, float* rgb,
                             float* alb, float* nrm, Counters* cnt)
 {
-    const int npix = cfg.width * cfg.height;
-    const int block = 128;
-    int grid = (npix + block - 1) / block;
-    k_megakernel<<<grid, block, 0, ctx->stream>>>(scene->dev, cam, cfg, rgb, alb, nrm, cnt, ctx->d_status);
-    FM_CUDA_TRY(ctx, cudaGetLastError(), "megakernel launch");
-    return FM_OK;
+    WfView v{};
+    v.scene = scene->d_dev;
+    v.num_lights = scene->dev.num_lights;
+    v.cam = cam;
+    v.cfg = cfg;
+    v.rgb = rgb;
+    v.alb = alb;
+    v.nrm = nrm;
+    return megakernel_views(ctx, {v}, cnt);
 }
 
 }  // namespace fm
@@ -223,7 +309,7 @@ extern "C" fm_status fm_render(fm_ctx* ctx, const fm_scene* scene, const fm_came
         stats->kernel_ms = ms;
         stats->trace_ms = 0.0;
         stats->shade_ms = 0.0;
-        stats->launches = params->mode == FM_MODE_WAVEFRONT ? -1 : 1;
+        stats->launches = params->mode == FM_MODE_WAVEFRONT ? -1 : 2;
     }
     if (hs & 1u) return set_error(ctx, FM_ERR_QUEUE_OVERFLOW, "render: traversal stack overflow");
     if (hs & 2u) return set_error(ctx, FM_ERR_QUEUE_OVERFLOW, "render: wavefront queue overflow");

@@ -6,6 +6,9 @@
 namespace fm {
 
 DevCamera make_camera(const fm_camera& c);
+// Output image size of a render: the region's when one is set, else the whole image's.
+inline int out_width(const fm_render_params& p) { return p.region_w > 0 ? p.region_w : p.width; }
+inline int out_height(const fm_render_params& p) { return p.region_w > 0 ? p.region_h : p.height; }
 RenderCfg make_cfg(const fm_render_params& p);
 fm_status validate_render(fm_ctx* ctx, const fm_scene* scene, const fm_camera* camera, const fm_render_params* p);
 
@@ -59,6 +62,11 @@ fm_status launch_wavefront(fm_ctx* ctx, const fm_scene* scene, const DevCamera& 
                            float* alb, float* nrm, Counters* cnt);
 fm_status launch_megakernel(fm_ctx* ctx, const fm_scene* scene, const DevCamera& cam, const RenderCfg& cfg, float* rgb,
                             float* alb, float* nrm, Counters* cnt);
+// The plain megakernel over several views (possibly of different scenes) in one launch.
+fm_status megakernel_views(fm_ctx* ctx, std::vector<WfView> views, Counters* cnt);
+// Per pixel of each view: sums the view's partial sums in chunk order and writes the
+// mean colour, albedo and normal images.
+fm_status reduce_views(fm_ctx* ctx, const std::vector<WfView>& views);
 // Renders several views (possibly of different scenes) in one wavefront.
 fm_status wavefront_views(fm_ctx* ctx, const std::vector<WfView>& views, const WfTuning& tune, Counters* cnt,
                           WfTimes* times);

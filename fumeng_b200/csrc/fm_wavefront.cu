@@ -719,15 +719,13 @@ FM_D void start_sample(const WfState& st, int slot, const WfView& V, int64_t ite
 {
     const int npix = V.cfg.width * V.cfg.height;
     const int c = (int)(item_local / npix);
-    const int p = (int)(item_local % npix);
-    const int row = p / V.cfg.width, i = p % V.cfg.width;
-    const int j = V.cfg.height - 1 - row;
+    const PixelRef pr = pixel_ref(V.cfg, (int)(item_local % npix));
     const int sample = c * V.chunk + k;
-    Rng rng = rng_for(V.cfg.seed, (uint64_t)p, (uint64_t)(V.cfg.sample_offset + sample));
+    Rng rng = rng_for(V.cfg.seed, pr.key, (uint64_t)(V.cfg.sample_offset + sample));
     const float fx = rng_1d(rng), fy = rng_1d(rng);
     const float lx = rng_1d(rng), ly = rng_1d(rng);
-    const float px = ((float)i + fx) / (float)V.cfg.width;
-    const float py = ((float)j + fy) / (float)V.cfg.height;
+    const float px = ((float)pr.i + fx) / (float)V.cfg.img_w;
+    const float py = ((float)pr.j + fy) / (float)V.cfg.img_h;
     f3 o, d;
     camera_ray(V.cam, px, py, lx, ly, o, d);
     st.ro[slot] = make_float4(o.x, o.y, o.z, 0.0f);
@@ -1626,6 +1624,16 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
 }
 
 }  // namespace
+
+fm_status reduce_views(fm_ctx* ctx, const std::vector<WfView>& views)
+{
+    for (const auto& v : views) {
+        const int npix = v.cfg.width * v.cfg.height;
+        k_wf_reduce<<<std::min((npix + 255) / 256, ctx->num_sms * 16), 256, 0, ctx->stream>>>(v);
+    }
+    FM_CUDA_TRY(ctx, cudaGetLastError(), "reduce views");
+    return FM_OK;
+}
 
 fm_status wavefront_views(fm_ctx* ctx, const std::vector<WfView>& views, const WfTuning& tune, Counters* cnt,
                           WfTimes* times)

@@ -284,7 +284,7 @@ class SceneSpec:
         return camera_struct(self.camera)
 
     def render_params(self, spp: int | None = None, seed: int = 0, mode: int = FM_MODE_WAVEFRONT,
-                      sample_offset: int = 0, clamp: float = 0.0) -> RenderParams:
+                      sample_offset: int = 0, clamp: float = 0.0, region=None) -> RenderParams:
         r = self.renderer
         p = RenderParams()
         p.width = int(r.get("width", 1))
@@ -298,6 +298,8 @@ class SceneSpec:
         p.mode = mode
         p.sample_offset = sample_offset
         p.max_sample_value = clamp
+        if region is not None:
+            p.region_x, p.region_y, p.region_w, p.region_h = (int(v) for v in region)
         return p
 
 

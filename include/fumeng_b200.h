@@ -177,6 +177,12 @@ typedef struct {
      * firefly-free previews and for comparisons whose variance must stay bounded.
      * fm_render_adjoint requires 0. */
     float max_sample_value;
+    /* Extension: render region.  With region_w > 0 only the pixels [region_x, region_x +
+     * region_w) x [region_y, region_y + region_h) of the width x height image (row 0 =
+     * top) are rendered, and the outputs are region_w x region_h images of exactly those
+     * pixels' values in a full render with the same seed (random streams are keyed by
+     * the full image's pixel index).  region_w = region_h = 0: the whole image. */
+    int32_t region_x, region_y, region_w, region_h;
 } fm_render_params;
 
 /* Counters of one render, read back after it completes. */
@@ -259,8 +265,9 @@ typedef struct {
  * cameras[i] with params[i] -- in one persistent wavefront whose kernel sequence is
  * captured as a CUDA graph.  rgb[i] / albedo[i] / normal[i] receive view i's images
  * (albedo and normal arrays, or their entries, may be NULL).  All params must use
- * FM_MODE_WAVEFRONT, or all FM_MODE_MEGAKERNEL (then the views are rendered one after
- * another by the plain megakernel, the baseline).  tuning == NULL selects the tuning
+ * FM_MODE_WAVEFRONT, or all FM_MODE_MEGAKERNEL (then all views are rendered by one launch
+ * of the plain megakernel, the baseline: persistent threads that each run whole camera
+ * paths, taking (view, pixel, sample chunk) items from a shared counter).  tuning == NULL selects the tuning
  * cached for this batch's shape class, running the autotuner on first use. */
 fm_status fm_render_batch(fm_ctx* ctx, int32_t n, const fm_scene* const* scenes, const fm_camera* cameras,
                           const fm_render_params* params, float* const* rgb, float* const* albedo,
