@@ -46,8 +46,8 @@ METRIC = "Mpaths/s batched wavefront vs plain megakernel at relMSE≤1e-3; adjoi
 WORKLOAD = "batched: 64 scenes x (1-40 displaced icosphere/box meshes, 1k-200k tris), 512x256 HDR env + 1 area light, 128^2-512^2, 4-64 spp, depth 8"
 NSCENES = 64
 # DRAM bytes the trace kernel moves per traced ray (read + write, cold L2 at each
-# launch), from ncu over every trace launch of the 8-scene case of this workload
-# (profiles/k_wf_trace_batched8.md); traffic grows with the rays a launch traces.
+# launch), from an ncu capture of trace launches of the 8-scene case of this workload;
+# traffic grows with the rays a launch traces.
 TRACE_DRAM_BYTES_PER_RAY = 80.4
 
 
@@ -128,9 +128,20 @@ def desc_bytes(holder) -> int:
 
 # ---- reference arm (CPU) ---------------------------------------------------------------
 
-def run_reference(args, specs=None, steps=None, warmup=None, sample_scenes=2, spp=1):
-    """The reference's own CPU integrator (oracle/_ref float build, RenderPixel per camera
-    sample on all host threads) on a bounded sample of the workload per step."""
+# Camera paths per scene and step in the CPU sample: about this many pixels of each of
+# the 64 scenes, spread over the image (every k-th pixel in row-major order, k odd so
+# that the sample runs diagonally across rows), at 1 spp.
+REF_PIXELS_PER_SCENE = 1024
+
+
+def run_reference(args, steps=None, warmup=None, per_scene=REF_PIXELS_PER_SCENE):
+    """The reference's own CPU integrator (oracle/_ref float build: its RenderPixel per
+    camera sample, on all host threads) on a bounded sample of the workload per step:
+    about `per_scene` pixels of every one of the 64 scenes at 1 spp.  The reference's
+    speed differs by three orders of magnitude between scenes, so the sample measures
+    each scene's rate r_s and reports the rate of the whole workload, whose scene s has
+    P_s = width x height x spp paths: sum_s P_s / sum_s (P_s / r_s).  Scene loading (the
+    reference's loader and BVH build) happens before the timed steps."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import fmref  # noqa: E402  (test/baseline infrastructure)
     from fumeng_b200 import synth
@@ -140,28 +151,42 @@ def run_reference(args, specs=None, steps=None, warmup=None, sample_scenes=2, sp
     warmup = args.warmup if warmup is None else warmup
     threads = os.cpu_count() or 1
     tmp = Path(tempfile.mkdtemp(prefix="fm_ref_"))
-    times, paths = [], []
-    loaded = {}
+    loaded, workload_paths = [], np.zeros(NSCENES)
+    for s in range(NSCENES):
+        spec = synth.batch_scene(s)
+        workload_paths[s] = float(spec.renderer["width"]) * float(spec.renderer["height"]) * float(spec.renderer["spp"])
+        loaded.append(fmref.RefScene(spec.write(tmp / f"s{s}"), "float"))
+    times = []
+    per_scene_t = np.zeros(NSCENES)
+    per_scene_p = np.zeros(NSCENES)
+    sample_paths = 0
     for it in range(warmup + steps):
-        ids = [(it * sample_scenes + k) % NSCENES for k in range(sample_scenes)]
-        t_step, p_step = 0.0, 0
-        for s in ids:
-            if s not in loaded:
-                spec = synth.batch_scene(s)
-                loaded[s] = fmref.RefScene(spec.write(tmp / f"s{s}"), "float")
-            rs = loaded[s]
+        t_step = 0.0
+        for s, rs in enumerate(loaded):
             w, h, _ = rs.image_size()
+            stride = max(1, (w * h) // per_scene) | 1
+            n = (w * h + stride - 1) // stride
             t0 = time.perf_counter()
-            rs.render(spp, seed=it, threads=threads)
-            t_step += time.perf_counter() - t0
-            p_step += w * h * spp
+            rs.render(1, seed=it, threads=threads, stride=stride)
+            dt = time.perf_counter() - t0
+            t_step += dt
+            if it >= warmup:
+                per_scene_t[s] += dt
+                per_scene_p[s] += n
         if it >= warmup:
             times.append(t_step)
-            paths.append(p_step)
-    value = sum(paths) / sum(times) / 1e6
+        sample_paths = int(per_scene_p.sum() / max(1, it + 1 - warmup))
+    for rs in loaded:
+        rs.close()
+    rates = per_scene_p / np.maximum(per_scene_t, 1e-12)
+    value = float(workload_paths.sum() / np.sum(workload_paths / rates)) / 1e6
     return {"value": value, "unit": "Mpaths/s", "cores": threads, "kind": "reference",
-            "sample": f"{sample_scenes} scenes x {spp} spp per step (scenes rotate through the batch), "
-                      f"reference float build, all {threads} host threads",
+            "sample": f"about {per_scene} pixels of each of the {NSCENES} scenes at 1 spp per step "
+                      f"({sample_paths} paths), reference float build, all {threads} host threads, "
+                      f"{warmup} warm-up step(s); value = workload paths / sum over scenes of "
+                      f"(scene paths / scene rate)",
+            "per_scene_mpaths": {"min": float(rates.min() / 1e6), "median": float(np.median(rates) / 1e6),
+                                 "max": float(rates.max() / 1e6)},
             "ms_per_step": 1e3 * sum(times) / len(times)}
 
 
@@ -367,7 +392,7 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic", "config": {"workload": WORKLOAD, "scenes": NSCENES},
-                "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample", "per_scene_mpaths")},
                 "e2e": {"value": r["value"], "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -508,8 +533,9 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r = run_reference(args, steps=2, warmup=0, sample_scenes=4, spp=1)
-        cpu = {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")} if "unavailable" not in r else r
+        r = run_reference(args, steps=2, warmup=1)
+        cpu = ({k: r[k] for k in ("value", "unit", "cores", "kind", "sample", "per_scene_mpaths")}
+               if "unavailable" not in r else r)
 
     for s in scenes:
         s.destroy()

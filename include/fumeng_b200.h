@@ -341,9 +341,15 @@ typedef struct {
  * samples (use a seed different from the forward render's for a decorrelated
  * estimate).  Each sample's path is traced once for its radiance and replayed with the
  * same random numbers to accumulate derivatives, so memory does not grow with depth or
- * spp.  Sampling, pdfs and MIS weights are treated as constants.  rgb (NULL, or an
- * array of per-view NULL or width*height*3 buffers) receives the primal image of the
- * samples used.  Host buffers unless FM_FLAG_DEVICE_PTRS. */
+ * spp.  The sampled directions are held fixed (the derivative of the estimator for its
+ * random numbers, which is unbiased for the gradient of the image's expectation);
+ * everything that depends on the parameters along the fixed path is differentiated: the
+ * BSDF values, the sampling pdfs in f / pdf, the MIS weights built from them and, for
+ * env-map texels, the env map's sampling and reported densities (their normalisation
+ * over all texels included).  rgb (NULL, or an
+ * array of per-view NULL or width*height*3 buffers -- region size when a region is set)
+ * receives the primal image of the samples used.  params[v].max_sample_value must be 0.
+ * Host buffers unless FM_FLAG_DEVICE_PTRS. */
 fm_status fm_render_adjoint(fm_ctx* ctx, const fm_scene* scene, int32_t num_views, const fm_camera* cameras,
                             const fm_render_params* params, const float* const* d_rgb, float* const* rgb,
                             const fm_grad_desc* grads, int32_t flags, fm_render_stats* stats);

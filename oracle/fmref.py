@@ -27,8 +27,9 @@ def available(precision: str = "float") -> bool:
     return LIBS[precision].exists()
 
 
-def build(reference_root: str = "/root/reference") -> bool:
-    """Compile the oracle libraries when the reference sources are present."""
+def build(reference_root: str) -> bool:
+    """Compile the oracle libraries from the reference checkout at reference_root when
+    its sources are present."""
     if not Path(reference_root, "src/engine").exists():
         return available("float") and available("double")
     subprocess.run(["make", "-C", str(HERE), "-j8", "ref", f"REF={reference_root}"], check=True,
