@@ -17,7 +17,10 @@
 //
 // Traversal keeps a short stack of node groups (child_base, hit bits << 24 | imask),
 // one entry per tree level at most, and tests each node's leaf primitives as soon as
-// the node is intersected.
+// the node is intersected.  The stack is an accessor type: a plain per-thread array
+// (LocalStack), or one whose top entries live in shared memory (SharedTopStack), which
+// keeps the traversal's most frequent stack traffic out of the L1 cache that holds the
+// nodes.
 #pragma once
 #include "fm_common.cuh"
 #include "fm_scene.cuh"
@@ -140,6 +143,31 @@ FM_D bool test_prim(const TraceScene& S, const RayPre& rp, f3 o, f3 d, int slot,
     return true;
 }
 
+// A per-thread traversal stack in local memory.
+struct LocalStack {
+    uint2 e[kTraversalStack];
+    FM_D void put(int i, uint2 v) { e[i] = v; }
+    FM_D uint2 get(int i) const { return e[i]; }
+};
+
+// A traversal stack whose K top entries are in shared memory (entry i of thread tid at
+// top[i * stride], stride = the block size, so a warp's accesses are consecutive 8-byte
+// words) and whose deeper entries are in local memory.
+template <int K>
+struct SharedTopStack {
+    uint2* top;
+    int stride;
+    uint2 e[kTraversalStack - K];
+    FM_D void put(int i, uint2 v)
+    {
+        if (i < K)
+            top[i * stride] = v;
+        else
+            e[i - K] = v;
+    }
+    FM_D uint2 get(int i) const { return i < K ? top[i * stride] : e[i - K]; }
+};
+
 // Resumable traversal: the state of one query, advanced one node at a time by
 // trav_step.  Kernels that keep a warp busy with a stream of rays (fetching a new ray
 // into a lane as soon as its query completes) drive it directly; trace_ray_any runs it
@@ -180,7 +208,8 @@ FM_D void trav_begin(Traversal& t, const TraceScene& S, f3 o, f3 d, float tmin, 
 // stack when the current group is exhausted.  Returns true when the query is complete
 // (t.hit.prim >= 0 on a hit).  *overflow is set when the traversal stack would overflow
 // (the builder bounds the tree depth so that this cannot happen for trees it accepted).
-FM_D bool trav_step(Traversal& t, const TraceScene& S, uint2* stack, uint32_t* overflow)
+template <class Stack>
+FM_D bool trav_step(Traversal& t, const TraceScene& S, Stack& stack, uint32_t* overflow)
 {
     if (t.ngrp.y > 0x00ffffffu) {
         const uint32_t key = 31u - __clz(t.ngrp.y) - 24u;
@@ -190,7 +219,7 @@ FM_D bool trav_step(Traversal& t, const TraceScene& S, uint2* stack, uint32_t* o
         const int child = (int)(t.ngrp.x + __popc(imask & ((1u << slot) - 1u)));
         if (t.ngrp.y > 0x00ffffffu) {
             if (t.sp < kTraversalStack)
-                stack[t.sp++] = t.ngrp;
+                stack.put(t.sp++, t.ngrp);
             else if (overflow)
                 atomicOr(overflow, 1u);
         }
@@ -206,7 +235,7 @@ FM_D bool trav_step(Traversal& t, const TraceScene& S, uint2* stack, uint32_t* o
     }
     if (t.ngrp.y <= 0x00ffffffu) {
         if (t.sp == 0) return true;
-        t.ngrp = stack[--t.sp];
+        t.ngrp = stack.get(--t.sp);
     }
     return false;
 }
@@ -218,7 +247,7 @@ static __device__ __noinline__ Hit trace_ray_any(TraceScene S, f3 o, f3 d, float
                                                  uint32_t* overflow)
 {
     Traversal t;
-    uint2 stack[kTraversalStack];
+    LocalStack stack;
     trav_begin(t, S, o, d, tmin, tmax, any);
     while (!trav_step(t, S, stack, overflow)) {
     }

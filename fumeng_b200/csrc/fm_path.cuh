@@ -12,11 +12,22 @@ struct PathOut {
     int closest, shadow, bounces;
 };
 
+// The path's large steps are called, not inlined: a lane of a warp may be sampling a
+// Disney lobe while its neighbour evaluates a dielectric or traverses the BVH, and with
+// every call site inlined the kernel's code outgrows the instruction caches (most issue
+// slots then wait for instruction fetch).  One copy each of BSDF sampling, hit
+// construction, next-event estimation and the MIS-BSDF step keeps the loop compact.
+static __device__ __noinline__ BsdfSample path_bsdf_sample(const Bsdf& b, f3 wo, f3 u) { return bsdf_sample(b, wo, u); }
+static __device__ __noinline__ HitInfo path_make_hit(const DevScene& S, f3 o, f3 d, const Hit& hit)
+{
+    return make_hit(S, o, d, hit);
+}
+
 // MisLight: NEE for one light.  The BSDF value and pdf are evaluated before the shadow
 // ray (the reference traces first), which skips rays whose contribution is zero without
 // changing any result.
-FM_D f3 mis_light(const DevScene& S, const DevLight& L, const HitInfo& h, const Bsdf& b, f3 u, int& nshadow,
-                  uint32_t* status)
+static __device__ __noinline__ f3 mis_light(const DevScene& S, const DevLight& L, const HitInfo& h, const Bsdf& b,
+                                            f3 u, int& nshadow, uint32_t* status)
 {
     LightSample ls;
     if (!light_sample(S, L, h.pos, u, ls)) return mk(0.0f);
@@ -34,9 +45,10 @@ FM_D f3 mis_light(const DevScene& S, const DevLight& L, const HitInfo& h, const 
 }
 
 // MisBSDF: a separate BSDF sample, traced to an emitter or the environment.
-FM_D f3 mis_bsdf(const DevScene& S, const HitInfo& h, const Bsdf& b, f3 u, int& nclosest, uint32_t* status)
+static __device__ __noinline__ f3 mis_bsdf(const DevScene& S, const HitInfo& h, const Bsdf& b, f3 u, int& nclosest,
+                                           uint32_t* status)
 {
-    const BsdfSample s = bsdf_sample(b, h.wo, u);
+    const BsdfSample s = path_bsdf_sample(b, h.wo, u);
     if (length(s.f) < kEpsPdf || s.pdf < kEpsPdf) return mk(0.0f);
     const f3 wi = normalize(s.wi);
     const f3 ro = spawn_origin(h, wi);
@@ -52,7 +64,7 @@ FM_D f3 mis_bsdf(const DevScene& S, const HitInfo& h, const Bsdf& b, f3 u, int& 
     const int obj = __ldg(S.prim_obj + lh.prim);
     const int li = __ldg(S.obj_light + obj);
     if (li < 0) return mk(0.0f);
-    const HitInfo lhit = make_hit(S, ro, wi, lh);
+    const HitInfo lhit = path_make_hit(S, ro, wi, lh);
     const f3 l2s = normalize(ro - lhit.pos);
     const DevLight& L = S.lights[li];
     const f3 rad = dot(lhit.ng, l2s) > 0 ? ld3(L.radiance) : mk(0.0f);
@@ -76,7 +88,7 @@ FM_D PathOut trace_path(const DevScene& S, const RenderCfg& cfg, f3 o, f3 d, Rng
             if (depth == 1 && S.env_light >= 0) out.color = env_radiance(S, cam_dir);
             break;
         }
-        const HitInfo h = make_hit(S, o, d, hit);
+        const HitInfo h = path_make_hit(S, o, d, hit);
         if (depth == 1) {
             const int li = __ldg(S.obj_light + h.obj);
             if (li >= 0) {
@@ -98,7 +110,7 @@ FM_D PathOut trace_path(const DevScene& S, const RenderCfg& cfg, f3 o, f3 d, Rng
             direct += beta * mis_bsdf(S, h, b, rng_3d(rng), out.closest, status);
         }
         out.color += direct / (float)cfg.direct_loop;
-        const BsdfSample s = bsdf_sample(b, h.wo, rng_3d(rng));
+        const BsdfSample s = path_bsdf_sample(b, h.wo, rng_3d(rng));
         if (length(s.f) < kEpsPdf || s.pdf < kEpsPdf) break;
         beta *= s.f * absdot(h.ng, s.wi) / s.pdf;
         o = spawn_origin(h, s.wi);

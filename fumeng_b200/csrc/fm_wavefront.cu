@@ -609,11 +609,17 @@ FM_D void finish_shadow(const WfState& st, int64_t q, const DevScene& S, const H
 // lane whose query completes takes the next unclaimed ray (one atomic per warp and
 // refill), so lanes do not idle while the warp's slowest traversal finishes, and the
 // loop holds nothing but traversal.
+// Stack entries per thread kept in shared memory by k_wf_trace (the rest in local memory).
+constexpr int kTraceSmemStack = 8;
+
 __global__ void __launch_bounds__(256, 4) k_wf_trace(WfState st)
 {
     const int64_t nc = st.qc[kQcTraceCont], nm = st.qc[kQcTraceMis], ns = st.qc[kQcTraceShadow];
     const int64_t total = nc + nm + ns;
-    uint2 stack[kTraversalStack];
+    extern __shared__ uint2 s_stack[];
+    SharedTopStack<kTraceSmemStack> stack;
+    stack.top = s_stack + threadIdx.x;
+    stack.stride = blockDim.x;
     Traversal t;
     const DevScene* Sp = nullptr;
     int kind = -1;   // ray kind held by this lane, -1 for none
@@ -1457,6 +1463,7 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
     // one graph body = `iters_per_graph` iterations of prep -> trace -> resolve -> shade
     // (Disney) -> shade (other materials) [-> replay shading] -> logic [-> gradient scatter]
     const int trace_grid = sms * 16;
+    const size_t trace_smem = sizeof(uint2) * kTraceSmemStack * (size_t)tune.trace_block;
     const int shade_grid = (int)std::min<int64_t>((pool + tune.shade_block - 1) / tune.shade_block, (int64_t)sms * 32);
     const int logic_grid = (int)std::min<int64_t>((pool + 255) / 256, (int64_t)sms * 32);
     const int resolve_grid = sms * 16;
@@ -1486,7 +1493,7 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
         for (int it = 0; it < tune.iters_per_graph; ++it) {
             k_wf_prep<<<1, 1, 0, s>>>(st);
             if (tune.profile) cudaEventRecordWithFlags(pev[3 * it], s, cudaEventRecordExternal);
-            k_wf_trace<<<trace_grid, tune.trace_block, 0, s>>>(st);
+            k_wf_trace<<<trace_grid, tune.trace_block, trace_smem, s>>>(st);
             if (tune.profile) cudaEventRecordWithFlags(pev[3 * it + 1], s, cudaEventRecordExternal);
             k_wf_resolve<ADJ><<<resolve_grid, 256, 0, s>>>(st);
             k_wf_shade<kClsDisney><<<shade_grid, tune.shade_block, 0, s>>>(st);

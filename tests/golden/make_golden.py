@@ -3,7 +3,7 @@
 Run on a machine that has the reference sources (the oracle libraries are built from
 them by oracle/Makefile):
 
-    python tests/golden/make_golden.py [hit] [images] [adjoint] [batch] [single] [large] [inverse] [digests] [force]
+    python tests/golden/make_golden.py [hit] [images] [adjoint] [batch] [single] [large] [inverse] [adjoint_texels] [digests] [force]
 
 Scenes and rays are regenerated from seeds by fumeng_b200.synth, so each fixture stores
 only the reference's answers plus a SHA-256 of the inputs, which the tests recompute to
@@ -270,6 +270,139 @@ def make_inverse_tile():
     render_clamped_fixture(inverse_target_scene(), "inverse_t0", INVERSE_SPP, INVERSE_SEED, BATCH_CLAMP, INVERSE_TILE)
 
 
+# ---- texel gradients of the inverse-rendering configuration ---------------------------
+# 4x4-pixel tiles of the first view (256^2) on a 17x17 grid over the image centre, the
+# first 256 that see the mesh through their centre pixel.  For each tile, the texel seen through its centre pixel (the camera ray's nearest hit on the
+# mesh, at its interpolated texture coordinate) and one channel of it, in turn: basecolor
+# r, g, b, roughness (rm G), metallic (rm B).  The loss of a case is sum(w * I) over its
+# tile with seeded weights w in [0.5, 1.5].
+C3_TILE, C3_GRID, C3_STEP, C3_CASES = 4, 17, 8, 256
+C3_CHANNELS = [("basecolor", 0), ("basecolor", 1), ("basecolor", 2), ("rm", 1), ("rm", 2)]
+
+
+def _nearest_hit(tri, o, d):
+    """Moller-Trumbore over all triangles (float64): (triangle index, b1, b2) or None."""
+    v0, v1, v2 = tri[:, 0], tri[:, 1], tri[:, 2]
+    e1, e2 = v1 - v0, v2 - v0
+    pv = np.cross(d, e2)
+    det = np.einsum("ij,ij->i", e1, pv)
+    ok = np.abs(det) > 1e-14
+    inv = np.where(ok, 1.0 / np.where(ok, det, 1.0), 0.0)
+    tv = o - v0
+    b1 = np.einsum("ij,ij->i", tv, pv) * inv
+    qv = np.cross(tv, e1)
+    b2 = (qv @ d) * inv
+    t = np.einsum("ij,ij->i", e2, qv) * inv
+    hit = ok & (b1 >= 0) & (b2 >= 0) & (b1 + b2 <= 1) & (t > 1e-6)
+    if not hit.any():
+        return None
+    k = int(np.argmin(np.where(hit, t, np.inf)))
+    return k, float(b1[k]), float(b2[k])
+
+
+def c3_gradient_cases(spec=None):
+    """[(tile (x0, y0, w, h), texture name, (row, col, channel), weights (4, 4, 3))]"""
+    spec = spec or inverse_target_scene()
+    desc = spec.to_desc()
+    tri = desc.tri_pos.reshape(-1, 3, 3).astype(np.float64)
+    uv = desc.tri_uv.reshape(-1, 3, 2).astype(np.float64)
+    cam = spec.camera
+    W, H = int(spec.renderer["width"]), int(spec.renderer["height"])
+    pos = np.asarray(cam["pos"], np.float64)
+    f = np.asarray(cam["look_at"], np.float64) - pos
+    f /= np.linalg.norm(f)
+    up = np.asarray(cam["up"], np.float64)
+    up /= np.linalg.norm(up)
+    sv = np.cross(up, f)
+    sv /= np.linalg.norm(sv)
+    uvv = np.cross(f, sv)
+    th = np.tan(np.radians(float(cam["fov"])) / 2.0)
+    asp = float(cam.get("aspect", 1.0))
+    x_start = (W - C3_GRID * C3_STEP) // 2
+    y_start = (H - C3_GRID * C3_STEP) // 2
+    rng = np.random.default_rng(23)
+    cases = []
+    for k in range(C3_GRID * C3_GRID):
+        x0 = x_start + C3_STEP * (k % C3_GRID)
+        y0 = y_start + C3_STEP * (k // C3_GRID)
+        col, row = x0 + C3_TILE // 2, y0 + C3_TILE // 2
+        px, py = (col + 0.5) / W, (H - 1 - row + 0.5) / H
+        d = f + (2 * px - 1) * th * asp * sv + (2 * py - 1) * th * uvv
+        d /= np.linalg.norm(d)
+        w = rng.uniform(0.5, 1.5, (C3_TILE, C3_TILE, 3)).astype(np.float32)
+        h = _nearest_hit(tri, pos, d)
+        if h is None or uv is None:
+            continue
+        ti, b1, b2 = h
+        u, v = (1 - b1 - b2) * uv[ti, 0] + b1 * uv[ti, 1] + b2 * uv[ti, 2]
+        tex, ch = C3_CHANNELS[len(cases) % len(C3_CHANNELS)]
+        th_, tw_ = spec.textures[tex].shape[:2]
+        tx = int(np.clip(np.floor((u - np.floor(u)) * tw_), 0, tw_ - 1))
+        ty = int(np.clip(np.floor((v - np.floor(v)) * th_), 0, th_ - 1))
+        cases.append(((x0, y0, C3_TILE, C3_TILE), tex, (ty, tx, ch), w))
+        if len(cases) == C3_CASES:
+            break
+    return cases
+
+
+# Central differences of the same tile losses from the reference's double build for a
+# few of these cases: the perturbed channel is its texel's largest (so the .hdr file's
+# shared exponent, and with it the other channels, stay unchanged) and the step is two
+# quanta of that exponent; per-pixel seeding makes the +-h renders use common random
+# numbers.
+C3_REF = {"cases": 4, "spp": 8192, "seeds": [401, 402, 403, 404]}
+
+
+def rgbe_step(x):
+    """Two quanta of the RGBE mantissa at value x (8-bit mantissa, shared exponent)."""
+    e = np.floor(np.log2(x)) + 1.0
+    return 2.0 * 2.0 ** (e - 8.0)
+
+
+def c3_reference_cases(spec=None):
+    spec = spec or inverse_target_scene()
+    out = []
+    for k, (tile, tex, (ty, tx, ch), w) in enumerate(c3_gradient_cases(spec)):
+        texel = spec.textures[tex][ty, tx]
+        x = float(texel[ch])
+        if x < 0.3 or x > 0.9 or x < float(np.max(texel)):
+            continue
+        h = rgbe_step(x)
+        if np.floor(np.log2(x - h)) != np.floor(np.log2(x + h)):
+            continue
+        out.append((k, tile, tex, (ty, tx, ch), w, h))
+        if len(out) == C3_REF["cases"]:
+            break
+    return out
+
+
+def make_adjoint_texels():
+    from fumeng_b200.scene import rgbe_quantize
+    spec = inverse_target_scene()
+    cases = c3_reference_cases(spec)
+    fd = np.zeros((len(cases), len(C3_REF["seeds"])))
+    spp = C3_REF["spp"]
+    for ci, (k, tile, tex, (ty, tx, ch), w, h) in enumerate(cases):
+        orig = spec.textures[tex]
+        for si, seed in enumerate(C3_REF["seeds"]):
+            L = []
+            for sign in (1.0, -1.0):
+                t = orig.copy()
+                t[ty, tx, ch] = orig[ty, tx, ch] + sign * h
+                assert np.array_equal(rgbe_quantize(t), t), "perturbed texture is not representable in .hdr"
+                spec.textures[tex] = t
+                with tempfile.TemporaryDirectory() as d:
+                    rs = fmref.RefScene(spec.write(Path(d)), "double")
+                    r = rs.render(spp, seed=seed, tile=tile)
+                    rs.close()
+                L.append(float((w.astype(np.float64) * r["sum"] / spp).sum()))
+            spec.textures[tex] = orig
+            fd[ci, si] = (L[0] - L[1]) / (2 * h)
+        print("c3 texel fd", k, tex, (ty, tx, ch), fd[ci].mean(), fd[ci].std(ddof=1) / 2, flush=True)
+    np.savez_compressed(GOLDEN / "adj_fd_texels_ref.npz", fd=fd, spp=spp, seeds=np.asarray(C3_REF["seeds"]),
+                        case_index=np.asarray([c[0] for c in cases]), h=np.asarray([c[5] for c in cases]))
+
+
 # SHA-256 of the scene inputs behind each image fixture (scene_digests.json), so that a
 # change of the scene generators that would invalidate a fixture is caught on the CPU.
 def scene_digest(spec) -> str:
@@ -376,6 +509,8 @@ if __name__ == "__main__":
         make_large_small()
     if "inverse" in what:
         make_inverse_tile()
+    if "adjoint_texels" in what:
+        make_adjoint_texels()
     if "digests" in what:
         make_digests()
     print("done in %.1fs" % (time.time() - t0))
