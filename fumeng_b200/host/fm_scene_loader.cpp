@@ -12,6 +12,7 @@
 #include <fstream>
 #include <sstream>
 #include <stdexcept>
+#include <system_error>
 #include <thread>
 
 #include "fm_image_io.h"
@@ -483,7 +484,9 @@ void SceneLoader::PreloadMeshes(const Json& objs)
             load(*sh, "type", type);
             if (type != "triangle_mesh") continue;
             load(*sh, "path", path);
-            if (m_meshes.emplace(m_root + path, PreloadedMesh{}).second) paths.push_back(m_root + path);
+            auto ins = m_meshes.emplace(m_root + path, PreloadedMesh{});
+            if (ins.second) paths.push_back(m_root + path);
+            ++ins.first->second.uses;
         } catch (const std::exception&) {
         }
     }
@@ -502,9 +505,21 @@ void SceneLoader::PreloadMeshes(const Json& objs)
         }
     };
     std::vector<std::thread> pool;
-    for (size_t t = 1; t < nthreads; ++t) pool.emplace_back(work);
+    try {
+        for (size_t t = 1; t < nthreads; ++t) pool.emplace_back(work);
+    } catch (const std::system_error&) {
+        // no more threads: the ones started and this thread share the files
+    }
     work();
     for (auto& t : pool) t.join();
+}
+
+void SceneLoader::release_mesh(const std::string& path)
+{
+    // a mesh's parsed file is dropped once the last object that names it is flattened,
+    // so that peak host memory stays near one copy of the scene's geometry
+    auto it = m_meshes.find(path);
+    if (it != m_meshes.end() && --it->second.uses <= 0) m_meshes.erase(it);
 }
 
 const ObjData& SceneLoader::mesh_data(const std::string& path)
@@ -602,6 +617,7 @@ void SceneLoader::ParseRenderObject(const Json& j)
             }
             (void)huv;
         }
+        release_mesh(m_root + path);
     } else if (type == "sphere") {
         float radius = 1.0f;
         load(*sh, "radius", radius);

@@ -90,6 +90,7 @@ private:
     // objects are flattened in order (mesh_data hands the results out).
     void PreloadMeshes(const Json& objs);
     const ObjData& mesh_data(const std::string& path);
+    void release_mesh(const std::string& path);
     fm_tex_ref ParseTexture(const Json& j, float dflt[3]);
     int32_t LoadTexture(const std::string& path, const std::string& sampler, const std::string& wrap_u,
                         const std::string& wrap_v);
@@ -105,6 +106,7 @@ private:
     struct PreloadedMesh {
         ObjData data;
         std::exception_ptr error;   // rethrown when the object that names the file is reached
+        int uses = 0;               // render objects still to flatten that name this file
     };
     std::map<std::string, PreloadedMesh> m_meshes;
 };

@@ -87,6 +87,28 @@ def write_hdr(path: Path, rgb: np.ndarray) -> None:
     Path(path).write_bytes(b"".join(parts))
 
 
+def write_png8(path: Path, codes01: np.ndarray) -> None:
+    """8-bit RGB PNG of values that are multiples of 1/255 (stored as round(255 x))."""
+    import struct
+    import zlib
+    a = np.clip(np.round(np.asarray(codes01, np.float64) * 255.0), 0, 255).astype(np.uint8)
+    h, w, _ = a.shape
+    raw = b"".join(b"\x00" + a[y].tobytes() for y in range(h))
+
+    def chunk(t, d):
+        return struct.pack(">I", len(d)) + t + d + struct.pack(">I", zlib.crc32(t + d) & 0xffffffff)
+    Path(path).write_bytes(b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, 8, 2, 0, 0, 0)) +
+                           chunk(b"IDAT", zlib.compress(raw, 6)) + chunk(b"IEND", b""))
+
+
+def srgb_to_linear(c: np.ndarray) -> np.ndarray:
+    """Image::to_linear of a decoded LDR image (utils.h SrgbToLinear), in float32."""
+    c = np.asarray(c, np.float32)
+    lo = c * np.float32(1.0 / 12.92)
+    hi = np.power((c + np.float32(0.055)) * np.float32(1.0 / 1.055), np.float32(2.4)).astype(np.float32)
+    return np.where(c <= np.float32(0.04045), lo, hi).astype(np.float32)
+
+
 # ---- transforms ---------------------------------------------------------------------
 
 def trs_matrix(translation, rotation_deg, scale) -> np.ndarray:
@@ -171,6 +193,9 @@ class SceneSpec:
     objects: list = field(default_factory=list)     # Mesh | Rect | Sphere
     lights: list = field(default_factory=list)      # dicts: env {texture, rotation, factor} | directional
     textures: dict = field(default_factory=dict)    # name -> HxWx3 float32 (RGBE-representable)
+    # textures stored as 8-bit sRGB PNG files: their arrays hold the sRGB codes / 255, and
+    # the scene decodes them to linear values as the reference's Image loader does
+    ldr_textures: set = field(default_factory=set)
 
     # -- derived ---------------------------------------------------------------------
     def material_index(self) -> dict:
@@ -188,8 +213,12 @@ class SceneSpec:
         root.mkdir(parents=True, exist_ok=True)
         tex_files = {}
         for name, arr in self.textures.items():
-            fn = f"tex_{name}.hdr"
-            write_hdr(root / fn, arr)
+            if name in self.ldr_textures:
+                fn = f"tex_{name}.png"
+                write_png8(root / fn, arr)
+            else:
+                fn = f"tex_{name}.hdr"
+                write_hdr(root / fn, arr)
             tex_files[name] = fn
 
         def tex_json(v):
@@ -404,7 +433,8 @@ class DescHolder:
         self.sphere_object = np.asarray(sph_obj, np.int32)
 
         # textures
-        self.tex_arrays = [np.ascontiguousarray(spec.textures[n], np.float32) for n in tex_names]
+        self.tex_arrays = [np.ascontiguousarray(srgb_to_linear(spec.textures[n]) if n in spec.ldr_textures
+                                                else spec.textures[n], np.float32) for n in tex_names]
         self.textures = (TextureDesc * max(1, len(tex_names)))()
         for i, a in enumerate(self.tex_arrays):
             self.textures[i].width = a.shape[1]

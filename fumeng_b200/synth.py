@@ -276,6 +276,55 @@ def pinhole_rays(rng: np.random.Generator, camera: dict, nx: int, ny: int) -> np
     return r
 
 
+def textured_scene(res: int = 48, spp: int = 16, depth: int = 5) -> SceneSpec:
+    """Image textures in every form the reference's ImageTexture has: a ground quad whose
+    uv run over [0, 3]^2 (repeat wrap) with a nearest-filtered 8-bit sRGB PNG checker; a
+    UV sphere whose Disney basecolor is a bilinear HDR texture sampled with clamp wrap
+    (uv over [-0.5, 1.5]) and whose roughness / metallic come from a nearest-filtered PNG
+    (decoded from sRGB like every LDR texture); a box with a bilinear, repeat-wrapped PNG
+    basecolor; a rectangle light and a small sky."""
+    rng = np.random.default_rng(31)
+    # ground quad, uv 0..3
+    g = np.array([[-2, -2, 0], [2, -2, 0], [2, 2, 0], [-2, 2, 0]], np.float32)
+    guv = np.array([[0, 0], [3, 0], [3, 3], [0, 3]], np.float32)
+    gf = np.array([[0, 1, 2], [0, 2, 3]])
+    chk = np.zeros((8, 8, 3), np.float32)
+    ii, jj = np.meshgrid(np.arange(8), np.arange(8), indexing="ij")
+    on = ((ii + jj) % 2 == 0)
+    chk[on] = np.array([200, 180, 60]) / 255.0
+    chk[~on] = np.array([40, 90, 160]) / 255.0
+    # sphere, uv mapped to [-0.5, 1.5]
+    sv, sf, suv = uv_sphere(48, 24, 0.6, (-0.5, 0.3, 0.6))
+    suv = (suv * 2.0 - 0.5).astype(np.float32)
+    hdr_base = rgbe_quantize(smooth_texture(32, 41, 0.1, 0.9))
+    rm = np.round(rng.uniform(0, 255, (16, 16, 3))) / 255.0
+    rm[..., 0] = 0.0
+    # box with repeat-wrapped bilinear PNG
+    bv, bf = subdivided_box(2)
+    bv = (bv * 0.35 + np.array([0.8, -0.4, 0.35])).astype(np.float32)
+    buv = np.stack([bv[:, 0] * 2.0 + bv[:, 2], bv[:, 1] * 2.0 - bv[:, 2]], 1).astype(np.float32)
+    stripes = np.round(rng.uniform(20, 235, (4, 8, 3))) / 255.0
+    objs = [Mesh(g, gf, "ground", uvs=guv), Mesh(sv, sf, "ball", uvs=suv), Mesh(bv, bf, "box", uvs=buv),
+            Rect((-0.5, -0.5, 3.0), (-0.5, 0.5, 3.0), (0.5, 0.5, 3.0), (0.5, -0.5, 3.0), "ground",
+                 emittance=(10.0, 10.0, 9.0))]
+    mats = [{"name": "ground", "type": "lambert_diffuse",
+             "basecolor": {"image": "checker", "sampler": "nearest", "wrap_u": "repeat", "wrap_v": "repeat"}},
+            {"name": "ball", "type": "disney", "specular": 0.5, "clearcoat": 0.3,
+             "basecolor": {"image": "hdrbase", "sampler": "linear", "wrap_u": "clamp", "wrap_v": "clamp"},
+             "roughness": {"image": "rm", "sampler": "nearest", "wrap_u": "repeat", "wrap_v": "repeat"},
+             "metallic": {"image": "rm", "sampler": "nearest", "wrap_u": "repeat", "wrap_v": "repeat"}},
+            {"name": "box", "type": "lambert_diffuse",
+             "basecolor": {"image": "stripes", "sampler": "linear", "wrap_u": "repeat", "wrap_v": "repeat"}}]
+    env = sky_env(64, 32, 33, sun_peak=30.0, sun_sigma_deg=6.0)
+    cam = {"type": "pin_hole", "pos": [0.4, -3.6, 2.0], "look_at": [0.0, 0.0, 0.4], "up": [0, 0, 1], "fov": 45.0,
+           "aspect": 1.0}
+    ren = {"width": res, "height": res, "spp": spp, "depth": depth, "rr_depth": 3, "rr_coef": 0.85}
+    lights = [{"type": "env", "texture": "sky", "rotation": [0, 0, 30.0], "factor": 1.0}]
+    tex = {"checker": chk, "hdrbase": hdr_base, "rm": rm.astype(np.float32), "stripes": stripes.astype(np.float32),
+           "sky": env}
+    return SceneSpec(cam, ren, mats, objs, lights, tex, ldr_textures={"checker", "rm", "stripes"})
+
+
 def material_scene(seed: int, res: int = 64, env_w: int = 128, env_h: int = 64, spp: int = 16, depth: int = 6) -> SceneSpec:
     """Small scene exercising every BSDF and light kind: Disney icosphere (specTrans 0),
     Disney clearcoat sphere, dielectric sphere, conductor sphere, Lambert floor, a

@@ -3,7 +3,7 @@
 Run on a machine that has the reference sources (the oracle libraries are built from
 them by oracle/Makefile):
 
-    python tests/golden/make_golden.py [hit] [images] [adjoint] [batch] [single] [large] [inverse] [adjoint_texels] [digests] [force]
+    python tests/golden/make_golden.py [hit] [images] [adjoint] [batch] [single] [large] [inverse] [textured] [adjoint_texels] [digests] [force]
 
 Scenes and rays are regenerated from seeds by fumeng_b200.synth, so each fixture stores
 only the reference's answers plus a SHA-256 of the inputs, which the tests recompute to
@@ -178,16 +178,18 @@ def moments(r, key, spp):
     return mean.astype(np.float32), var.astype(np.float32)
 
 
-def render_clamped_fixture(spec, name, spp, seed, clamp, tile=None):
+def render_clamped_fixture(spec, name, spp, seed, clamp, tile=None, aov=False):
     with tempfile.TemporaryDirectory() as d:
         rs = fmref.RefScene(spec.write(Path(d)), "double")
         t0 = time.time()
-        r = rs.render(spp, seed=seed, tile=tile, clamp=clamp)
+        r = rs.render(spp, seed=seed, tile=tile, clamp=clamp, aov=aov)
         dt = time.time() - t0
         rs.close()
     mean, var = moments(r, "sum", spp)
     cmean, cvar = moments(r, "csum", spp)
     extra = {"tile": np.asarray(tile)} if tile is not None else {}
+    if aov:
+        extra.update(albedo=(r["albedo"] / spp).astype(np.float32), normal=(r["normal"] / spp).astype(np.float32))
     np.savez_compressed(GOLDEN / f"{name}.npz", mean=mean, var=var, cmean=cmean, cvar=cvar, spp=spp, clamp=clamp,
                         stride=1, **extra)
     print(name, "tile", tile, "%.1fs" % dt, "mean", mean.mean(axis=(0, 1)), "clamped", cmean.mean(axis=(0, 1)),
@@ -268,6 +270,19 @@ def make_inverse_tile():
     if (GOLDEN / "inverse_t0.npz").exists():
         return
     render_clamped_fixture(inverse_target_scene(), "inverse_t0", INVERSE_SPP, INVERSE_SEED, BATCH_CLAMP, INVERSE_TILE)
+
+
+# Image textures in every form ImageTexture has (synth.textured_scene: nearest and
+# bilinear filtering, repeat and clamp wrap, 8-bit sRGB PNG and HDR files, an LDR
+# roughness / metallic map decoded from sRGB), full 48x48 frame, double build, 16384 spp,
+# plain and clamped sums and the albedo / normal AOVs.
+TEXTURED_SPP, TEXTURED_SEED = 16384, 19
+
+
+def make_textured():
+    if (GOLDEN / "textured.npz").exists():
+        return
+    render_clamped_fixture(synth.textured_scene(), "textured", TEXTURED_SPP, TEXTURED_SEED, BATCH_CLAMP, aov=True)
 
 
 # ---- texel gradients of the inverse-rendering configuration ---------------------------
@@ -423,6 +438,8 @@ def scene_digest(spec) -> str:
         h.update(str(getattr(o, "material", "")).encode())
     for name in sorted(spec.textures):
         h.update(name.encode())
+        if name in getattr(spec, "ldr_textures", ()):
+            h.update(b"ldr")
         h.update(np.ascontiguousarray(spec.textures[name], np.float32).tobytes())
     return h.hexdigest()
 
@@ -431,7 +448,8 @@ def image_fixture_scenes():
     """(fixture name, scene builder) of every image fixture."""
     out = [(name, builder) for name, builder, _, _, _ in IMAGE_CASES]
     out += [(f"batch_s{s}", (lambda s=s: synth.batch_scene(s))) for s in BATCH_CASES]
-    out += [("single", single_scene), ("large_small", large_small_scene), ("inverse_t0", inverse_target_scene)]
+    out += [("single", single_scene), ("large_small", large_small_scene), ("inverse_t0", inverse_target_scene),
+            ("textured", synth.textured_scene)]
     return out
 
 
@@ -509,6 +527,8 @@ if __name__ == "__main__":
         make_large_small()
     if "inverse" in what:
         make_inverse_tile()
+    if "textured" in what:
+        make_textured()
     if "adjoint_texels" in what:
         make_adjoint_texels()
     if "digests" in what:
