@@ -104,6 +104,13 @@ class Tuning(C.Structure):
                 "iters_per_graph": self.iters_per_graph}
 
 
+FM_POST_TONEMAP, FM_POST_LINEAR_TO_SRGB, FM_POST_SRGB_TO_LINEAR, FM_POST_DENOISE = range(4)
+
+
+class PostStep(C.Structure):
+    _fields_ = [("type", C.c_int32), ("lum", C.c_float)]
+
+
 class FumengError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"fumeng_b200 error {status}: {message}")
@@ -153,6 +160,8 @@ def load_library() -> C.CDLL:
         "fm_scene_update_texture": ([vp, vp, C.c_int32, vp, C.c_int32], C.c_int),
         "fm_scene_info": ([vp, vp, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                            C.POINTER(C.c_int32)], C.c_int),
+        "fm_postprocess": ([vp, C.c_int32, C.c_int32, C.POINTER(PostStep), C.c_int32, vp, vp, vp, vp, vp, vp,
+                            C.c_int32], C.c_int),
         "fm_render_adjoint": ([vp, vp, C.c_int32, C.POINTER(Camera), C.POINTER(RenderParams), C.POINTER(vp),
                                C.POINTER(vp), C.POINTER(GradDesc), C.c_int32, C.POINTER(RenderStats)], C.c_int),
     }
@@ -167,7 +176,7 @@ def load_library() -> C.CDLL:
 EXPORTED_SYMBOLS = ["fm_ctx_create", "fm_ctx_destroy", "fm_last_error", "fm_scene_create", "fm_scene_destroy",
                     "fm_scene_bvh_stats", "fm_trace_closest", "fm_trace_any", "fm_render", "fm_render_batch",
                     "fm_autotune_batch", "fm_scene_load", "fm_draw_frame", "fm_trace_closest_noalloc",
-                    "fm_scene_update_texture", "fm_render_adjoint", "fm_scene_info"]
+                    "fm_scene_update_texture", "fm_render_adjoint", "fm_scene_info", "fm_postprocess"]
 
 
 def _ptr(a, ctype=C.c_void_p):
@@ -252,6 +261,22 @@ class Context:
         params = RenderParams()
         self.check(self.lib.fm_scene_load(self.h, str(json_path).encode(), C.byref(h), C.byref(cam), C.byref(params)))
         return Scene(self, h, None), cam, params
+
+    def postprocess(self, steps, rgb, albedo=None, normal=None):
+        """The post-process chain and 8-bit conversion (fm_postprocess) of HxWx3 float32
+        images; steps: [(type, lum)].  Returns (rgb after the chain, rgb8, albedo8,
+        normal8), the 8-bit arrays None where the input was None."""
+        rgb = np.array(rgb, np.float32, copy=True, order="C")
+        h, w, _ = rgb.shape
+        st = (PostStep * max(1, len(steps)))(*[PostStep(int(t), float(l)) for t, l in steps])
+        a = None if albedo is None else np.ascontiguousarray(albedo, np.float32)
+        n = None if normal is None else np.ascontiguousarray(normal, np.float32)
+        c8 = np.empty((h, w, 3), np.uint8)
+        a8 = np.empty((h, w, 3), np.uint8) if a is not None else None
+        n8 = np.empty((h, w, 3), np.uint8) if n is not None else None
+        self.check(self.lib.fm_postprocess(self.h, w, h, st, len(steps), _ptr(rgb), _ptr(a), _ptr(n), _ptr(c8),
+                                           _ptr(a8), _ptr(n8), 0))
+        return rgb, c8, a8, n8
 
     def draw_frame(self, json_path) -> None:
         """SceneLoader::DrawFrame: render the scene file and write its PNG outputs."""

@@ -240,16 +240,23 @@ ImageF read_image(const std::string& path, bool is_hdr) { return is_hdr ? read_h
 
 void write_png(const std::string& path, int w, int h, const float* rgb)
 {
+    std::vector<uint8_t> q((size_t)3 * w * h);
+    for (size_t i = 0; i < q.size(); ++i) {
+        float c = rgb[i];
+        c = c > 1.0f ? 1.0f : (c < 0.0f ? 0.0f : c);
+        if (!(c == c)) c = 0.0f;
+        q[i] = (uint8_t)std::lround(255.0f * c);
+    }
+    write_png_u8(path, w, h, q.data());
+}
+
+void write_png_u8(const std::string& path, int w, int h, const uint8_t* rgb8)
+{
     std::string raw;
     raw.reserve((size_t)(3 * w + 1) * h);
     for (int y = 0; y < h; ++y) {
         raw += (char)0;
-        for (int x = 0; x < 3 * w; ++x) {
-            float c = rgb[(size_t)y * 3 * w + x];
-            c = c > 1.0f ? 1.0f : (c < 0.0f ? 0.0f : c);
-            if (!(c == c)) c = 0.0f;
-            raw += (char)(uint8_t)std::lround(255.0f * c);
-        }
+        raw.append(reinterpret_cast<const char*>(rgb8) + (size_t)y * 3 * w, (size_t)3 * w);
     }
     uLongf cap = compressBound((uLong)raw.size());
     std::string z(cap, '\0');

@@ -6,6 +6,7 @@
 // SrgbToLinear (core/utils.h:120-125).  Writing mirrors Image::save_to_file
 // (image.cpp:81-109): PNG bytes are round(255 * clamp(c, 0, 1)).
 #pragma once
+#include <cstdint>
 #include <string>
 #include <vector>
 
@@ -19,6 +20,8 @@ struct ImageF {
 // Reads .hdr (when `is_hdr`) or PNG.  Throws std::runtime_error on failure.
 ImageF read_image(const std::string& path, bool is_hdr);
 void write_png(const std::string& path, int w, int h, const float* rgb);
+// 8-bit RGB PNG of already quantized values (row-major, top row first).
+void write_png_u8(const std::string& path, int w, int h, const uint8_t* rgb8);
 void write_hdr(const std::string& path, int w, int h, const float* rgb);
 
 float srgb_to_linear(float c);

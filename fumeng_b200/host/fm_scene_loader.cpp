@@ -711,7 +711,8 @@ void SceneLoader::ParsePostProcess(const Json& root)
         if (s.type == "tonemapping") {
             load(p, "lum", s.lum);
         } else if (s.type == "oidn_denoise") {
-            warn("oidn_denoise: OIDN is not available; the step leaves the image unchanged");
+            warn("oidn_denoise: OIDN is not available; an edge-avoiding a-trous filter guided by the albedo and "
+                 "normal images runs instead");
         } else if (s.type != "linear_to_srgb" && s.type != "srgb_to_linear") {
             warn("Post process type not supported: " + s.type + ".");
             continue;
@@ -743,23 +744,25 @@ fm_status SceneLoader::CreateScene(fm_ctx* ctx, fm_scene** out) const
     return fm_scene_create(ctx, &d, out);
 }
 
-void apply_post_process(const std::vector<PostStep>& steps, std::vector<float>& rgb)
+std::vector<fm_post_step> post_steps(const std::vector<PostStep>& steps)
 {
-    // ToneMapping::Filmic (post/tonemapping.cpp:10-32)
-    auto filmic_core = [](float x) {
-        const float A = 0.22f, B = 0.30f, C = 0.10f, D = 0.20f, E = 0.01f, F = 0.30f;
-        return ((x * (A * x + C * B) + D * E) / (x * (A * x + B) + D * F)) - E / F;
-    };
+    std::vector<fm_post_step> out;
     for (const auto& s : steps) {
-        if (s.type == "tonemapping") {
-            const float white = filmic_core(11.2f);
-            for (auto& v : rgb) v = filmic_core(1.6f * v * s.lum) / white;
-        } else if (s.type == "linear_to_srgb") {
-            for (auto& v : rgb) v = linear_to_srgb(v);
-        } else if (s.type == "srgb_to_linear") {
-            for (auto& v : rgb) v = srgb_to_linear(v);
-        }
+        fm_post_step p{};
+        p.lum = s.lum;
+        if (s.type == "tonemapping")
+            p.type = FM_POST_TONEMAP;
+        else if (s.type == "linear_to_srgb")
+            p.type = FM_POST_LINEAR_TO_SRGB;
+        else if (s.type == "srgb_to_linear")
+            p.type = FM_POST_SRGB_TO_LINEAR;
+        else if (s.type == "oidn_denoise")
+            p.type = FM_POST_DENOISE;
+        else
+            continue;
+        out.push_back(p);
     }
+    return out;
 }
 
 fm_status SceneLoader::DrawFrame(fm_ctx* ctx)
@@ -775,10 +778,16 @@ fm_status SceneLoader::DrawFrame(fm_ctx* ctx)
     if (st != FM_OK) return st;
     std::fprintf(stderr, "[fumeng_b200] Current progress is : 1.00 (%lld paths in %.1f ms)\n", (long long)stats.paths,
                  stats.kernel_ms);
-    apply_post_process(m_post, rgb);
-    write_png(m_output + ".png", m_params.width, m_params.height, rgb.data());
-    write_png(m_output + "_albedo.png", m_params.width, m_params.height, alb.data());
-    write_png(m_output + "_normal.png", m_params.width, m_params.height, nrm.data());
+    // the post-process chain and the 8-bit conversion on the device (fm_postprocess),
+    // then RenderTarget::save_to_file's three PNG files
+    const std::vector<fm_post_step> steps = post_steps(m_post);
+    std::vector<uint8_t> c8(n), a8(n), n8(n);
+    st = fm_postprocess(ctx, m_params.width, m_params.height, steps.data(), (int32_t)steps.size(), rgb.data(),
+                        alb.data(), nrm.data(), c8.data(), a8.data(), n8.data(), 0);
+    if (st != FM_OK) return st;
+    write_png_u8(m_output + ".png", m_params.width, m_params.height, c8.data());
+    write_png_u8(m_output + "_albedo.png", m_params.width, m_params.height, a8.data());
+    write_png_u8(m_output + "_normal.png", m_params.width, m_params.height, n8.data());
     return FM_OK;
 }
 

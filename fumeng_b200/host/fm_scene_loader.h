@@ -112,6 +112,7 @@ private:
 };
 
 // Post-process chain on a float RGB image (post/tonemapping.cpp, post/*_srgb.cpp).
-void apply_post_process(const std::vector<PostStep>& steps, std::vector<float>& rgb);
+// The post-process chain as the C-ABI's steps (unknown types were dropped when parsed).
+std::vector<fm_post_step> post_steps(const std::vector<PostStep>& steps);
 
 }  // namespace fmhost

@@ -309,6 +309,36 @@ fm_status fm_draw_frame(fm_ctx* ctx, const char* json_path);
 fm_status fm_trace_closest_noalloc(fm_ctx* ctx, const fm_scene* scene, const float* rays, int64_t n,
                                    int32_t* obj_id, float* t);
 
+/* ---- post-processing ----------------------------------------------------------------- */
+enum {
+    FM_POST_TONEMAP = 0,         /* "tonemapping" (post/tonemapping.cpp), parameter lum */
+    FM_POST_LINEAR_TO_SRGB = 1,  /* "linear_to_srgb" (post/linear_to_srgb.cpp) */
+    FM_POST_SRGB_TO_LINEAR = 2,  /* "srgb_to_linear" (post/srgb_to_linear.cpp) */
+    FM_POST_DENOISE = 3          /* "oidn_denoise" (post/oidn_denoise.cpp): see fm_postprocess */
+};
+
+typedef struct {
+    int32_t type;
+    float lum;                   /* FM_POST_TONEMAP only */
+} fm_post_step;
+
+/* Replaces: the PostProcess chain Renderer::DrawFrame runs on the finished frame
+ * (core/renderer.h:131-135) and the 8-bit conversion of RenderTarget::save_to_file
+ * (render_target.h:26-31 -> Image::save_to_file, image/image.cpp:98-109, RealToUInt8
+ * core/utils.h:134-137).  Applies steps[0..num_steps) in order to rgb (width*height*3
+ * floats, updated in place) and writes round(255 * clamp(x, 0, 1)) of rgb, albedo and
+ * normal to the non-NULL 8-bit outputs (albedo and normal are not post-processed, as in
+ * the reference).  The per-pixel steps use the reference's float arithmetic, so the bytes
+ * equal the reference's float build's for the same input (the sRGB steps' pow may differ
+ * in its last bit, which can move a value sitting on a rounding boundary by one code).
+ * FM_POST_DENOISE needs albedo and normal: the reference calls Intel Open Image Denoise
+ * there, which is not available; this library runs an edge-avoiding a-trous wavelet
+ * filter guided by the same albedo and normal images instead (its output is not
+ * OIDN's).  At most 16 steps.  Host buffers unless FM_FLAG_DEVICE_PTRS. */
+fm_status fm_postprocess(fm_ctx* ctx, int32_t width, int32_t height, const fm_post_step* steps, int32_t num_steps,
+                         float* rgb, const float* albedo, const float* normal, uint8_t* rgb8, uint8_t* albedo8,
+                         uint8_t* normal8, int32_t flags);
+
 /* ---- differentiable rendering ------------------------------------------------------
  * The reference renders forward only; the two entry points below have no counterpart
  * in it. */

@@ -69,6 +69,8 @@ def lib(precision: str = "float") -> C.CDLL:
     L.fmref_env_radiance.argtypes = [vp, _D, C.c_int64, _D]
     L.fmref_env_sample.argtypes = [vp, _D, C.c_int64, _D]
     L.fmref_bsdf.argtypes = [vp, C.c_char_p, _D, C.c_int64, _D, _D, _D, _D, _D]
+    U8 = C.POINTER(C.c_uint8)
+    L.fmref_postprocess.argtypes = [C.POINTER(C.c_int), _D, C.c_int, C.c_int, C.c_int, _D, _D, _D, U8, U8, U8]
     _cache[precision] = L
     return L
 
@@ -264,3 +266,20 @@ def restate_closest_spheres(tri_pos: np.ndarray, centers: np.ndarray, radii: np.
                                      len(rad), r.ctypes.data_as(F), len(r), prim.ctypes.data_as(C.POINTER(C.c_int32)),
                                      t.ctypes.data_as(F))
     return prim, t
+
+
+def postprocess_u8(steps, rgb, albedo, normal, precision: str = "float"):
+    """The reference's post-process chain and 8-bit conversion (fmref_postprocess).
+    steps: [(type, lum)] with type 0 tonemapping, 1 linear_to_srgb, 2 srgb_to_linear.
+    Returns (rgb8, albedo8, normal8) as h x w x 3 uint8."""
+    L = lib(precision)
+    h, w, _ = rgb.shape
+    types = (C.c_int * max(1, len(steps)))(*[int(t) for t, _ in steps])
+    lums = np.asarray([float(l) for _, l in steps] or [0.0], np.float64)
+    a = [np.ascontiguousarray(x, np.float64) for x in (rgb, albedo, normal)]
+    outs = [np.empty((h, w, 3), np.uint8) for _ in range(3)]
+    U8 = C.POINTER(C.c_uint8)
+    if L.fmref_postprocess(types, _dp(lums), len(steps), w, h, _dp(a[0]), _dp(a[1]), _dp(a[2]),
+                           *[o.ctypes.data_as(U8) for o in outs]) != 0:
+        raise RuntimeError(L.fmref_last_error().decode())
+    return tuple(outs)

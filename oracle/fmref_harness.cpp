@@ -75,6 +75,7 @@
 #define private public
 #define protected public
 #include <engine/create/scene_loader.h>
+#include <engine/create/post_process.h>
 #include <renderer/path_tracing.cpp>
 #include <geometry/triangle.h>
 #include <engine/core/fresnel.h>
@@ -537,6 +538,51 @@ double fmref_draw_frame(void* h)
     s->loader.DrawFrame();
     const auto t1 = std::chrono::steady_clock::now();
     return std::chrono::duration<double>(t1 - t0).count();
+}
+
+// The reference's PostProcess chain (create/post_process.h: ToneMapping with its lum,
+// LinearToSrgb, SrgbToLinear) over a frame held in a RenderTarget, then the 8-bit values
+// RenderTarget::save_to_file writes (Image::save_to_file -> RealToUInt8 per channel, of
+// the colour, albedo and normal images; only the colour is post-processed).
+// types: 0 tonemapping, 1 linear_to_srgb, 2 srgb_to_linear.  Images: h x w x 3.
+int fmref_postprocess(const int* types, const double* lums, int nsteps, int w, int h, const double* rgb,
+                      const double* alb, const double* nrm, uint8_t* rgb8, uint8_t* alb8, uint8_t* nrm8)
+{
+    try {
+        fe::RenderTarget target;
+        target.resize(size_t(w), size_t(h));
+        const size_t npix = size_t(w) * size_t(h);
+        for (size_t i = 0; i < npix; ++i) {
+            target.m_color(i) = vec3(real(rgb[3 * i]), real(rgb[3 * i + 1]), real(rgb[3 * i + 2]));
+            target.m_albedo(i) = vec3(real(alb[3 * i]), real(alb[3 * i + 1]), real(alb[3 * i + 2]));
+            target.m_normal(i) = vec3(real(nrm[3 * i]), real(nrm[3 * i + 1]), real(nrm[3 * i + 2]));
+        }
+        for (int k = 0; k < nsteps; ++k) {
+            fe::SP<fe::PostProcess> step;
+            if (types[k] == 0) {
+                fe::ToneMappingConfig cfg;
+                cfg.lum = real(lums[k]);
+                step = fe::CreateToneMapping(cfg);
+            } else if (types[k] == 1) {
+                step = fe::CreateLinearToSrgb();
+            } else if (types[k] == 2) {
+                step = fe::CreateSrgbToLinear();
+            } else {
+                return 1;
+            }
+            step->Process(target);
+        }
+        for (size_t i = 0; i < npix; ++i)
+            for (int c = 0; c < 3; ++c) {
+                rgb8[3 * i + c] = fe::RealToUInt8(target.m_color(i)[c]);
+                alb8[3 * i + c] = fe::RealToUInt8(target.m_albedo(i)[c]);
+                nrm8[3 * i + c] = fe::RealToUInt8(target.m_normal(i)[c]);
+            }
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 1;
+    }
 }
 
 // Image::load_from_file (image.cpp:81-96) as the reference decodes textures and env maps.

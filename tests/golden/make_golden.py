@@ -3,7 +3,7 @@
 Run on a machine that has the reference sources (the oracle libraries are built from
 them by oracle/Makefile):
 
-    python tests/golden/make_golden.py [hit] [images] [adjoint] [batch] [single] [large] [inverse] [textured] [adjoint_texels] [digests] [force]
+    python tests/golden/make_golden.py [hit] [images] [adjoint] [batch] [single] [large] [inverse] [textured] [post] [adjoint_texels] [digests] [force]
 
 Scenes and rays are regenerated from seeds by fumeng_b200.synth, so each fixture stores
 only the reference's answers plus a SHA-256 of the inputs, which the tests recompute to
@@ -285,6 +285,49 @@ def make_textured():
     render_clamped_fixture(synth.textured_scene(), "textured", TEXTURED_SPP, TEXTURED_SEED, BATCH_CLAMP, aov=True)
 
 
+# ---- post-processing and the 8-bit conversion ----------------------------------------
+# A seeded 64x64 frame whose values cover what the chain meets: negative and zero,
+# [0, 4] uniform, 1e-6 .. 1e4 log-uniform, the sRGB breakpoints, the exact 8-bit codes
+# k / 255 and the rounding midpoints (k + 0.5) / 255 with their float neighbours; albedo
+# in [0, 1], normals in [-1, 1].  Chains as DrawFrame runs them (core/renderer.h:131-135).
+POST_CHAINS = [[(0, 1.0), (1, 0.0)], [(1, 0.0)], [(2, 0.0)], [(0, 0.35)], []]
+
+
+def post_inputs():
+    rng = np.random.default_rng(29)
+    n = 64 * 64 * 3
+    v = rng.uniform(0.0, 4.0, n)
+    k = rng.integers(0, n, n // 2)
+    v[k[: n // 8]] = -rng.uniform(0.0, 1.0, n // 8)
+    v[k[n // 8: n // 4]] = np.exp(rng.uniform(np.log(1e-6), np.log(1e4), n // 4 - n // 8))
+    codes = np.arange(256) / 255.0
+    mids = (np.arange(255) + 0.5) / 255.0
+    special = np.concatenate([[0.0, 1.0, 0.0031308, 0.04045], codes, mids,
+                              np.nextafter(mids.astype(np.float32), np.float32(2)),
+                              np.nextafter(mids.astype(np.float32), np.float32(-1))])
+    v[: len(special)] = special
+    rgb = v.astype(np.float32).reshape(64, 64, 3)
+    alb = rng.uniform(0.0, 1.0, (64, 64, 3)).astype(np.float32)
+    nrm = rng.uniform(-1.0, 1.0, (64, 64, 3)).astype(np.float32)
+    return rgb, alb, nrm
+
+
+def make_post():
+    rgb, alb, nrm = post_inputs()
+    out = {}
+    for i, chain in enumerate(POST_CHAINS):
+        c8, a8, n8 = fmref.postprocess_u8(chain, rgb.astype(np.float64), alb.astype(np.float64),
+                                         nrm.astype(np.float64), "float")
+        out[f"rgb8_{i}"] = c8
+        if i == 0:
+            out["albedo8"], out["normal8"] = a8, n8
+    h = hashlib.sha256()
+    for a in (rgb, alb, nrm):
+        h.update(a.tobytes())
+    np.savez_compressed(GOLDEN / "post_u8.npz", sha256=h.hexdigest(), **out)
+    print("post_u8", len(POST_CHAINS), "chains")
+
+
 # ---- texel gradients of the inverse-rendering configuration ---------------------------
 # 4x4-pixel tiles of the first view (256^2) on a 17x17 grid over the image centre, the
 # first 256 that see the mesh through their centre pixel.  For each tile, the texel seen through its centre pixel (the camera ray's nearest hit on the
@@ -527,6 +570,8 @@ if __name__ == "__main__":
         make_large_small()
     if "inverse" in what:
         make_inverse_tile()
+    if "post" in what:
+        make_post()
     if "textured" in what:
         make_textured()
     if "adjoint_texels" in what:

@@ -48,7 +48,8 @@ def test_struct_layouts_match_the_header(tmp_path):
                "fm_material_desc": fumeng_b200.MaterialDesc, "fm_light_desc": fumeng_b200.LightDesc,
                "fm_scene_desc": fumeng_b200.SceneDesc, "fm_camera": fumeng_b200.Camera,
                "fm_render_params": fumeng_b200.RenderParams, "fm_render_stats": fumeng_b200.RenderStats,
-               "fm_tuning": fumeng_b200.Tuning, "fm_grad_desc": fumeng_b200.GradDesc}
+               "fm_tuning": fumeng_b200.Tuning, "fm_grad_desc": fumeng_b200.GradDesc,
+               "fm_post_step": fumeng_b200.PostStep}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "fumeng_b200.h"', 'int main(void) {']
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
