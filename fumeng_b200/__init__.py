@@ -66,7 +66,7 @@ class SceneDesc(C.Structure):
                 ("num_spheres", C.c_int64), ("sphere_radius", _fp), ("sphere_xform", _fp), ("sphere_object", _ip),
                 ("num_materials", C.c_int32), ("materials", C.POINTER(MaterialDesc)),
                 ("num_textures", C.c_int32), ("textures", C.POINTER(TextureDesc)),
-                ("num_lights", C.c_int32), ("lights", C.POINTER(LightDesc))]
+                ("num_lights", C.c_int32), ("lights", C.POINTER(LightDesc)), ("tri_light_group", _ip)]
 
 
 class Camera(C.Structure):

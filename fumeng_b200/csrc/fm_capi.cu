@@ -68,6 +68,36 @@ void rotation_zyx(const float rot[3], Xf& l2w, Xf& w2l)
     }
 }
 
+// Vose's alias method (M. D. Vose, "A linear algorithm for generating random numbers with
+// a given distribution", IEEE TSE 1991) over non-negative weights: slot i keeps itself
+// with probability prob[i], else its alias.
+void vose_alias(const std::vector<double>& w, std::vector<float>& prob, std::vector<int32_t>& alias)
+{
+    const size_t n = w.size();
+    double sum = 0.0;
+    for (double x : w) sum += x;
+    std::vector<double> p(n);
+    std::vector<size_t> small, large;
+    for (size_t i = 0; i < n; ++i) {
+        p[i] = w[i] * (double)n / sum;
+        (p[i] < 1.0 ? small : large).push_back(i);
+    }
+    prob.assign(n, 1.0f);
+    alias.resize(n);
+    for (size_t i = 0; i < n; ++i) alias[i] = (int32_t)i;
+    while (!small.empty() && !large.empty()) {
+        const size_t s = small.back(), l = large.back();
+        small.pop_back();
+        prob[s] = (float)p[s];
+        alias[s] = (int32_t)l;
+        p[l] = (p[l] + p[s]) - 1.0;
+        if (p[l] < 1.0) {
+            large.pop_back();
+            small.push_back(l);
+        }
+    }
+}
+
 bool affine_inverse(const float m16[16], Xf& fwd, Xf& inv)
 {
     double A[9], t[3];
@@ -413,6 +443,9 @@ fm_status fm_scene_create(fm_ctx* ctx, const fm_scene_desc* d, fm_scene** out)
         // Aggregate::ConstructAreaLight, core/scene.h:21-25), then the given lights
         std::vector<DevLight> lights;
         std::vector<int32_t> obj_light((size_t)d->num_objects, -1);
+        // mesh lights: group id -> light index, and each mesh light's triangles
+        std::map<int32_t, int32_t> group_light;
+        std::vector<std::vector<int32_t>> mesh_tris;
         if (d->obj_emission) {
             for (int64_t o = 0; o < d->num_objects; ++o) {
                 const float* em = d->obj_emission + 3 * o;
@@ -421,14 +454,71 @@ fm_status fm_scene_create(fm_ctx* ctx, const fm_scene_desc* d, fm_scene** out)
                     st = set_error(ctx, FM_ERR_INVALID, "scene_create: an emissive object must have exactly one shape");
                     goto fail;
                 }
+                const int32_t group =
+                    geo_kind[o] == LK_AREA_TRI && d->tri_light_group ? d->tri_light_group[geo_index[o]] : -1;
+                if (group >= 0) {
+                    auto it = group_light.find(group);
+                    if (it != group_light.end()) {
+                        const DevLight& G = lights[it->second];
+                        if (G.radiance[0] != em[0] || G.radiance[1] != em[1] || G.radiance[2] != em[2]) {
+                            st = set_error(ctx, FM_ERR_INVALID, "scene_create: a mesh light's triangles differ in emission");
+                            goto fail;
+                        }
+                        mesh_tris[G.index].push_back(geo_index[o]);
+                        obj_light[o] = it->second;
+                        continue;
+                    }
+                }
                 DevLight L{};
-                L.kind = geo_kind[o];
+                L.kind = group >= 0 ? LK_AREA_MESH : geo_kind[o];
                 L.obj = (int32_t)o;
                 L.index = geo_index[o];
                 for (int k = 0; k < 3; ++k) L.radiance[k] = em[k];
+                if (group >= 0) {
+                    // index: the light's slot in mesh_tris until the tables are laid out
+                    L.index = (int32_t)mesh_tris.size();
+                    mesh_tris.push_back({geo_index[o]});
+                    group_light[group] = (int32_t)lights.size();
+                }
                 obj_light[o] = (int32_t)lights.size();
                 lights.push_back(L);
             }
+        }
+        if (!mesh_tris.empty()) {
+            // each mesh light's triangles, contiguous, with an alias table over their areas
+            std::vector<int32_t> mtri, malias;
+            std::vector<float> mprob;
+            for (auto& L : lights) {
+                if (L.kind != LK_AREA_MESH) continue;
+                const std::vector<int32_t>& tris = mesh_tris[L.index];
+                std::vector<double> area(tris.size());
+                double total = 0.0;
+                for (size_t k = 0; k < tris.size(); ++k) {
+                    const float* v = d->tri_pos + 9 * (size_t)tris[k];
+                    const double e1[3] = {(double)v[3] - v[0], (double)v[4] - v[1], (double)v[5] - v[2]};
+                    const double e2[3] = {(double)v[6] - v[0], (double)v[7] - v[1], (double)v[8] - v[2]};
+                    const double c[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                                         e1[0] * e2[1] - e1[1] * e2[0]};
+                    area[k] = 0.5 * std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+                    total += area[k];
+                }
+                if (!(total > 0.0)) {
+                    st = set_error(ctx, FM_ERR_INVALID, "scene_create: a mesh light has zero area");
+                    goto fail;
+                }
+                std::vector<float> prob;
+                std::vector<int32_t> alias;
+                vose_alias(area, prob, alias);
+                L.index = (int32_t)mtri.size();
+                L.count = (int32_t)tris.size();
+                L.inv_area = (float)(1.0 / total);
+                mtri.insert(mtri.end(), tris.begin(), tris.end());
+                mprob.insert(mprob.end(), prob.begin(), prob.end());
+                malias.insert(malias.end(), alias.begin(), alias.end());
+            }
+            FM_TRY(upload(ctx, sc, mtri.data(), mtri.size(), &S.mlight_tri));
+            FM_TRY(upload(ctx, sc, mprob.data(), mprob.size(), &S.mlight_prob));
+            FM_TRY(upload(ctx, sc, malias.data(), malias.size(), &S.mlight_alias));
         }
         S.env_light = -1;
         for (int32_t i = 0; i < d->num_lights; ++i) {

@@ -176,7 +176,16 @@ FM_D void area_geom_sample(const DevScene& S, const DevLight& L, f3 ref, f3 u, f
         pdf_area = 1.0f / R.area;
         return;
     }
-    const int t = L.index;
+    int t = L.index;
+    if (L.kind == LK_AREA_MESH) {
+        // TriangleEmbree::Sample (geometry/triangle_embree.cpp:253-260): a triangle by area
+        // with sample.z (alias table instead of the CDF search), a point on it with
+        // sample.xy, area pdf 1 / (total area)
+        const float x = u.z * (float)L.count;
+        int k = min((int)x, L.count - 1);
+        if (x - (float)k >= __ldg(S.mlight_prob + L.index + k)) k = __ldg(S.mlight_alias + L.index + k);
+        t = __ldg(S.mlight_tri + L.index + k);
+    }
     const float* v = S.tri_pos + 9 * (size_t)t;
     const f3 v0 = ld3(v), v1 = ld3(v + 3), v2 = ld3(v + 6);
     pos = b0 * v0 + b1 * v1 + b2 * v2;
@@ -186,7 +195,7 @@ FM_D void area_geom_sample(const DevScene& S, const DevLight& L, f3 ref, f3 u, f
     } else {
         n = normalize(cross(v0 - v2, v1 - v2));
     }
-    pdf_area = 1.0f / tri_area(v0, v1, v2);
+    pdf_area = L.kind == LK_AREA_MESH ? L.inv_area : 1.0f / tri_area(v0, v1, v2);
 }
 
 // Light::Sample at a shading position (area_light.cpp:16-26, directional_light.cpp:15-18,
@@ -237,6 +246,8 @@ FM_D float area_light_pdf(const DevScene& S, const DevLight& L, f3 shd, f3 lpos,
     } else if (L.kind == LK_AREA_TRI) {
         const float* v = S.tri_pos + 9 * (size_t)L.index;
         pa = 1.0f / tri_area(ld3(v), ld3(v + 3), ld3(v + 6));
+    } else if (L.kind == LK_AREA_MESH) {
+        pa = L.inv_area;   // TriangleEmbree::Pdf (triangle_embree.cpp:267-270)
     } else {
         const SphereDev& sp = S.spheres[L.index];
         const float dis = length(xf_point(sp.w2o, shd));

@@ -51,15 +51,17 @@ struct DevMaterial {
     float cond_eta2[3], cond_etak2[3];   // ConductorFresnel members (fresnel.h:77-84)
 };
 
-enum LightKind : int32_t { LK_AREA_TRI = 0, LK_AREA_RECT = 1, LK_AREA_SPHERE = 2, LK_DIR = 3, LK_ENV = 4 };
+enum LightKind : int32_t { LK_AREA_TRI = 0, LK_AREA_RECT = 1, LK_AREA_SPHERE = 2, LK_DIR = 3, LK_ENV = 4, LK_AREA_MESH = 5 };
 
 struct DevLight {
     int32_t kind;
-    int32_t obj;     // emissive object (area lights)
-    int32_t index;   // triangle / rect / sphere index (area lights)
-    int32_t pad;
+    int32_t obj;     // emissive object (area lights; mesh lights: the first triangle's object)
+    int32_t index;   // triangle / rect / sphere index (area lights); mesh lights: first entry
+                     // of the light's triangles in DevScene::mlight_tri
+    int32_t count;   // mesh lights: number of triangles
     float radiance[3];
     float direction[3];   // directional: light-to-scene direction
+    float inv_area;       // mesh lights: 1 / total area
 };
 
 struct DevEnv {
@@ -110,6 +112,11 @@ struct DevScene {
     const DevTexture* textures;
     const DevLight* lights;
     int32_t num_materials, num_textures, num_lights, env_light;   // env_light: index in lights or -1
+    // mesh lights: triangle indices of every mesh light (grouped, in object order) and an
+    // alias table over each light's triangle areas (acceptance, alias as a local index)
+    const int32_t* mlight_tri;
+    const float* mlight_prob;
+    const int32_t* mlight_alias;
     DevEnv env;
 };
 

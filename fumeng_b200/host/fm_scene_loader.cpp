@@ -276,6 +276,7 @@ fm_scene_desc FlatScene::desc() const
     d.textures = textures.data();
     d.num_lights = (int32_t)lights.size();
     d.lights = lights.data();
+    d.tri_light_group = mesh_lights ? tri_light_group.data() : nullptr;
     return d;
 }
 
@@ -579,6 +580,8 @@ void SceneLoader::ParseRenderObject(const Json& j)
         grow(F.tri_has_normal, nf);
         grow(F.tri_normal, 9 * nf);
         grow(F.tri_uv, 6 * nf);
+        if (F.mesh_lights) F.tri_light_group.insert(F.tri_light_group.end(), nf, F.num_meshes);
+        ++F.num_meshes;
         for (const auto& f : obj.faces) {
             const int32_t o = add_object();
             F.tri_object.push_back(o);
@@ -678,7 +681,11 @@ void SceneLoader::ParseScene(const Json& root)
     if (const Json* acc = c->find("accelerator")) {
         std::string t = "bvh";
         load(*acc, "type", t);
-        if (t == "embree") warn("accelerator 'embree': the device BVH is used");
+        if (t == "embree") {
+            warn("accelerator 'embree': the device BVH is used; each emissive mesh is one light sampled by area, "
+                 "as the reference's Embree meshes are");
+            m_flat.mesh_lights = true;
+        }
     }
     if (const Json* mats = c->find("materials"))
         for (const auto& m : mats->arr) ParseMaterial(m);

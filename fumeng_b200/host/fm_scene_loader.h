@@ -39,6 +39,11 @@ struct FlatScene {
     std::vector<std::vector<float>> texels;
     mutable std::vector<fm_texture_desc> textures;   // texel pointers are set by desc()
     std::vector<fm_light_desc> lights;
+    // "accelerator": "embree" -- each emissive mesh is one light sampled by area, as the
+    // reference's Embree meshes are; tri_light_group holds each triangle's mesh ordinal
+    bool mesh_lights = false;
+    std::vector<int32_t> tri_light_group;
+    int32_t num_meshes = 0;
 
     fm_scene_desc desc() const;
 };

@@ -196,6 +196,10 @@ class SceneSpec:
     # textures stored as 8-bit sRGB PNG files: their arrays hold the sRGB codes / 255, and
     # the scene decodes them to linear values as the reference's Image loader does
     ldr_textures: set = field(default_factory=set)
+    # "bvh" (the reference's built-in BVH: every emissive triangle is its own light) or
+    # "embree" (each emissive mesh is one light sampled by area, as the reference's Embree
+    # meshes; the device BVH serves both)
+    accelerator: str = "bvh"
 
     # -- derived ---------------------------------------------------------------------
     def material_index(self) -> dict:
@@ -281,7 +285,8 @@ class SceneSpec:
         cam = {k: v for k, v in self.camera.items()}
         ren = {"type": "path_tracer", "thread_count": 8, "output": output, **self.renderer}
         doc = {"camera": cam, "renderer": ren,
-               "scene": {"accelerator": {"type": "bvh"}, "materials": mats, "render_objects": objs, "lights": lights}}
+               "scene": {"accelerator": {"type": self.accelerator}, "materials": mats, "render_objects": objs,
+                         "lights": lights}}
         p = root / "scene.json"
         p.write_text(json.dumps(doc, indent=1))
         return p
@@ -369,6 +374,8 @@ class DescHolder:
         any_nrm = any(isinstance(o, Mesh) and o.normals is not None for o in spec.objects)
         vdim = max([o.vattr.shape[1] for o in spec.objects if isinstance(o, Mesh) and o.vattr is not None] or [0])
         has_nrm = []
+        light_group = []
+        n_mesh = 0
         obj = 0
         for o in spec.objects:
             em = list(o.emittance) if o.emittance is not None else [0.0, 0.0, 0.0]
@@ -378,6 +385,8 @@ class DescHolder:
                 f = np.asarray(o.faces, np.int64)
                 nf = len(f)
                 tri_pos.append(v[f].reshape(nf, 9))
+                light_group.append(np.full(nf, n_mesh, np.int32))
+                n_mesh += 1
                 if any_uv:
                     if o.uvs is not None:
                         uv = np.asarray(o.uvs, np.float32).copy()
@@ -537,5 +546,9 @@ class DescHolder:
         d.textures = self.textures
         d.num_lights = len(spec.lights)
         d.lights = self.lights
+        # "embree": one light per emissive mesh (its triangles share the mesh's ordinal)
+        self.tri_light_group = (np.ascontiguousarray(np.concatenate(light_group), np.int32)
+                                if spec.accelerator == "embree" and light_group else None)
+        d.tri_light_group = self.tri_light_group.ctypes.data_as(ip) if self.tri_light_group is not None else None
         self.desc = d
         self._keep = keep

@@ -325,6 +325,36 @@ def textured_scene(res: int = 48, spp: int = 16, depth: int = 5) -> SceneSpec:
     return SceneSpec(cam, ren, mats, objs, lights, tex, ldr_textures={"checker", "rm", "stripes"})
 
 
+def emitters_scene(res: int = 32, spp: int = 16, depth: int = 5, accelerator: str = "bvh") -> SceneSpec:
+    """Emissive meshes and an emissive sphere as the only lights: a displaced icosphere of
+    20 triangles and a box of 12 triangles, each emitting as a whole, and an analytic
+    sphere light (cone sampling from outside, sphere.cpp:143-193), over a Lambert floor
+    and back wall with a Disney icosphere and a Lambert box.  accelerator "bvh" makes every
+    emissive triangle its own light (the reference's built-in path), "embree" one light
+    per emissive mesh sampled by area (the reference's Embree meshes)."""
+    v0, f0 = displaced_icosphere(0, 51, amp=0.05)
+    lamp = (v0 * 0.25 + np.array([-0.9, 0.4, 1.6])).astype(np.float32)
+    bv, bf = subdivided_box(1)
+    box_lamp = (bv * np.array([0.3, 0.15, 0.05]) + np.array([0.7, 0.6, 1.9])).astype(np.float32)
+    dv, df = displaced_icosphere(2, 52)
+    disney = (dv * 0.45 + np.array([0.1, -0.1, 0.45])).astype(np.float32)
+    cv, cf = subdivided_box(2)
+    cube = (cv * 0.25 + np.array([-0.7, -0.6, 0.25])).astype(np.float32)
+    objs = [Rect((-2, -2, 0), (2, -2, 0), (2, 2, 0), (-2, 2, 0), "floor"),
+            Rect((-2, 1.5, 0), (-2, 1.5, 3), (2, 1.5, 3), (2, 1.5, 0), "floor"),
+            Mesh(disney, df, "disney"), Mesh(cube, cf, "floor"),
+            Mesh(lamp, f0, "floor", emittance=(6.0, 5.0, 3.0)),
+            Mesh(box_lamp, bf, "floor", emittance=(9.0, 9.0, 12.0)),
+            Sphere(0.12, translation=(0.9, -0.8, 1.3), material="floor", emittance=(20.0, 14.0, 10.0))]
+    mats = [{"name": "floor", "type": "lambert_diffuse", "basecolor": [0.6, 0.55, 0.5]},
+            {"name": "disney", "type": "disney", "basecolor": [0.7, 0.3, 0.2], "roughness": 0.35, "metallic": 0.4,
+             "specular": 0.5, "clearcoat": 0.5}]
+    cam = {"type": "pin_hole", "pos": [0.2, -3.8, 1.6], "look_at": [0.0, 0.2, 0.6], "up": [0, 0, 1], "fov": 50.0,
+           "aspect": 1.0}
+    ren = {"width": res, "height": res, "spp": spp, "depth": depth, "rr_depth": 3, "rr_coef": 0.85}
+    return SceneSpec(cam, ren, mats, objs, [], {}, accelerator=accelerator)
+
+
 def material_scene(seed: int, res: int = 64, env_w: int = 128, env_h: int = 64, spp: int = 16, depth: int = 6) -> SceneSpec:
     """Small scene exercising every BSDF and light kind: Disney icosphere (specTrans 0),
     Disney clearcoat sphere, dielectric sphere, conductor sphere, Lambert floor, a

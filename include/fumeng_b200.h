@@ -145,6 +145,17 @@ typedef struct {
     const fm_texture_desc* textures;
     int32_t num_lights;            /* JSON lights, appended after area lights */
     const fm_light_desc* lights;
+
+    /* Extension: mesh lights.  NULL, or [num_triangles] group ids: the emissive triangles
+     * that share a group id >= 0 form ONE area light, sampled by picking a triangle in
+     * proportion to its area and a point on it (area pdf 1 / total area), as the
+     * reference's Embree meshes do (geometry/triangle_embree.cpp:119-130, 253-270) --
+     * one light sample per mesh per bounce instead of one per triangle.  The light takes
+     * the place of the group's first triangle in the light list; every triangle of a
+     * group must have the same emission.  Object indices (hit IDs) are unchanged.
+     * Triangles with group -1 stay one light each (the built-in BVH path,
+     * core/render_object.h:29-32). */
+    const int32_t* tri_light_group;
 } fm_scene_desc;
 
 /* ---- camera and render parameters ---------------------------------------------- */

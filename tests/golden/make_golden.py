@@ -3,7 +3,7 @@
 Run on a machine that has the reference sources (the oracle libraries are built from
 them by oracle/Makefile):
 
-    python tests/golden/make_golden.py [hit] [images] [adjoint] [batch] [single] [large] [inverse] [textured] [post] [adjoint_texels] [digests] [force]
+    python tests/golden/make_golden.py [hit] [images] [adjoint] [batch] [single] [large] [inverse] [textured] [emitters] [post] [adjoint_texels] [digests] [force]
 
 Scenes and rays are regenerated from seeds by fumeng_b200.synth, so each fixture stores
 only the reference's answers plus a SHA-256 of the inputs, which the tests recompute to
@@ -285,6 +285,18 @@ def make_textured():
     render_clamped_fixture(synth.textured_scene(), "textured", TEXTURED_SPP, TEXTURED_SEED, BATCH_CLAMP, aov=True)
 
 
+# Emissive meshes and an emissive sphere as the only lights (synth.emitters_scene), full
+# 32x32 frame, double build with the built-in BVH (one light per emissive triangle),
+# 16384 spp, plain and clamped sums.
+EMITTERS_SPP, EMITTERS_SEED = 16384, 37
+
+
+def make_emitters():
+    if (GOLDEN / "emitters.npz").exists():
+        return
+    render_clamped_fixture(synth.emitters_scene(), "emitters", EMITTERS_SPP, EMITTERS_SEED, BATCH_CLAMP)
+
+
 # ---- post-processing and the 8-bit conversion ----------------------------------------
 # A seeded 64x64 frame whose values cover what the chain meets: negative and zero,
 # [0, 4] uniform, 1e-6 .. 1e4 log-uniform, the sRGB breakpoints, the exact 8-bit codes
@@ -469,6 +481,8 @@ def scene_digest(spec) -> str:
     h = hashlib.sha256()
     h.update(_json.dumps([spec.camera, spec.renderer, spec.materials, spec.lights], sort_keys=True,
                          default=float).encode())
+    if getattr(spec, "accelerator", "bvh") != "bvh":
+        h.update(spec.accelerator.encode())
     for o in spec.objects:
         if isinstance(o, Mesh):
             h.update(np.ascontiguousarray(o.vertices, np.float32).tobytes())
@@ -492,7 +506,7 @@ def image_fixture_scenes():
     out = [(name, builder) for name, builder, _, _, _ in IMAGE_CASES]
     out += [(f"batch_s{s}", (lambda s=s: synth.batch_scene(s))) for s in BATCH_CASES]
     out += [("single", single_scene), ("large_small", large_small_scene), ("inverse_t0", inverse_target_scene),
-            ("textured", synth.textured_scene)]
+            ("textured", synth.textured_scene), ("emitters", synth.emitters_scene)]
     return out
 
 
@@ -570,6 +584,8 @@ if __name__ == "__main__":
         make_large_small()
     if "inverse" in what:
         make_inverse_tile()
+    if "emitters" in what:
+        make_emitters()
     if "post" in what:
         make_post()
     if "textured" in what:

@@ -307,3 +307,37 @@ def test_textured_scene_through_loader_matches_reference(ctx, mode, tmp_path):
     mad = float(np.mean(np.abs(out[0.0][1] - g["albedo"])))
     log_result({"case": "textured", "mode": mode_name(mode), "albedo_mad": mad})
     assert mad < 5e-3, mad
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", [fb.FM_MODE_MEGAKERNEL, fb.FM_MODE_WAVEFRONT], ids=["megakernel", "wavefront"])
+def test_emissive_meshes_and_sphere_light_match_reference(ctx, mode):
+    """Emissive meshes (20 and 12 triangles) and an analytic sphere light as the only
+    lights, 32x32, against the reference's double build with its built-in BVH
+    (tests/golden/emitters.npz, 16384 spp): with one light per emissive triangle, as the
+    reference, clamped (strict) and plain; and with one light per emissive mesh sampled
+    by area (accelerator "embree", the reference's Embree meshes), whose estimator differs
+    but whose expectation is the same, plain and strict."""
+    path = GOLDEN_DIR / "emitters.npz"
+    if not path.exists():
+        pytest.skip("no emitters fixture (tests/golden/make_golden.py emitters)")
+    g = np.load(path)
+    spec = synth.emitters_scene()
+    full = (0, 0, int(spec.renderer["width"]), int(spec.renderer["height"]))
+    plain = render_tiles(ctx, [spec], [full], mode, 0.0, CLAMP_BATCHES, CLAMP_SPP)[0]
+    clamped = render_tiles(ctx, [spec], [full], mode, BATCH_CLAMP, CLAMP_BATCHES, CLAMP_SPP)[0]
+    check_clamped_fixture(plain, clamped, g, "emitters", mode)
+    mesh = synth.emitters_scene(accelerator="embree")
+    holder = mesh.to_desc()
+    sc = ctx.create_scene(holder)
+    try:
+        info = sc.info()
+        # 2 mesh lights + 1 sphere light instead of 32 + 1
+        assert info["lights"] == 3, info
+    finally:
+        sc.destroy()
+    per_mesh = render_tiles(ctx, [mesh], [full], mode, 0.0, CLAMP_BATCHES, CLAMP_SPP)[0]
+    res = compare(per_mesh, g, "mean", "var")
+    res.update(case="emitters_mesh_lights", mode=mode_name(mode), estimator="plain")
+    log_result(res)
+    assert_parity_strict(res)
