@@ -92,6 +92,9 @@ struct WfState {
     float4* sh_o;
     float4* sh_d;
     float4* sh_c;
+    float4* cont_h;       // trace results in continuation-queue order: hit (t, prim, b1, b2)
+    int32_t* cont_v;      // ... and the ray's view, so that hit resolution starts from
+                          // coalesced loads instead of the slot indirection
     float4* mis_h;        // trace results: MIS ray hits (t, prim, b1, b2)
     uint32_t* sh_h;       // ... shadow ray occluded (1) or not (0)
     int64_t cap_cont, cap_mis, cap_sh;
@@ -435,11 +438,13 @@ FM_D unsigned long long global_ns()
 constexpr int kRayCont = 0, kRayMis = 1, kRayShadow = 2;
 
 // Sets up the traversal of ray `idx` of the combined index space.
-FM_D int begin_ray(const WfState& st, int64_t idx, int64_t nc, int64_t nm, Traversal& t, const DevScene*& Sp)
+FM_D int begin_ray(const WfState& st, int64_t idx, int64_t nc, int64_t nm, Traversal& t, const DevScene*& Sp,
+                   int& vid)
 {
     if (idx < nc) {
         const int slot = st.cont_q[idx];
-        Sp = st.views[st.view[slot]].scene;
+        vid = st.view[slot];
+        Sp = st.views[vid].scene;
         const float4 o4 = st.ro[slot], d4 = st.rd[slot];
         trav_begin(t, trace_scene(*Sp), f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, 0.0f, kRealMax, false);
         return kRayCont;
@@ -622,6 +627,7 @@ __global__ void __launch_bounds__(256, 4) k_wf_trace(WfState st)
     stack.stride = blockDim.x;
     Traversal t;
     const DevScene* Sp = nullptr;
+    int vid = 0;
     int kind = -1;   // ray kind held by this lane, -1 for none
     int64_t idx = 0;
     bool exhausted = false;
@@ -640,14 +646,16 @@ __global__ void __launch_bounds__(256, 4) k_wf_trace(WfState st)
                 if (idx >= total)
                     exhausted = true;
                 else
-                    kind = begin_ray(st, idx, nc, nm, t, Sp);
+                    kind = begin_ray(st, idx, nc, nm, t, Sp, vid);
             }
         }
         if (__ballot_sync(0xffffffffu, kind >= 0) == 0) break;
         if (kind >= 0 && trav_step(t, trace_scene(*Sp), stack, st.status)) {
             const Hit& h = t.hit;
-            if (kind == kRayCont)
-                st.hit[st.cont_q[idx]] = make_float4(h.t, __int_as_float(h.prim), h.b1, h.b2);
+            if (kind == kRayCont) {
+                st.cont_h[idx] = make_float4(h.t, __int_as_float(h.prim), h.b1, h.b2);
+                st.cont_v[idx] = vid;
+            }
             else if (kind == kRayMis)
                 st.mis_h[idx - nc] = make_float4(h.t, __int_as_float(h.prim), h.b1, h.b2);
             else
@@ -675,9 +683,10 @@ __global__ void __launch_bounds__(256) k_wf_resolve(WfState st)
         if (i < nc) {
             ++n_closest;
             const int slot = st.cont_q[i];
-            const float4 h4 = st.hit[slot];
-            finish_cont<ADJ>(st, i, *st.views[st.view[slot]].scene,
-                             Hit{h4.x, __float_as_int(h4.y), h4.z, h4.w});
+            const float4 h4 = st.cont_h[i];
+            const int vid = st.cont_v[i];
+            st.hit[slot] = h4;   // the shading kernels read it by slot
+            finish_cont<ADJ>(st, i, *st.views[vid].scene, Hit{h4.x, __float_as_int(h4.y), h4.z, h4.w});
         } else if (i < nc + nm) {
             ++n_closest;
             const int64_t q = i - nc;
@@ -1350,6 +1359,8 @@ fm_status wf_cache_reserve(fm_ctx* ctx, bool adj, int64_t pool, int64_t cap_mis,
         A(b.asum, pool);
         A(b.nsum, pool);
         A(b.cont_q, pool);
+        A(b.cont_h, pool);
+        A(b.cont_v, pool);
         A(b.disney_q, pool);
         A(b.simple_q, pool);
         A(b.mis_o, cap_mis);
