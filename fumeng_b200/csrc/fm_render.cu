@@ -50,7 +50,7 @@ FM_D void add_counters(Counters* cnt, unsigned long long paths, unsigned long lo
 // item writes its Kahan-compensated colour sum and its albedo / normal sums once; the
 // per-pixel reduction (reduce_views) adds the chunks in order, so the image does not
 // depend on which thread ran which item.
-__global__ void __launch_bounds__(128) k_megakernel(const WfView* __restrict__ views, int nviews, int64_t total_items,
+__global__ void __launch_bounds__(128, 4) k_megakernel(const WfView* __restrict__ views, int nviews, int64_t total_items,
                                                     unsigned long long* next, Counters* cnt, uint32_t* status)
 {
     unsigned long long np = 0, nc = 0, ns = 0, nb = 0, nn = 0;

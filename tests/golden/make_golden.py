@@ -292,9 +292,21 @@ EMITTERS_SPP, EMITTERS_SEED = 16384, 37
 
 
 def make_emitters():
-    if (GOLDEN / "emitters.npz").exists():
+    """Double build (mean / var, plain and clamped) and the reference's float build
+    (f_mean / f_var) of the same scene."""
+    if not (GOLDEN / "emitters.npz").exists():
+        render_clamped_fixture(synth.emitters_scene(), "emitters", EMITTERS_SPP, EMITTERS_SEED, BATCH_CLAMP)
+    g = dict(np.load(GOLDEN / "emitters.npz"))
+    if "f_mean" in g:
         return
-    render_clamped_fixture(synth.emitters_scene(), "emitters", EMITTERS_SPP, EMITTERS_SEED, BATCH_CLAMP)
+    with tempfile.TemporaryDirectory() as d:
+        rs = fmref.RefScene(synth.emitters_scene().write(Path(d)), "float")
+        r = rs.render(EMITTERS_SPP, seed=EMITTERS_SEED + 1)
+        rs.close()
+    g["f_mean"], g["f_var"] = moments(r, "sum", EMITTERS_SPP)
+    g["f_spp"] = EMITTERS_SPP
+    np.savez_compressed(GOLDEN / "emitters.npz", **g)
+    print("emitters float build", g["f_mean"].mean(axis=(0, 1)), flush=True)
 
 
 # ---- post-processing and the 8-bit conversion ----------------------------------------
@@ -470,7 +482,7 @@ def make_adjoint_texels():
                 L.append(float((w.astype(np.float64) * r["sum"] / spp).sum()))
             spec.textures[tex] = orig
             fd[ci, si] = (L[0] - L[1]) / (2 * h)
-        print("c3 texel fd", k, tex, (ty, tx, ch), fd[ci].mean(), fd[ci].std(ddof=1) / 2, flush=True)
+        print("c3 texel fd", k, tex, (ty, tx, ch), fd[ci].mean(), fd[ci].std(ddof=1) / np.sqrt(fd.shape[1]), flush=True)
     np.savez_compressed(GOLDEN / "adj_fd_texels_ref.npz", fd=fd, spp=spp, seeds=np.asarray(C3_REF["seeds"]),
                         case_index=np.asarray([c[0] for c in cases]), h=np.asarray([c[5] for c in cases]))
 
