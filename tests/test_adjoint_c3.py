@@ -21,6 +21,8 @@ perturbation survives the .hdr file exactly (tests/golden/adj_fd_texels_ref.npz)
 the adjoint, max(2e-2 |FD|, 4 standard errors) (the reference's CPU time limits its
 sample count).
 """
+import json
+import os
 from pathlib import Path
 
 import numpy as np
@@ -93,6 +95,11 @@ def test_texel_gradients_match_central_differences_at_one_percent(c3):
         if abs(a - f) > tol:
             fails.append((k, tex, texel, a, sa, f, sf))
     med = float(np.median(rel))
+    if os.environ.get("FUMENG_B200_PARITY_LOG"):
+        with open(os.environ["FUMENG_B200_PARITY_LOG"], "a") as fh:
+            fh.write(json.dumps({"case": "c3_texel_gradients", "cases": len(cases), "median_rel_err": med,
+                                 "p90_rel_err": float(np.percentile(rel, 90)), "bound_1e-2_binds": int(powered),
+                                 "outside_tolerance": len(fails)}) + "\n")
     print(f"c3 texels: median |adjoint - FD| / |FD| = {med:.2e}, 90th percentile {np.percentile(rel, 90):.2e}, "
           f"cases where the 1e-2 bound binds: {powered}/{len(cases)}")
     assert not fails, f"{len(fails)} of {len(cases)} cases outside tolerance: {fails[:5]}"
@@ -111,4 +118,8 @@ def test_texel_gradients_match_reference_double_fd(c3):
         f, sf = _sem(g["fd"][ci])
         tol = max(2e-2 * abs(f), 4.0 * np.hypot(sa, sf))
         print(f"reference FD case {int(k)} {tex}{texel}: adjoint {a:.5g} +- {sa:.2g}, reference {f:.5g} +- {sf:.2g}")
+        if os.environ.get("FUMENG_B200_PARITY_LOG"):
+            with open(os.environ["FUMENG_B200_PARITY_LOG"], "a") as fh:
+                fh.write(json.dumps({"case": f"c3_reference_fd_{int(k)}", "adjoint": a, "adjoint_se": sa,
+                                     "reference_fd": f, "reference_fd_se": sf}) + "\n")
         assert abs(a - f) <= tol, f"case {k} {tex}{texel}: adjoint {a:.6g} +- {sa:.2g} vs reference FD {f:.6g} +- {sf:.2g}"
