@@ -72,20 +72,25 @@ FM_D void intersect_node(const uint4* __restrict__ nodes, int node, f3 o, f3 idi
     const float bz = (pz - o.z) * idir.z;
     uint32_t nbits = 0, pbits = 0;
     const float tfar_limit = tmax;
+    // Near and far planes per axis chosen once per node from the ray's direction signs
+    // (t = q a + b grows with q when a = 2^e / d >= 0), so the per-child slab test needs
+    // no min / max to order the two planes.  Equal to min / max of the two plane
+    // distances, so the results do not change.
+    const bool sx = idir.x >= 0.0f, sy = idir.y >= 0.0f, sz = idir.z >= 0.0f;
+    const uint32_t nx0 = sx ? w2.x : w3.z, nx1 = sx ? w2.y : w3.w, fx0 = sx ? w3.z : w2.x, fx1 = sx ? w3.w : w2.y;
+    const uint32_t ny0 = sy ? w2.z : w4.x, ny1 = sy ? w2.w : w4.y, fy0 = sy ? w4.x : w2.z, fy1 = sy ? w4.y : w2.w;
+    const uint32_t nz0 = sz ? w3.x : w4.z, nz1 = sz ? w3.y : w4.w, fz0 = sz ? w4.z : w3.x, fz1 = sz ? w4.w : w3.y;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         const uint32_t wm = i < 4 ? w1.z : w1.w;
         const uint32_t meta = (wm >> (8 * (i & 3))) & 0xffu;
         if (meta == 0) continue;
         const int k = i & 3;
-        const float qlx = byte_f(i < 4 ? w2.x : w2.y, k), qly = byte_f(i < 4 ? w2.z : w2.w, k);
-        const float qlz = byte_f(i < 4 ? w3.x : w3.y, k), qhx = byte_f(i < 4 ? w3.z : w3.w, k);
-        const float qhy = byte_f(i < 4 ? w4.x : w4.y, k), qhz = byte_f(i < 4 ? w4.z : w4.w, k);
-        const float tx0 = fmaf(qlx, ax, bx), tx1 = fmaf(qhx, ax, bx);
-        const float ty0 = fmaf(qly, ay, by), ty1 = fmaf(qhy, ay, by);
-        const float tz0 = fmaf(qlz, az, bz), tz1 = fmaf(qhz, az, bz);
-        const float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
-        const float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tfar_limit));
+        const float txn = fmaf(byte_f(i < 4 ? nx0 : nx1, k), ax, bx), txf = fmaf(byte_f(i < 4 ? fx0 : fx1, k), ax, bx);
+        const float tyn = fmaf(byte_f(i < 4 ? ny0 : ny1, k), ay, by), tyf = fmaf(byte_f(i < 4 ? fy0 : fy1, k), ay, by);
+        const float tzn = fmaf(byte_f(i < 4 ? nz0 : nz1, k), az, bz), tzf = fmaf(byte_f(i < 4 ? fz0 : fz1, k), az, bz);
+        const float tn = fmaxf(fmaxf(txn, tyn), fmaxf(tzn, tmin));
+        const float tf = fminf(fminf(txf, tyf), fminf(tzf, tfar_limit));
         // Widen the interval by a few ulps so that rounding in the slab arithmetic can
         // never reject a box that the exact box test accepts.
         if (tn <= tf * 1.0000010f + 1e-30f) {
