@@ -17,8 +17,8 @@ roofline: the trace kernel's algorithmic bytes (fixed per-ray formula, live ray 
          inside the kernel (earliest block start to latest block end of each launch;
          the render runs as one conditional CUDA graph, which admits no event nodes).
 e2e    : the same metric through the C-ABI from host memory: every step creates the 64
-         scenes from host descriptors (upload + device BVH build + env tables), renders
-         into host images and destroys the scenes.
+         scenes from host descriptors in one fm_scene_create_batch call (upload + device
+         BVH builds + env tables), renders into host images and destroys the scenes.
 The plain per-pixel megakernel is timed on the same batch for comparison, and the
 path-replay adjoint against its own forward pass on the inverse-rendering workload
 (fumeng_b200.synth.inverse_scene: 120k triangles, 512^2 basecolor and roughness /
@@ -512,7 +512,7 @@ def main():
         d2h = sum(p.width * p.height * 3 * 4 for p in params_wf)
 
         def step_e2e():
-            sc = [ctx.create_scene(h) for h in holders]
+            sc = ctx.create_scenes(holders)
             ctx.render_batch(sc, cams, params_wf, tuning=tuning)
             for s in sc:
                 s.destroy()

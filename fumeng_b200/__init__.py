@@ -142,6 +142,7 @@ def load_library() -> C.CDLL:
         "fm_ctx_destroy": ([vp], None),
         "fm_last_error": ([vp], C.c_char_p),
         "fm_scene_create": ([vp, C.POINTER(SceneDesc), C.POINTER(vp)], C.c_int),
+        "fm_scene_create_batch": ([vp, C.c_int32, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(vp)], C.c_int),
         "fm_scene_destroy": ([vp, vp], C.c_int),
         "fm_scene_bvh_stats": ([vp, vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32),
                                 C.POINTER(C.c_double)], C.c_int),
@@ -173,7 +174,8 @@ def load_library() -> C.CDLL:
     return lib
 
 
-EXPORTED_SYMBOLS = ["fm_ctx_create", "fm_ctx_destroy", "fm_last_error", "fm_scene_create", "fm_scene_destroy",
+EXPORTED_SYMBOLS = ["fm_ctx_create", "fm_ctx_destroy", "fm_last_error", "fm_scene_create", "fm_scene_create_batch",
+                    "fm_scene_destroy",
                     "fm_scene_bvh_stats", "fm_trace_closest", "fm_trace_any", "fm_render", "fm_render_batch",
                     "fm_autotune_batch", "fm_scene_load", "fm_draw_frame", "fm_trace_closest_noalloc",
                     "fm_scene_update_texture", "fm_render_adjoint", "fm_scene_info", "fm_postprocess"]
@@ -286,6 +288,14 @@ class Context:
         h = C.c_void_p()
         self.check(self.lib.fm_scene_create(self.h, C.byref(desc_holder.desc), C.byref(h)))
         return Scene(self, h, desc_holder)
+
+    def create_scenes(self, desc_holders) -> list:
+        """All scenes in one fm_scene_create_batch call (uploads and BVH builds overlapped)."""
+        n = len(desc_holders)
+        descs = (C.POINTER(SceneDesc) * n)(*[C.pointer(h.desc) for h in desc_holders])
+        hs = (C.c_void_p * n)()
+        self.check(self.lib.fm_scene_create_batch(self.h, n, descs, hs))
+        return [Scene(self, C.c_void_p(hs[i]), desc_holders[i]) for i in range(n)]
 
 
 class Scene:

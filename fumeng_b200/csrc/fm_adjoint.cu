@@ -7,15 +7,7 @@
 
 namespace fm {
 
-fm_status env_build_tables(fm_ctx* ctx, fm_scene* scene, const DevTexture& tex, DevEnv& env);
-
 namespace {
-
-__global__ void k_rgb_to_texels(const float* __restrict__ src, float4* __restrict__ dst, size_t n)
-{
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        dst[i] = make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0f);
-}
 
 // out[i] += sum over the copies of acc (FP64 sums of the FP32 accumulators).
 __global__ void k_grad_reduce(const float* __restrict__ acc, int copies, size_t n, double* __restrict__ out)
@@ -84,13 +76,12 @@ extern "C" fm_status fm_scene_update_texture(fm_ctx* ctx, fm_scene* scene, int32
                         "update_texture h2d");
             src = staged;
         }
-        const int grid = (int)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 16);
-        k_rgb_to_texels<<<grid, 256, 0, s>>>(src, const_cast<float4*>(t.texels), n);
+        launch_rgb_to_texels(s, src, const_cast<float4*>(t.texels), n, ctx->num_sms);
         FM_CUDA_TRY(ctx, cudaGetLastError(), "update_texture");
     }
     if (scene->dev.env_light >= 0 && scene->dev.env.tex == texture) {
         // the environment's importance tables follow its texels (rebuilt in place)
-        const fm_status st = env_build_tables(ctx, scene, t, scene->dev.env);
+        const fm_status st = env_build_tables(ctx, s, scene, t, scene->dev.env);
         if (st != FM_OK) return st;
     }
     FM_CUDA_TRY(ctx, cudaStreamSynchronize(s), "update_texture");

@@ -15,6 +15,7 @@
 #include "fm_bvh_build.h"
 
 #include <algorithm>
+#include <new>
 #include <vector>
 
 namespace fm {
@@ -91,6 +92,14 @@ __global__ void k_init_bins(Bins* bins, const int32_t* ntasks_p)
             w[i] = v;
         }
     }
+}
+
+// Root-bounds accumulator before k_root_bounds: minima at +inf bits, maxima at 0
+// (orderable-uint encoding of the bounds).
+__global__ void k_init_root_bounds(uint32_t* rb)
+{
+    const int i = threadIdx.x;
+    if (i < 12) rb[i] = (i % 6) < 3 ? 0xffffffffu : 0u;
 }
 
 __global__ void k_root_bounds(const float4* __restrict__ plo, const float4* __restrict__ phi, int n, uint32_t* out)
@@ -1103,6 +1112,9 @@ cudaError_t build_graph(cudaStream_t s, const BuildBufs& b, cudaGraph_t& graph)
     cudaGraphNode_t n_pre = nullptr, n_split = nullptr, n_mid = nullptr, n_collapse = nullptr, n_post = nullptr;
     cudaGraphConditionalHandle h_split{}, h_collapse{};
     e = add_captured(graph, nullptr, s, n_pre, [&]() {
+        k_init_root_bounds<<<1, 32, 0, s>>>(b.rb);
+        cudaMemsetAsync(b.counters, 0, sizeof(int32_t) * 16, s);
+        cudaMemsetAsync(b.leaf_prim, 0xff, sizeof(int32_t) * n, s);
         k_prim_bounds<<<grid_for(n, 256), 256, 0, s>>>(b.src, b.plo, b.phi);
         k_root_bounds<<<grid_for(n, 256), 256, 0, s>>>(b.plo, b.phi, n, b.rb);
         k_make_root<<<1, 1, 0, s>>>(b.rb, n, b.bnodes, b.tasks, b.pos_task, b.small_list, b.counters);
@@ -1132,32 +1144,76 @@ cudaError_t build_graph(cudaStream_t s, const BuildBufs& b, cudaGraph_t& graph)
     });
 }
 
+// Releases the build's temporaries (stream-ordered) and its graph.
+void free_temporaries(cudaStream_t s, BuildBufs& b)
+{
+    void* bufs[] = {b.plo,   b.phi,      b.pidx,  b.pidx2, b.pos_task, b.pos_task2, b.flags,
+                    b.scan,  b.tile_sums, b.small_list, b.counters, b.rb, b.bnodes, b.tasks,
+                    b.tasks2, b.splits,  b.bins,  b.front, b.front2,  b.leaf_prim};
+    for (void* p : bufs)
+        if (p) cudaFreeAsync(p, s);
+}
+
 }  // namespace
 
-int bvh_build(cudaStream_t stream, const PrimSource& src, BvhResult& out, std::string& err)
-{
-    const int n = src.num_tris + 2 * src.num_rects + src.num_spheres;
-    out = BvhResult{};
-    if (n == 0) return 0;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+// A build in flight: its buffers, graph and the events around it.
+struct BvhJob {
+    BuildBufs b{};
+    cudaStream_t stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    BuildBufs b{};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    const int32_t* h_cnt = nullptr;
+};
+
+namespace {
+
+// Drops a job: waits for its stream (on failure paths only), then frees everything,
+// including the result arrays when `free_out`.
+void drop_job(BvhJob* job, BvhResult& out, bool free_out)
+{
+    cudaGetLastError();
+    cudaStreamSynchronize(job->stream);
+    if (job->exec) cudaGraphExecDestroy(job->exec);
+    if (job->graph) cudaGraphDestroy(job->graph);
+    free_temporaries(job->stream, job->b);
+    if (free_out) {
+        if (out.nodes) cudaFreeAsync(out.nodes, job->stream);
+        if (out.leaf) cudaFreeAsync(out.leaf, job->stream);
+        cudaStreamSynchronize(job->stream);
+        out = BvhResult{};
+    }
+    if (job->ev0) cudaEventDestroy(job->ev0);
+    if (job->ev1) cudaEventDestroy(job->ev1);
+    delete job;
+}
+
+}  // namespace
+
+int bvh_build_begin(cudaStream_t stream, const PrimSource& src, int32_t* h_counters, int sms, BvhJob*& job_out,
+                    BvhResult& out, std::string& err)
+{
+    const int n = src.num_tris + 2 * src.num_rects + src.num_spheres;
+    job_out = nullptr;
+    out = BvhResult{};
+    if (n == 0) return 0;
+    BvhJob* job = new (std::nothrow) BvhJob();
+    if (!job) {
+        err = "bvh build: host allocation failed";
+        return -1;
+    }
+    job->stream = stream;
+    job->h_cnt = h_counters;
+    BuildBufs& b = job->b;
     b.n = n;
     b.src = src;
     b.max_tasks = n / (kSmall + 1) + 2;
     b.ntiles = (n + kScanTile - 1) / kScanTile;
-    {
-        int dev = 0, sms = 148;
-        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        b.sms = sms;
-    }
+    b.sms = sms;
     const int max_nodes = 2 * n + 2;
-    int32_t h_cnt[16];
-    int nwide = 0, nleaf = 0, depth = 0;
-    FM_BUILD_CHECK(cudaEventCreate(&ev0));
-    FM_BUILD_CHECK(cudaEventCreate(&ev1));
-    FM_BUILD_CHECK(cudaEventRecord(ev0, stream));
+    FM_BUILD_CHECK(cudaEventCreate(&job->ev0));
+    FM_BUILD_CHECK(cudaEventCreate(&job->ev1));
+    FM_BUILD_CHECK(cudaEventRecord(job->ev0, stream));
     FM_BUILD_CHECK(cudaMallocAsync(&b.plo, sizeof(float4) * n, stream));
     FM_BUILD_CHECK(cudaMallocAsync(&b.phi, sizeof(float4) * n, stream));
     FM_BUILD_CHECK(cudaMallocAsync(&b.pidx, sizeof(int32_t) * n, stream));
@@ -1184,19 +1240,24 @@ int bvh_build(cudaStream_t stream, const PrimSource& src, BvhResult& out, std::s
     FM_BUILD_CHECK(cudaMallocAsync(&out.leaf, sizeof(float4) * 3 * (size_t)n, stream));
     b.wnodes = out.nodes;
     b.leaf = out.leaf;
-    {
-        const uint32_t init[12] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u,
-                                   0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
-        FM_BUILD_CHECK(cudaMemcpyAsync(b.rb, init, sizeof(init), cudaMemcpyHostToDevice, stream));
-    }
-    FM_BUILD_CHECK(cudaMemsetAsync(b.counters, 0, sizeof(int32_t) * 16, stream));
-    FM_BUILD_CHECK(cudaMemsetAsync(b.leaf_prim, 0xff, sizeof(int32_t) * n, stream));
-    FM_BUILD_CHECK(build_graph(stream, b, graph));
-    FM_BUILD_CHECK(cudaGraphInstantiate(&exec, graph, 0));
-    FM_BUILD_CHECK(cudaGraphLaunch(exec, stream));
-    FM_BUILD_CHECK(cudaMemcpyAsync(h_cnt, b.counters, sizeof(h_cnt), cudaMemcpyDeviceToHost, stream));
-    FM_BUILD_CHECK(cudaEventRecord(ev1, stream));
-    FM_BUILD_CHECK(cudaEventSynchronize(ev1));
+    FM_BUILD_CHECK(build_graph(stream, b, job->graph));
+    FM_BUILD_CHECK(cudaGraphInstantiate(&job->exec, job->graph, 0));
+    FM_BUILD_CHECK(cudaGraphLaunch(job->exec, stream));
+    FM_BUILD_CHECK(cudaMemcpyAsync(h_counters, b.counters, sizeof(int32_t) * 16, cudaMemcpyDeviceToHost, stream));
+    FM_BUILD_CHECK(cudaEventRecord(job->ev1, stream));
+    job_out = job;
+    return 0;
+fail:
+    drop_job(job, out, true);
+    return -1;
+}
+
+int bvh_build_end(BvhJob* job, BvhResult& out, std::string& err)
+{
+    if (!job) return 0;
+    const int32_t* h_cnt = job->h_cnt;
+    int nwide = 0, nleaf = 0, depth = 0;
+    FM_BUILD_CHECK(cudaEventSynchronize(job->ev1));
     if (h_cnt[5] & 1) {
         err = "bvh build: task list overflow";
         goto fail;
@@ -1212,7 +1273,7 @@ int bvh_build(cudaStream_t stream, const PrimSource& src, BvhResult& out, std::s
     nwide = h_cnt[8 + 0];
     nleaf = h_cnt[8 + 1];
     depth = h_cnt[8 + 4];
-    if (nleaf != n) {
+    if (nleaf != job->b.n) {
         err = "bvh build: leaf count mismatch";
         goto fail;
     }
@@ -1222,69 +1283,27 @@ int bvh_build(cudaStream_t stream, const PrimSource& src, BvhResult& out, std::s
     }
     {
         float ms = 0.0f;
-        cudaEventElapsedTime(&ms, ev0, ev1);
+        cudaEventElapsedTime(&ms, job->ev0, job->ev1);
         out.build_ms = ms;
     }
     out.num_nodes = nwide;
     out.num_leaf = nleaf;
     out.depth = depth;
-    cudaGraphExecDestroy(exec);
-    cudaGraphDestroy(graph);
-    cudaFreeAsync(b.plo, stream);
-    cudaFreeAsync(b.phi, stream);
-    cudaFreeAsync(b.pidx, stream);
-    cudaFreeAsync(b.pidx2, stream);
-    cudaFreeAsync(b.pos_task, stream);
-    cudaFreeAsync(b.pos_task2, stream);
-    cudaFreeAsync(b.flags, stream);
-    cudaFreeAsync(b.scan, stream);
-    cudaFreeAsync(b.tile_sums, stream);
-    cudaFreeAsync(b.small_list, stream);
-    cudaFreeAsync(b.counters, stream);
-    cudaFreeAsync(b.rb, stream);
-    cudaFreeAsync(b.bnodes, stream);
-    cudaFreeAsync(b.tasks, stream);
-    cudaFreeAsync(b.tasks2, stream);
-    cudaFreeAsync(b.splits, stream);
-    cudaFreeAsync(b.bins, stream);
-    cudaFreeAsync(b.front, stream);
-    cudaFreeAsync(b.front2, stream);
-    cudaFreeAsync(b.leaf_prim, stream);
-    cudaEventDestroy(ev0);
-    cudaEventDestroy(ev1);
+    cudaGraphExecDestroy(job->exec);
+    cudaGraphDestroy(job->graph);
+    free_temporaries(job->stream, job->b);
+    cudaEventDestroy(job->ev0);
+    cudaEventDestroy(job->ev1);
+    delete job;
     return 0;
 fail:
-    cudaGetLastError();
-    cudaStreamSynchronize(stream);
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
-    cudaFreeAsync(b.plo, stream);
-    cudaFreeAsync(b.phi, stream);
-    cudaFreeAsync(b.pidx, stream);
-    cudaFreeAsync(b.pidx2, stream);
-    cudaFreeAsync(b.pos_task, stream);
-    cudaFreeAsync(b.pos_task2, stream);
-    cudaFreeAsync(b.flags, stream);
-    cudaFreeAsync(b.scan, stream);
-    cudaFreeAsync(b.tile_sums, stream);
-    cudaFreeAsync(b.small_list, stream);
-    cudaFreeAsync(b.counters, stream);
-    cudaFreeAsync(b.rb, stream);
-    cudaFreeAsync(b.bnodes, stream);
-    cudaFreeAsync(b.tasks, stream);
-    cudaFreeAsync(b.tasks2, stream);
-    cudaFreeAsync(b.splits, stream);
-    cudaFreeAsync(b.bins, stream);
-    cudaFreeAsync(b.front, stream);
-    cudaFreeAsync(b.front2, stream);
-    cudaFreeAsync(b.leaf_prim, stream);
-    cudaFreeAsync(out.nodes, stream);
-    cudaFreeAsync(out.leaf, stream);
-    cudaStreamSynchronize(stream);
-    out = BvhResult{};
-    if (ev0) cudaEventDestroy(ev0);
-    if (ev1) cudaEventDestroy(ev1);
+    drop_job(job, out, true);
     return -1;
+}
+
+void bvh_build_abort(BvhJob* job, BvhResult& out)
+{
+    if (job) drop_job(job, out, true);
 }
 
 }  // namespace fm

@@ -22,7 +22,22 @@ struct BvhResult {
     double build_ms = 0.0;
 };
 
-// Builds the wide BVH on `stream`.  Returns 0 on success, -1 with `err` set otherwise.
-int bvh_build(cudaStream_t stream, const PrimSource& src, BvhResult& out, std::string& err);
+struct BvhJob;   // a build in flight
+
+// Enqueues the wide-BVH build on `stream`: allocations (stream-ordered, from the device's
+// pool), one graph launch, and the copy of the build's 16 counters into `h_counters`
+// (pinned host memory that stays valid until bvh_build_end).  `out.nodes` / `out.leaf` are
+// allocated here.  No host wait.  Returns 0 with `job` set (null for an empty scene), or
+// -1 with `err` set and nothing left allocated.
+int bvh_build_begin(cudaStream_t stream, const PrimSource& src, int32_t* h_counters, int sms, BvhJob*& job,
+                    BvhResult& out, std::string& err);
+
+// Waits for the build, checks its counters (overflows, leaf count, depth), fills
+// out.num_nodes / num_leaf / depth / build_ms and releases the temporaries.  Returns 0, or
+// -1 with `err` set and `out` freed.  Consumes `job`.
+int bvh_build_end(BvhJob* job, BvhResult& out, std::string& err);
+
+// Drops a job that will not be finished (another scene of its batch failed); frees `out`.
+void bvh_build_abort(BvhJob* job, BvhResult& out);
 
 }  // namespace fm

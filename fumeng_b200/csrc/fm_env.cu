@@ -244,7 +244,7 @@ fm_status env_grad_finalize(fm_ctx* ctx, const DevTexture& tex, const double* en
     return FM_OK;
 }
 
-fm_status env_build_tables(fm_ctx* ctx, fm_scene* scene, const DevTexture& tex, DevEnv& env)
+fm_status env_build_tables(fm_ctx* ctx, cudaStream_t st, fm_scene* scene, const DevTexture& tex, DevEnv& env)
 {
     const int w = tex.w, h = tex.h;
     const size_t n = (size_t)w * h;
@@ -261,25 +261,24 @@ fm_status env_build_tables(fm_ctx* ctx, fm_scene* scene, const DevTexture& tex, 
         marg_prob = const_cast<float*>(env.marg_prob);
         marg_alias = const_cast<int32_t*>(env.marg_alias);
     } else {
-        FM_CUDA_TRY(ctx, cudaMallocAsync(&pdf_sample, n * sizeof(float), ctx->stream), "env tables");
+        FM_CUDA_TRY(ctx, cudaMallocAsync(&pdf_sample, n * sizeof(float), st), "env tables");
         track(pdf_sample);
-        FM_CUDA_TRY(ctx, cudaMallocAsync(&pdf_eval, n * sizeof(float), ctx->stream), "env tables");
+        FM_CUDA_TRY(ctx, cudaMallocAsync(&pdf_eval, n * sizeof(float), st), "env tables");
         track(pdf_eval);
-        FM_CUDA_TRY(ctx, cudaMallocAsync(&row_prob, n * sizeof(float), ctx->stream), "env tables");
+        FM_CUDA_TRY(ctx, cudaMallocAsync(&row_prob, n * sizeof(float), st), "env tables");
         track(row_prob);
-        FM_CUDA_TRY(ctx, cudaMallocAsync(&row_alias, n * sizeof(int32_t), ctx->stream), "env tables");
+        FM_CUDA_TRY(ctx, cudaMallocAsync(&row_alias, n * sizeof(int32_t), st), "env tables");
         track(row_alias);
-        FM_CUDA_TRY(ctx, cudaMallocAsync(&marg_prob, h * sizeof(float), ctx->stream), "env tables");
+        FM_CUDA_TRY(ctx, cudaMallocAsync(&marg_prob, h * sizeof(float), st), "env tables");
         track(marg_prob);
-        FM_CUDA_TRY(ctx, cudaMallocAsync(&marg_alias, h * sizeof(int32_t), ctx->stream), "env tables");
+        FM_CUDA_TRY(ctx, cudaMallocAsync(&marg_alias, h * sizeof(int32_t), st), "env tables");
         track(marg_alias);
     }
     // temporaries
-    FM_CUDA_TRY(ctx, cudaMallocAsync(&lum, n * sizeof(float), ctx->stream), "env tables");
-    FM_CUDA_TRY(ctx, cudaMallocAsync(&scratch, 2 * n * sizeof(int32_t), ctx->stream), "env tables");
-    FM_CUDA_TRY(ctx, cudaMallocAsync(&rowsum, h * sizeof(double), ctx->stream), "env tables");
-    FM_CUDA_TRY(ctx, cudaMallocAsync(&totals, 2 * sizeof(double), ctx->stream), "env tables");
-    cudaStream_t st = ctx->stream;
+    FM_CUDA_TRY(ctx, cudaMallocAsync(&lum, n * sizeof(float), st), "env tables");
+    FM_CUDA_TRY(ctx, cudaMallocAsync(&scratch, 2 * n * sizeof(int32_t), st), "env tables");
+    FM_CUDA_TRY(ctx, cudaMallocAsync(&rowsum, h * sizeof(double), st), "env tables");
+    FM_CUDA_TRY(ctx, cudaMallocAsync(&totals, 2 * sizeof(double), st), "env tables");
     k_env_lum<<<(int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096), 256, 0, st>>>(tex, w, h, lum);
     k_env_rowsum<<<h, 256, 0, st>>>(lum, w, rowsum);
     k_env_totals<<<1, 256, 0, st>>>(rowsum, w, h, totals);
@@ -298,8 +297,6 @@ fm_status env_build_tables(fm_ctx* ctx, fm_scene* scene, const DevTexture& tex, 
     cudaFreeAsync(scratch, st);
     cudaFreeAsync(rowsum, st);
     cudaFreeAsync(totals, st);
-    cudaError_t e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return cuda_error(ctx, e, "env tables");
     FM_CUDA_TRY(ctx, cudaGetLastError(), "env tables");
     env.w = w;
     env.h = h;

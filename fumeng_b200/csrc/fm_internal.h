@@ -25,6 +25,13 @@ struct fm_ctx {
     // wavefront workspaces (forward, adjoint): state buffers, pinned staging and the
     // instantiated graph, kept between renders
     fm::WfCache* wf_cache[2] = {nullptr, nullptr};
+    // scene creation: streams that build scenes side by side, and a pinned staging ring
+    // the host arrays pass through on their way to the device
+    std::vector<cudaStream_t> build_streams;
+    std::vector<cudaEvent_t> build_events;
+    char* stage = nullptr;
+    size_t stage_bytes = 0;
+    std::vector<cudaEvent_t> stage_events;
 };
 
 struct fm_scene {
@@ -57,7 +64,14 @@ inline fm_status cuda_error(fm_ctx* ctx, cudaError_t e, const char* where)
         if (e__ != cudaSuccess) return ::fm::cuda_error(ctx, e__, where); \
     } while (0)
 
-// Environment-map importance tables (fm_env.cu).
-fm_status env_build_tables(fm_ctx* ctx, fm_scene* scene, const DevTexture& tex, DevEnv& env);
+// Environment-map importance tables (fm_env.cu), enqueued on `stream` (no host wait; the
+// tables are ready in stream order).
+fm_status env_build_tables(fm_ctx* ctx, cudaStream_t stream, fm_scene* scene, const DevTexture& tex, DevEnv& env);
+
+// RGB float texels (3 per texel) -> the float4 texels the device samples (fm_adjoint.cu).
+void launch_rgb_to_texels(cudaStream_t stream, const float* src, float4* dst, size_t n, int num_sms);
+
+// Releases the scene builder's streams and pinned staging (fm_scene_build.cu).
+void scene_builder_release(fm_ctx* ctx);
 
 }  // namespace fm

@@ -228,6 +228,15 @@ const char* fm_last_error(const fm_ctx* ctx);
  * and the area-light collection of Scene::Scene (core/scene.h:21-25).  Copies the
  * description to the device and builds the BVH there (binned SAH, 8-wide nodes). */
 fm_status fm_scene_create(fm_ctx* ctx, const fm_scene_desc* desc, fm_scene** out);
+
+/* Creates n scenes in one call (out[i] from descs[i]; all or none: on an error every
+ * out[i] is null).  The same work as n fm_scene_create calls -- the reference loads one
+ * scene per run (SceneLoader::Load, create/scene_loader.h:293-302) -- with the uploads
+ * of all scenes streamed through one pinned staging ring and the BVH builds of different
+ * scenes running side by side on the device; the host waits twice per call instead of
+ * several times per scene.  The context keeps the ring (32 MiB pinned) and its builder
+ * streams until fm_ctx_destroy. */
+fm_status fm_scene_create_batch(fm_ctx* ctx, int32_t n, const fm_scene_desc* const* descs, fm_scene** out);
 fm_status fm_scene_destroy(fm_ctx* ctx, fm_scene* scene);
 /* BVH statistics: wide nodes, leaf primitive slots, max depth, build milliseconds. */
 fm_status fm_scene_bvh_stats(fm_ctx* ctx, const fm_scene* scene, int64_t* nodes, int64_t* prims,
