@@ -95,9 +95,6 @@ struct WfState {
     float4* cont_h;       // trace results in continuation-queue order: hit (t, prim, b1, b2)
     int32_t* cont_v;      // ... and the ray's view, so that hit resolution starts from
                           // coalesced loads instead of the slot indirection
-    int32_t* cont_i;      // ... and the hit primitive's light / material-class word
-                          // (DevScene::prim_info; 0 on a miss)
-    int32_t* mis_i;       // the same word for MIS ray hits
     float4* mis_h;        // trace results: MIS ray hits (t, prim, b1, b2)
     uint32_t* sh_h;       // ... shadow ray occluded (1) or not (0)
     int64_t cap_cont, cap_mis, cap_sh;
@@ -469,7 +466,7 @@ FM_D int begin_ray(const WfState& st, int64_t idx, int64_t nc, int64_t nm, Trave
 // A continuation ray's result: route the slot to the shading queue of the hit's material
 // class; a miss or a first-bounce emitter hit ends the path here.
 template <bool ADJ>
-FM_D void finish_cont(const WfState& st, int64_t idx, const DevScene& S, const Hit& h, int info)
+FM_D void finish_cont(const WfState& st, int64_t idx, const DevScene& S, const Hit& h)
 {
     const int cslot = st.cont_q[idx];
     const int cflags = st.flags[cslot];
@@ -488,6 +485,7 @@ FM_D void finish_cont(const WfState& st, int64_t idx, const DevScene& S, const H
             if (ADJ && (cflags & kReplay)) scatter_env(st, S, d, pixel_delta(st, cslot, st.views[st.view[cslot]]));
         }
     } else {
+        const int info = __ldg(S.prim_info + h.prim);
         const int li = depth == 1 ? (info >> 2) - 1 : -1;
         if (li >= 0) {
             const float4 o4 = st.ro[cslot];
@@ -515,7 +513,7 @@ FM_D void finish_cont(const WfState& st, int64_t idx, const DevScene& S, const H
 
 // An MIS-BSDF ray's result: the emitter (or environment) it reaches, MIS-weighted.
 template <bool ADJ>
-FM_D void finish_mis(const WfState& st, int64_t q, const DevScene& S, const Hit& h, int info)
+FM_D void finish_mis(const WfState& st, int64_t q, const DevScene& S, const Hit& h)
 {
     const float4 o4 = st.mis_o[q], d4 = st.mis_d[q], a4 = st.mis_a[q];
     const int slot = __float_as_int(o4.w);
@@ -535,7 +533,7 @@ FM_D void finish_mis(const WfState& st, int64_t q, const DevScene& S, const Hit&
             env_hit = true;
         }
     } else {
-        const int li = (info >> 2) - 1;
+        const int li = (__ldg(S.prim_info + h.prim) >> 2) - 1;
         if (li >= 0) {
             const HitInfo lh = make_hit(S, o, d, h);
             const f3 l2s = normalize(o - lh.pos);
@@ -657,19 +655,14 @@ __global__ void __launch_bounds__(256, 4) k_wf_trace(WfState st)
         if (__ballot_sync(0xffffffffu, kind >= 0) == 0) break;
         if (kind >= 0 && trav_step(t, trace_scene(*Sp), stack, st.status)) {
             const Hit& h = t.hit;
-            // the hit primitive's light / class word travels with the result, so that
-            // hit resolution does not wait for it behind the scene lookup
-            const int info = kind != kRayShadow && h.prim >= 0 ? __ldg(Sp->prim_info + h.prim) : 0;
             if (kind == kRayCont) {
                 st.cont_h[idx] = make_float4(h.t, __int_as_float(h.prim), h.b1, h.b2);
                 st.cont_v[idx] = vid;
-                st.cont_i[idx] = info;
-            } else if (kind == kRayMis) {
-                st.mis_h[idx - nc] = make_float4(h.t, __int_as_float(h.prim), h.b1, h.b2);
-                st.mis_i[idx - nc] = info;
-            } else {
-                st.sh_h[idx - nc - nm] = h.prim >= 0 ? 1u : 0u;
             }
+            else if (kind == kRayMis)
+                st.mis_h[idx - nc] = make_float4(h.t, __int_as_float(h.prim), h.b1, h.b2);
+            else
+                st.sh_h[idx - nc - nm] = h.prim >= 0 ? 1u : 0u;
             kind = -1;
         }
     }
@@ -696,13 +689,13 @@ __global__ void __launch_bounds__(256) k_wf_resolve(WfState st)
             const float4 h4 = st.cont_h[i];
             const int vid = st.cont_v[i];
             st.hit[slot] = h4;   // the shading kernels read it by slot
-            finish_cont<ADJ>(st, i, *st.views[vid].scene, Hit{h4.x, __float_as_int(h4.y), h4.z, h4.w}, st.cont_i[i]);
+            finish_cont<ADJ>(st, i, *st.views[vid].scene, Hit{h4.x, __float_as_int(h4.y), h4.z, h4.w});
         } else if (i < nc + nm) {
             ++n_closest;
             const int64_t q = i - nc;
             const float4 h4 = st.mis_h[q];
             finish_mis<ADJ>(st, q, *st.views[__float_as_int(st.mis_a[q].w)].scene,
-                            Hit{h4.x, __float_as_int(h4.y), h4.z, h4.w}, st.mis_i[q]);
+                            Hit{h4.x, __float_as_int(h4.y), h4.z, h4.w});
         } else {
             ++n_shadow;
             const int64_t q = i - nc - nm;
@@ -1371,14 +1364,12 @@ fm_status wf_cache_reserve(fm_ctx* ctx, bool adj, int64_t pool, int64_t cap_mis,
         A(b.cont_q, pool);
         A(b.cont_h, pool);
         A(b.cont_v, pool);
-        A(b.cont_i, pool);
         A(b.disney_q, pool);
         A(b.simple_q, pool);
         A(b.mis_o, cap_mis);
         A(b.mis_d, cap_mis);
         A(b.mis_a, cap_mis);
         A(b.mis_h, cap_mis);
-        A(b.mis_i, cap_mis);
         A(b.sh_o, cap_sh);
         A(b.sh_d, cap_sh);
         A(b.sh_c, cap_sh);
