@@ -4,6 +4,7 @@
 #include <vector>
 
 #include "fm_render.h"
+#include "fm_staging.h"
 
 namespace fm {
 
@@ -263,12 +264,15 @@ extern "C" fm_status fm_render_batch(fm_ctx* ctx, int32_t n, const fm_scene* con
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
     }
+    cudaError_t ecopy = cudaSuccess;
     if (st == FM_OK && !dev) {
+        std::vector<OutCopy> out;
         for (int i = 0; i < n; ++i) {
-            cudaMemcpyAsync(rgb[i], d_rgb[i], bytes[i], cudaMemcpyDeviceToHost, ctx->stream);
-            if (d_alb[i]) cudaMemcpyAsync(albedo[i], d_alb[i], bytes[i], cudaMemcpyDeviceToHost, ctx->stream);
-            if (d_nrm[i]) cudaMemcpyAsync(normal[i], d_nrm[i], bytes[i], cudaMemcpyDeviceToHost, ctx->stream);
+            out.push_back(OutCopy{rgb[i], d_rgb[i], bytes[i]});
+            if (d_alb[i]) out.push_back(OutCopy{albedo[i], d_alb[i], bytes[i]});
+            if (d_nrm[i]) out.push_back(OutCopy{normal[i], d_nrm[i], bytes[i]});
         }
+        ecopy = copy_out(ctx, ctx->stream, out);
     }
     Counters hc{};
     uint32_t hs = 0;
@@ -277,6 +281,7 @@ extern "C" fm_status fm_render_batch(fm_ctx* ctx, int32_t n, const fm_scene* con
     cudaFreeAsync(staging, ctx->stream);
     const cudaError_t e = cudaStreamSynchronize(ctx->stream);
     if (st != FM_OK) return st;
+    if (ecopy != cudaSuccess) return cuda_error(ctx, ecopy, "batch: image copy");
     if (e != cudaSuccess) return cuda_error(ctx, e, "batch");
     if (stats) {
         stats->paths = (int64_t)hc.paths;

@@ -1190,8 +1190,8 @@ void drop_job(BvhJob* job, BvhResult& out, bool free_out)
 
 }  // namespace
 
-int bvh_build_begin(cudaStream_t stream, const PrimSource& src, int32_t* h_counters, int sms, BvhJob*& job_out,
-                    BvhResult& out, std::string& err)
+int bvh_build_begin(cudaStream_t stream, cudaStream_t capture, const PrimSource& src, int32_t* h_counters, int sms,
+                    BvhJob*& job_out, BvhResult& out, std::string& err)
 {
     const int n = src.num_tris + 2 * src.num_rects + src.num_spheres;
     job_out = nullptr;
@@ -1240,7 +1240,7 @@ int bvh_build_begin(cudaStream_t stream, const PrimSource& src, int32_t* h_count
     FM_BUILD_CHECK(cudaMallocAsync(&out.leaf, sizeof(float4) * 3 * (size_t)n, stream));
     b.wnodes = out.nodes;
     b.leaf = out.leaf;
-    FM_BUILD_CHECK(build_graph(stream, b, job->graph));
+    FM_BUILD_CHECK(build_graph(capture, b, job->graph));
     FM_BUILD_CHECK(cudaGraphInstantiate(&job->exec, job->graph, 0));
     FM_BUILD_CHECK(cudaGraphLaunch(job->exec, stream));
     FM_BUILD_CHECK(cudaMemcpyAsync(h_counters, b.counters, sizeof(int32_t) * 16, cudaMemcpyDeviceToHost, stream));

@@ -26,11 +26,13 @@ struct BvhJob;   // a build in flight
 
 // Enqueues the wide-BVH build on `stream`: allocations (stream-ordered, from the device's
 // pool), one graph launch, and the copy of the build's 16 counters into `h_counters`
-// (pinned host memory that stays valid until bvh_build_end).  `out.nodes` / `out.leaf` are
-// allocated here.  No host wait.  Returns 0 with `job` set (null for an empty scene), or
-// -1 with `err` set and nothing left allocated.
-int bvh_build_begin(cudaStream_t stream, const PrimSource& src, int32_t* h_counters, int sms, BvhJob*& job,
-                    BvhResult& out, std::string& err);
+// (pinned host memory that stays valid until bvh_build_end).  The graph is captured on
+// `capture`, a stream that nothing else uses (work another thread puts on `stream`
+// meanwhile must not join the capture).  `out.nodes` / `out.leaf` are allocated here.  No
+// host wait.  Returns 0 with `job` set (null for an empty scene), or -1 with `err` set and
+// nothing left allocated.
+int bvh_build_begin(cudaStream_t stream, cudaStream_t capture, const PrimSource& src, int32_t* h_counters, int sms,
+                    BvhJob*& job, BvhResult& out, std::string& err);
 
 // Waits for the build, checks its counters (overflows, leaf count, depth), fills
 // out.num_nodes / num_leaf / depth / build_ms and releases the temporaries.  Returns 0, or

@@ -6,6 +6,7 @@
 
 #include "fm_bvh.cuh"
 #include "fm_internal.h"
+#include "fm_staging.h"
 
 using namespace fm;
 
@@ -117,6 +118,7 @@ void fm_ctx_destroy(fm_ctx* ctx)
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     fm::scene_builder_release(ctx);
+    fm::staging_release(ctx);
     fm::wf_cache_release(ctx);
     cudaFree(ctx->d_status);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);

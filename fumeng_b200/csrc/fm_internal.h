@@ -10,7 +10,8 @@
 #include "fm_scene.cuh"
 
 namespace fm {
-struct WfCache;   // wavefront workspace (fm_wavefront.cu)
+struct WfCache;    // wavefront workspace (fm_wavefront.cu)
+class CopyPool;    // host copy threads (fm_staging.cu)
 void wf_cache_release(fm_ctx* ctx);
 }  // namespace fm
 
@@ -25,13 +26,17 @@ struct fm_ctx {
     // wavefront workspaces (forward, adjoint): state buffers, pinned staging and the
     // instantiated graph, kept between renders
     fm::WfCache* wf_cache[2] = {nullptr, nullptr};
-    // scene creation: streams that build scenes side by side, and a pinned staging ring
-    // the host arrays pass through on their way to the device
+    // scene creation: streams that build scenes side by side
     std::vector<cudaStream_t> build_streams;
     std::vector<cudaEvent_t> build_events;
+    cudaStream_t capture_stream = nullptr;   // BVH build graphs are captured here, never run
+    int32_t* build_counters = nullptr;   // pinned, 16 per scene of the largest batch
+    int64_t build_counters_cap = 0;
+    // pinned staging ring for host <-> device transfers (fm_staging.h): kStageChunks
+    // chunks, an event per chunk, and the host copy threads
     char* stage = nullptr;
-    size_t stage_bytes = 0;
     std::vector<cudaEvent_t> stage_events;
+    fm::CopyPool* copy_pool = nullptr;
 };
 
 struct fm_scene {
@@ -71,7 +76,7 @@ fm_status env_build_tables(fm_ctx* ctx, cudaStream_t stream, fm_scene* scene, co
 // RGB float texels (3 per texel) -> the float4 texels the device samples (fm_adjoint.cu).
 void launch_rgb_to_texels(cudaStream_t stream, const float* src, float4* dst, size_t n, int num_sms);
 
-// Releases the scene builder's streams and pinned staging (fm_scene_build.cu).
+// Releases the scene builder's streams (fm_scene_build.cu).
 void scene_builder_release(fm_ctx* ctx);
 
 }  // namespace fm

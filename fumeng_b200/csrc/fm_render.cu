@@ -7,6 +7,7 @@
 #include "fm_internal.h"
 #include "fm_path.cuh"
 #include "fm_render.h"
+#include "fm_staging.h"
 
 namespace fm {
 
@@ -283,10 +284,12 @@ extern "C" fm_status fm_render(fm_ctx* ctx, const fm_scene* scene, const fm_came
     else
         st = launch_megakernel(ctx, scene, cam, cfg, d_rgb, d_alb, d_nrm, d_cnt);
     cudaEventRecord(e1, ctx->stream);
+    cudaError_t ecopy = cudaSuccess;
     if (st == FM_OK && !dev) {
-        cudaMemcpyAsync(rgb, d_rgb, img_bytes, cudaMemcpyDeviceToHost, ctx->stream);
-        if (albedo) cudaMemcpyAsync(albedo, d_alb, img_bytes, cudaMemcpyDeviceToHost, ctx->stream);
-        if (normal) cudaMemcpyAsync(normal, d_nrm, img_bytes, cudaMemcpyDeviceToHost, ctx->stream);
+        std::vector<OutCopy> out{OutCopy{rgb, d_rgb, img_bytes}};
+        if (albedo) out.push_back(OutCopy{albedo, d_alb, img_bytes});
+        if (normal) out.push_back(OutCopy{normal, d_nrm, img_bytes});
+        ecopy = copy_out(ctx, ctx->stream, out);
     }
     Counters hc{};
     uint32_t hs = 0;
@@ -299,6 +302,7 @@ extern "C" fm_status fm_render(fm_ctx* ctx, const fm_scene* scene, const fm_came
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (st != FM_OK) return st;
+    if (ecopy != cudaSuccess) return cuda_error(ctx, ecopy, "render: image copy");
     if (e != cudaSuccess) return cuda_error(ctx, e, "render");
     if (stats) {
         stats->paths = (int64_t)hc.paths;

@@ -10,12 +10,16 @@
 // for all builds, writes each scene's DevScene record, and waits once more.
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <new>
+#include <thread>
 
 #include "fm_bvh.cuh"
 #include "fm_internal.h"
+#include "fm_staging.h"
 
 using namespace fm;
 
@@ -41,10 +45,8 @@ void launch_rgb_to_texels(cudaStream_t stream, const float* src, float4* dst, si
 
 namespace {
 
-constexpr int kBuildStreams = 8;                 // scenes whose device work runs side by side
-constexpr int kStageChunks = 4;                  // pinned staging ring: chunks ...
-constexpr size_t kStageChunk = size_t(8) << 20;  // ... of 8 MiB
-constexpr size_t kAlign = 256;                   // sub-array alignment inside a scene's block
+constexpr int kBuildStreams = 8;   // scenes whose device work runs side by side
+constexpr size_t kAlign = 256;     // sub-array alignment inside a scene's block
 
 size_t align_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
 
@@ -200,6 +202,14 @@ struct SceneBuild {
     std::vector<SphereDev> sph;
     std::vector<DevMaterial> mats;
 
+    std::string error;
+
+    fm_status fail(fm_status st, const char* msg)
+    {
+        error = msg;
+        return st;
+    }
+
     template <typename T>
     void add(const T* host, size_t count, const T** field)
     {
@@ -212,29 +222,30 @@ struct SceneBuild {
 };
 
 // Validates a description and prepares everything host-side: derived arrays, lights and
-// their tables, and the layout of the scene's device block.  No device work.
-fm_status prepare_scene(fm_ctx* ctx, const fm_scene_desc* d, SceneBuild& B)
+// their tables, and the layout of the scene's device block.  No device work and no
+// context state (scenes are prepared on several threads); errors go to B.error.
+fm_status prepare_scene(const fm_scene_desc* d, SceneBuild& B)
 {
-    if (!d) return set_error(ctx, FM_ERR_INVALID, "scene_create: null argument");
+    if (!d) return B.fail(FM_ERR_INVALID, "scene_create: null argument");
     if (d->num_objects < 0 || d->num_triangles < 0 || d->num_rects < 0 || d->num_spheres < 0 ||
         d->num_materials < 0 || d->num_textures < 0 || d->num_lights < 0)
-        return set_error(ctx, FM_ERR_INVALID, "scene_create: negative count");
+        return B.fail(FM_ERR_INVALID, "scene_create: negative count");
     const int64_t nprim = d->num_triangles + 2 * d->num_rects + d->num_spheres;
-    if (nprim > (int64_t)0x3fffffff) return set_error(ctx, FM_ERR_INVALID, "scene_create: too many primitives");
-    if (d->num_objects > 0 && !d->obj_material) return set_error(ctx, FM_ERR_INVALID, "scene_create: obj_material is null");
+    if (nprim > (int64_t)0x3fffffff) return B.fail(FM_ERR_INVALID, "scene_create: too many primitives");
+    if (d->num_objects > 0 && !d->obj_material) return B.fail(FM_ERR_INVALID, "scene_create: obj_material is null");
     if (d->num_triangles > 0 && (!d->tri_pos || !d->tri_object))
-        return set_error(ctx, FM_ERR_INVALID, "scene_create: triangle arrays are null");
+        return B.fail(FM_ERR_INVALID, "scene_create: triangle arrays are null");
     if (d->num_rects > 0 && (!d->rect_pts || !d->rect_object))
-        return set_error(ctx, FM_ERR_INVALID, "scene_create: rectangle arrays are null");
+        return B.fail(FM_ERR_INVALID, "scene_create: rectangle arrays are null");
     if (d->num_spheres > 0 && (!d->sphere_radius || !d->sphere_xform || !d->sphere_object))
-        return set_error(ctx, FM_ERR_INVALID, "scene_create: sphere arrays are null");
-    if (d->num_materials > 0 && !d->materials) return set_error(ctx, FM_ERR_INVALID, "scene_create: materials is null");
-    if (d->num_textures > 0 && !d->textures) return set_error(ctx, FM_ERR_INVALID, "scene_create: textures is null");
-    if (d->num_lights > 0 && !d->lights) return set_error(ctx, FM_ERR_INVALID, "scene_create: lights is null");
-    if (d->tri_vattr && d->vattr_dim < 6) return set_error(ctx, FM_ERR_INVALID, "scene_create: vattr_dim < 6");
+        return B.fail(FM_ERR_INVALID, "scene_create: sphere arrays are null");
+    if (d->num_materials > 0 && !d->materials) return B.fail(FM_ERR_INVALID, "scene_create: materials is null");
+    if (d->num_textures > 0 && !d->textures) return B.fail(FM_ERR_INVALID, "scene_create: textures is null");
+    if (d->num_lights > 0 && !d->lights) return B.fail(FM_ERR_INVALID, "scene_create: lights is null");
+    if (d->tri_vattr && d->vattr_dim < 6) return B.fail(FM_ERR_INVALID, "scene_create: vattr_dim < 6");
     for (int64_t o = 0; o < d->num_objects; ++o)
         if (d->obj_material[o] < 0 || d->obj_material[o] >= d->num_materials)
-            return set_error(ctx, FM_ERR_INVALID, "scene_create: object material index out of range");
+            return B.fail(FM_ERR_INVALID, "scene_create: object material index out of range");
     // object -> geometry (needed for area lights), and range checks
     std::vector<int32_t> geo_kind(d->num_objects, -1), geo_index(d->num_objects, -1), geo_count(d->num_objects, 0);
     auto note = [&](int32_t obj, int kind, int64_t idx) -> bool {
@@ -245,39 +256,39 @@ fm_status prepare_scene(fm_ctx* ctx, const fm_scene_desc* d, SceneBuild& B)
         return true;
     };
     for (int64_t i = 0; i < d->num_triangles; ++i)
-        if (!note(d->tri_object[i], LK_AREA_TRI, i)) return set_error(ctx, FM_ERR_INVALID, "scene_create: triangle object out of range");
+        if (!note(d->tri_object[i], LK_AREA_TRI, i)) return B.fail(FM_ERR_INVALID, "scene_create: triangle object out of range");
     for (int64_t i = 0; i < d->num_rects; ++i)
-        if (!note(d->rect_object[i], LK_AREA_RECT, i)) return set_error(ctx, FM_ERR_INVALID, "scene_create: rectangle object out of range");
+        if (!note(d->rect_object[i], LK_AREA_RECT, i)) return B.fail(FM_ERR_INVALID, "scene_create: rectangle object out of range");
     for (int64_t i = 0; i < d->num_spheres; ++i)
-        if (!note(d->sphere_object[i], LK_AREA_SPHERE, i)) return set_error(ctx, FM_ERR_INVALID, "scene_create: sphere object out of range");
+        if (!note(d->sphere_object[i], LK_AREA_SPHERE, i)) return B.fail(FM_ERR_INVALID, "scene_create: sphere object out of range");
     for (int32_t i = 0; i < d->num_textures; ++i) {
         const fm_texture_desc& t = d->textures[i];
-        if (t.width <= 0 || t.height <= 0 || !t.texels) return set_error(ctx, FM_ERR_INVALID, "scene_create: bad texture");
+        if (t.width <= 0 || t.height <= 0 || !t.texels) return B.fail(FM_ERR_INVALID, "scene_create: bad texture");
     }
     auto tex_ok = [&](const fm_tex_ref& r) { return r.texture < d->num_textures; };
     for (int32_t i = 0; i < d->num_materials; ++i) {
         const fm_material_desc& m = d->materials[i];
-        if (m.type < FM_MAT_LAMBERT || m.type > FM_MAT_DISNEY) return set_error(ctx, FM_ERR_INVALID, "scene_create: bad material type");
+        if (m.type < FM_MAT_LAMBERT || m.type > FM_MAT_DISNEY) return B.fail(FM_ERR_INVALID, "scene_create: bad material type");
         const fm_tex_ref* refs = &m.basecolor;
         for (int k = 0; k < MP_COUNT; ++k)
-            if (!tex_ok(refs[k])) return set_error(ctx, FM_ERR_INVALID, "scene_create: material texture out of range");
+            if (!tex_ok(refs[k])) return B.fail(FM_ERR_INVALID, "scene_create: material texture out of range");
         if (m.vattr_offset >= 0 && (!d->tri_vattr || m.vattr_offset + 6 > d->vattr_dim))
-            return set_error(ctx, FM_ERR_INVALID, "scene_create: material vertex attributes out of range");
+            return B.fail(FM_ERR_INVALID, "scene_create: material vertex attributes out of range");
     }
     int env_light_desc = -1;
     for (int32_t i = 0; i < d->num_lights; ++i) {
         const fm_light_desc& l = d->lights[i];
         if (l.type == FM_LIGHT_ENV) {
-            if (l.texture < 0 || l.texture >= d->num_textures) return set_error(ctx, FM_ERR_INVALID, "scene_create: env texture out of range");
+            if (l.texture < 0 || l.texture >= d->num_textures) return B.fail(FM_ERR_INVALID, "scene_create: env texture out of range");
             if (env_light_desc < 0) env_light_desc = i;
         } else if (l.type != FM_LIGHT_DIRECTIONAL) {
-            return set_error(ctx, FM_ERR_INVALID, "scene_create: bad light type");
+            return B.fail(FM_ERR_INVALID, "scene_create: bad light type");
         }
     }
     B.env_light_desc = env_light_desc;
 
     fm_scene* sc = new (std::nothrow) fm_scene();
-    if (!sc) return set_error(ctx, FM_ERR_OOM, "scene_create: host allocation");
+    if (!sc) return B.fail(FM_ERR_OOM, "scene_create: host allocation");
     B.sc = sc;
     sc->num_objects = d->num_objects;
     DevScene& S = sc->dev;
@@ -335,7 +346,7 @@ fm_status prepare_scene(fm_ctx* ctx, const fm_scene_desc* d, SceneBuild& B)
     for (int64_t i = 0; i < d->num_spheres; ++i) {
         SphereDev& P = B.sph[i];
         if (!affine_inverse(d->sphere_xform + 16 * i, P.o2w, P.w2o))
-            return set_error(ctx, FM_ERR_INVALID, "scene_create: singular sphere transform");
+            return B.fail(FM_ERR_INVALID, "scene_create: singular sphere transform");
         P.radius = d->sphere_radius[i];
         const f3 ax = f3{P.o2w.m[0], P.o2w.m[4], P.o2w.m[8]};
         P.radius_world = P.radius * length(ax);
@@ -395,7 +406,7 @@ fm_status prepare_scene(fm_ctx* ctx, const fm_scene_desc* d, SceneBuild& B)
             const float* em = d->obj_emission + 3 * o;
             if (is_black_h(em)) continue;
             if (geo_count[o] != 1)
-                return set_error(ctx, FM_ERR_INVALID, "scene_create: an emissive object must have exactly one shape");
+                return B.fail(FM_ERR_INVALID, "scene_create: an emissive object must have exactly one shape");
             const int32_t group =
                 geo_kind[o] == LK_AREA_TRI && d->tri_light_group ? d->tri_light_group[geo_index[o]] : -1;
             if (group >= 0) {
@@ -403,7 +414,7 @@ fm_status prepare_scene(fm_ctx* ctx, const fm_scene_desc* d, SceneBuild& B)
                 if (it != group_light.end()) {
                     const DevLight& G = lights[it->second];
                     if (G.radiance[0] != em[0] || G.radiance[1] != em[1] || G.radiance[2] != em[2])
-                        return set_error(ctx, FM_ERR_INVALID, "scene_create: a mesh light's triangles differ in emission");
+                        return B.fail(FM_ERR_INVALID, "scene_create: a mesh light's triangles differ in emission");
                     mesh_tris[G.index].push_back(geo_index[o]);
                     B.obj_light[o] = it->second;
                     continue;
@@ -440,7 +451,7 @@ fm_status prepare_scene(fm_ctx* ctx, const fm_scene_desc* d, SceneBuild& B)
                 area[k] = 0.5 * std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
                 total += area[k];
             }
-            if (!(total > 0.0)) return set_error(ctx, FM_ERR_INVALID, "scene_create: a mesh light has zero area");
+            if (!(total > 0.0)) return B.fail(FM_ERR_INVALID, "scene_create: a mesh light has zero area");
             std::vector<float> prob;
             std::vector<int32_t> alias;
             vose_alias(area, prob, alias);
@@ -496,92 +507,35 @@ fm_status prepare_scene(fm_ctx* ctx, const fm_scene_desc* d, SceneBuild& B)
     return FM_OK;
 }
 
-// Copies host bytes to device addresses through the context's pinned ring, on one
-// stream: consecutive bytes bound for consecutive device addresses go as one copy.
-struct Stager {
-    fm_ctx* ctx;
-    cudaStream_t s;
-    int chunk = -1;
-    size_t used = kStageChunk;
-    char* run_dst = nullptr;
-    const char* run_src = nullptr;
-    size_t run_len = 0;
-    cudaError_t err = cudaSuccess;
-
-    void flush()
-    {
-        if (run_len && err == cudaSuccess) err = cudaMemcpyAsync(run_dst, run_src, run_len, cudaMemcpyHostToDevice, s);
-        run_len = 0;
-    }
-    // Closes the current chunk (its copies are issued) and waits until the next chunk's
-    // previous copies have finished reading it.
-    void next_chunk()
-    {
-        flush();
-        if (chunk >= 0 && err == cudaSuccess) err = cudaEventRecord(ctx->stage_events[chunk], s);
-        chunk = (chunk + 1) % kStageChunks;
-        if (err == cudaSuccess) err = cudaEventSynchronize(ctx->stage_events[chunk]);
-        used = 0;
-    }
-    void put(void* dst_dev, const void* src_host, size_t bytes)
-    {
-        char* dst = static_cast<char*>(dst_dev);
-        const char* src = static_cast<const char*>(src_host);
-        while (bytes > 0 && err == cudaSuccess) {
-            if (used == kStageChunk) next_chunk();
-            if (err != cudaSuccess) return;
-            const size_t k = std::min(bytes, kStageChunk - used);
-            char* h = ctx->stage + (size_t)chunk * kStageChunk + used;
-            std::memcpy(h, src, k);
-            if (run_len && run_dst + run_len == dst && run_src + run_len == h) {
-                run_len += k;
-            } else {
-                flush();
-                run_dst = dst;
-                run_src = h;
-                run_len = k;
-            }
-            used += k;
-            dst += k;
-            src += k;
-            bytes -= k;
-        }
-    }
-    // Issues what is pending and marks the current chunk busy until its copies finish.
-    void close()
-    {
-        flush();
-        if (chunk >= 0 && err == cudaSuccess) err = cudaEventRecord(ctx->stage_events[chunk], s);
-        used = kStageChunk;
-    }
-};
-
 fm_status ensure_builder(fm_ctx* ctx)
 {
     if (ctx->build_streams.empty()) {
-        for (int k = 0; k < kBuildStreams; ++k) {
+        // streams [0, kBuildStreams) run builds, the last one only captures their graphs;
+        // events: [0] a scene's arrays are on the device, [1 + k] builder stream k is done
+        std::vector<cudaStream_t> streams;
+        std::vector<cudaEvent_t> events;
+        cudaError_t e = cudaSuccess;
+        for (int k = 0; k <= kBuildStreams && e == cudaSuccess; ++k) {
             cudaStream_t s = nullptr;
-            FM_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "scene builder streams");
-            ctx->build_streams.push_back(s);
+            e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+            if (e == cudaSuccess) streams.push_back(s);
         }
-        // [0]: a scene's arrays are on the device; [1 + k]: builder stream k is done
-        for (int k = 0; k < kBuildStreams + 1; ++k) {
-            cudaEvent_t e = nullptr;
-            FM_CUDA_TRY(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "scene builder events");
-            ctx->build_events.push_back(e);
+        for (int k = 0; k <= kBuildStreams && e == cudaSuccess; ++k) {
+            cudaEvent_t ev = nullptr;
+            e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+            if (e == cudaSuccess) events.push_back(ev);
         }
+        if (e != cudaSuccess) {
+            for (cudaStream_t s : streams) cudaStreamDestroy(s);
+            for (cudaEvent_t ev : events) cudaEventDestroy(ev);
+            return cuda_error(ctx, e, "scene builder streams");
+        }
+        ctx->capture_stream = streams.back();
+        streams.pop_back();
+        ctx->build_streams = streams;
+        ctx->build_events = events;
     }
-    if (!ctx->stage) {
-        void* p = nullptr;
-        FM_CUDA_TRY(ctx, cudaHostAlloc(&p, kStageChunk * kStageChunks, cudaHostAllocDefault), "scene staging");
-        ctx->stage = static_cast<char*>(p);
-        ctx->stage_bytes = kStageChunk * kStageChunks;
-        for (int k = 0; k < kStageChunks; ++k) {
-            cudaEvent_t e = nullptr;
-            FM_CUDA_TRY(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "scene staging events");
-            ctx->stage_events.push_back(e);
-        }
-    }
+    FM_CUDA_TRY(ctx, staging_ensure(ctx), "scene staging");
     return FM_OK;
 }
 
@@ -603,40 +557,127 @@ void discard(fm_ctx* ctx, std::vector<SceneBuild>& builds)
     cudaGetLastError();
 }
 
-fm_status create_scenes(fm_ctx* ctx, int32_t n, const fm_scene_desc* const* descs, fm_scene** out)
-{
-    std::vector<SceneBuild> builds((size_t)n);
-    for (int32_t i = 0; i < n; ++i) {
-        const fm_status st = prepare_scene(ctx, descs[i], builds[i]);
-        if (st != FM_OK) {
-            for (SceneBuild& B : builds) delete B.sc;
-            return st;
+// Issues the BVH builds on a thread of their own, in scene order, as the main thread
+// hands scenes over; the host cost of a build (allocations, graph capture and
+// instantiation) then overlaps the main thread's uploads.
+class BvhIssuer {
+public:
+    BvhIssuer(fm_ctx* ctx, std::vector<SceneBuild>& builds) : ctx_(ctx), builds_(builds)
+    {
+        thread_ = std::thread([this] { loop(); });
+    }
+    ~BvhIssuer() { finish(); }
+    void hand_over(int i, cudaStream_t s)
+    {
+        std::lock_guard<std::mutex> lk(m_);
+        queue_.push_back({i, s});
+        cv_.notify_one();
+    }
+    // Waits until every handed-over scene has been issued; returns false (with `err`) if
+    // one failed (the later ones are then not issued).
+    bool finish()
+    {
+        if (thread_.joinable()) {
+            {
+                std::lock_guard<std::mutex> lk(m_);
+                closed_ = true;
+            }
+            cv_.notify_one();
+            thread_.join();
+        }
+        return err_.empty();
+    }
+    const std::string& error() const { return err_; }
+
+private:
+    void loop()
+    {
+        cudaSetDevice(ctx_->device);
+        size_t next = 0;
+        for (;;) {
+            std::pair<int, cudaStream_t> job;
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                cv_.wait(lk, [&] { return closed_ || next < queue_.size(); });
+                if (next == queue_.size()) return;
+                job = queue_[next++];
+            }
+            if (!err_.empty()) continue;
+            SceneBuild& B = builds_[(size_t)job.first];
+            const DevScene& S = B.sc->dev;
+            PrimSource src;
+            src.num_tris = S.num_tris;
+            src.num_rects = S.num_rects;
+            src.num_spheres = S.num_spheres;
+            src.tri_pos = S.tri_pos;
+            src.rects = S.rects;
+            src.spheres = S.spheres;
+            std::string err;
+            if (bvh_build_begin(job.second, ctx_->capture_stream, src, B.h_counters, ctx_->num_sms, B.job, B.sc->bvh,
+                                err) != 0)
+                err_ = err.empty() ? std::string("bvh build failed") : err;
         }
     }
+    fm_ctx* ctx_;
+    std::vector<SceneBuild>& builds_;
+    std::thread thread_;
+    std::mutex m_;
+    std::condition_variable cv_;
+    std::vector<std::pair<int, cudaStream_t>> queue_;
+    bool closed_ = false;
+    std::string err_;
+};
+
+fm_status create_scenes(fm_ctx* ctx, int32_t n, const fm_scene_desc* const* descs, fm_scene** out)
+{
     FM_CUDA_TRY(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
     {
         const fm_status st = ensure_builder(ctx);
-        if (st != FM_OK) {
-            for (SceneBuild& B : builds) delete B.sc;
-            return st;
+        if (st != FM_OK) return st;
+    }
+    std::vector<SceneBuild> builds((size_t)n);
+    // host preparation, scenes side by side
+    {
+        std::vector<fm_status> sts((size_t)n, FM_OK);
+        host_parallel(ctx, n, [&](int i) {
+            try {
+                sts[i] = prepare_scene(descs[i], builds[i]);
+            } catch (const std::bad_alloc&) {
+                sts[i] = builds[i].fail(FM_ERR_OOM, "scene_create: host allocation failed");
+            }
+        });
+        for (int32_t i = 0; i < n; ++i) {
+            if (sts[i] != FM_OK) {
+                const std::string msg = builds[i].error;
+                for (SceneBuild& B : builds) delete B.sc;
+                return set_error(ctx, sts[i], msg);
+            }
         }
     }
-    // BVH counters (pinned)
-    int32_t* counters = nullptr;
-    FM_CUDA_TRY(ctx, cudaHostAlloc(reinterpret_cast<void**>(&counters), sizeof(int32_t) * 16 * (size_t)n, 0),
-                "scene build counters");
-    struct PinnedFree {
-        int32_t* p;
-        ~PinnedFree() { cudaFreeHost(p); }
-    } counters_guard{counters};
+    if (ctx->build_counters_cap < n) {
+        if (ctx->build_counters) cudaFreeHost(ctx->build_counters);
+        ctx->build_counters = nullptr;
+        ctx->build_counters_cap = 0;
+        void* p = nullptr;
+        const cudaError_t e = cudaHostAlloc(&p, sizeof(int32_t) * 16 * (size_t)n, cudaHostAllocDefault);
+        if (e != cudaSuccess) {
+            for (SceneBuild& B : builds) delete B.sc;
+            return cuda_error(ctx, e, "scene build counters");
+        }
+        ctx->build_counters = static_cast<int32_t*>(p);
+        ctx->build_counters_cap = n;
+    }
     cudaStream_t cs = ctx->stream;
-    Stager stager{ctx, cs};
-    std::string err;
+    Stager stager(ctx, cs);
     fm_status st = FM_OK;
-    auto fail_cuda = [&](cudaError_t e, const char* where) {
-        st = cuda_error(ctx, e, where);
+    BvhIssuer issuer(ctx, builds);
+    auto fail = [&](fm_status code, const std::string& msg) {
+        issuer.finish();
         discard(ctx, builds);
-        return st;
+        return set_error(ctx, code, msg);
+    };
+    auto fail_cuda = [&](cudaError_t e, const char* where) {
+        return fail(FM_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
     };
     for (int32_t i = 0; i < n; ++i) {
         SceneBuild& B = builds[i];
@@ -676,35 +717,20 @@ fm_status create_scenes(fm_ctx* ctx, int32_t n, const fm_scene_desc* const* desc
         if (e != cudaSuccess) return fail_cuda(e, "texel expansion");
         if (B.env_light_desc >= 0) {
             st = env_build_tables(ctx, bs, sc, sc->textures[S.env.tex], S.env);
-            if (st != FM_OK) {
-                const std::string msg = ctx->error;
-                discard(ctx, builds);
-                return set_error(ctx, st, msg);
-            }
+            if (st != FM_OK) return fail(st, ctx->error);
         }
-        PrimSource src;
-        src.num_tris = S.num_tris;
-        src.num_rects = S.num_rects;
-        src.num_spheres = S.num_spheres;
-        src.tri_pos = S.tri_pos;
-        src.rects = S.rects;
-        src.spheres = S.spheres;
-        B.h_counters = counters + 16 * (size_t)i;
-        if (bvh_build_begin(bs, src, B.h_counters, ctx->num_sms, B.job, sc->bvh, err) != 0) {
-            discard(ctx, builds);
-            return set_error(ctx, FM_ERR_CUDA, err);
-        }
+        B.h_counters = ctx->build_counters + 16 * (size_t)i;
+        issuer.hand_over(i, bs);
     }
+    if (!issuer.finish()) return fail(FM_ERR_CUDA, issuer.error());
     // wait for the builds; then every scene's record
     for (int32_t i = 0; i < n; ++i) {
         SceneBuild& B = builds[i];
         fm_scene* sc = B.sc;
         BvhJob* job = B.job;
         B.job = nullptr;
-        if (bvh_build_end(job, sc->bvh, err) != 0) {
-            discard(ctx, builds);
-            return set_error(ctx, FM_ERR_CUDA, err);
-        }
+        std::string err;
+        if (bvh_build_end(job, sc->bvh, err) != 0) return fail(FM_ERR_CUDA, err);
         if (sc->bvh.nodes) sc->allocations.push_back(sc->bvh.nodes);
         if (sc->bvh.leaf) sc->allocations.push_back(sc->bvh.leaf);
         DevScene& S = sc->dev;
@@ -740,16 +766,13 @@ void scene_builder_release(fm_ctx* ctx)
         cudaStreamDestroy(s);
     }
     for (cudaEvent_t e : ctx->build_events) cudaEventDestroy(e);
-    for (cudaEvent_t e : ctx->stage_events) {
-        cudaEventSynchronize(e);
-        cudaEventDestroy(e);
-    }
-    if (ctx->stage) cudaFreeHost(ctx->stage);
+    if (ctx->capture_stream) cudaStreamDestroy(ctx->capture_stream);
+    ctx->capture_stream = nullptr;
     ctx->build_streams.clear();
     ctx->build_events.clear();
-    ctx->stage_events.clear();
-    ctx->stage = nullptr;
-    ctx->stage_bytes = 0;
+    if (ctx->build_counters) cudaFreeHost(ctx->build_counters);
+    ctx->build_counters = nullptr;
+    ctx->build_counters_cap = 0;
 }
 
 }  // namespace fm
