@@ -84,13 +84,22 @@ FM_D void intersect_node(const uint4* __restrict__ nodes, int node, f3 o, f3 idi
     for (int i = 0; i < 8; ++i) {
         const uint32_t wm = i < 4 ? w1.z : w1.w;
         const uint32_t meta = (wm >> (8 * (i & 3))) & 0xffu;
-        if (meta == 0) continue;
         const int k = i & 3;
         const float txn = fmaf(byte_f(i < 4 ? nx0 : nx1, k), ax, bx), txf = fmaf(byte_f(i < 4 ? fx0 : fx1, k), ax, bx);
         const float tyn = fmaf(byte_f(i < 4 ? ny0 : ny1, k), ay, by), tyf = fmaf(byte_f(i < 4 ? fy0 : fy1, k), ay, by);
         const float tzn = fmaf(byte_f(i < 4 ? nz0 : nz1, k), az, bz), tzf = fmaf(byte_f(i < 4 ? fz0 : fz1, k), az, bz);
-        const float tn = fmaxf(fmaxf(txn, tyn), fmaxf(tzn, tmin));
-        const float tf = fminf(fminf(txf, tyf), fminf(tzf, tfar_limit));
+        // The slab interval with three-input integer min / max on the float bits (one
+        // instruction each instead of two float ones).  Signed-integer order is float
+        // order among non-negative floats and puts every negative float below them, so
+        // tn, a maximum that includes tmin >= 0, is the float maximum exactly; tf is the
+        // float minimum when it is non-negative and otherwise some negative candidate,
+        // which rejects the box just as the float minimum does (tn >= 0) except within
+        // 1e-30 of zero, where it can only accept a box more -- never reject one.
+        // An empty slot (meta 0) needs no branch: its bits below are zero.
+        const float tn = __int_as_float(__vimax3_s32(__float_as_int(txn), __float_as_int(tyn),
+                                                     max(__float_as_int(tzn), __float_as_int(tmin))));
+        const float tf = __int_as_float(__vimin3_s32(__float_as_int(txf), __float_as_int(tyf),
+                                                     min(__float_as_int(tzf), __float_as_int(tfar_limit))));
         // Widen the interval by a few ulps so that rounding in the slab arithmetic can
         // never reject a box that the exact box test accepts.
         if (tn <= tf * 1.0000010f + 1e-30f) {

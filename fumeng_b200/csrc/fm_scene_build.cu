@@ -45,7 +45,7 @@ void launch_rgb_to_texels(cudaStream_t stream, const float* src, float4* dst, si
 
 namespace {
 
-constexpr int kBuildStreams = 8;   // scenes whose device work runs side by side
+constexpr int kBuildStreams = 16;   // scenes whose device work runs side by side
 constexpr size_t kAlign = 256;     // sub-array alignment inside a scene's block
 
 size_t align_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }

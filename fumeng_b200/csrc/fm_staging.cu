@@ -132,22 +132,6 @@ void staging_release(fm_ctx* ctx)
     ctx->copy_pool = nullptr;
 }
 
-void host_copy(fm_ctx* ctx, void* dst, const void* src, size_t bytes)
-{
-    constexpr size_t kSlice = size_t(1) << 20;
-    CopyPool* pool = ctx->copy_pool;
-    if (!pool || pool->size() == 1 || bytes < kSlice) {
-        std::memcpy(dst, src, bytes);
-        return;
-    }
-    const int tasks = (int)std::min<size_t>((bytes + kSlice - 1) / kSlice, (size_t)pool->size());
-    const size_t per = ((bytes + tasks - 1) / tasks + 63) & ~size_t(63);
-    pool->run(tasks, [&](int i) {
-        const size_t a = std::min(bytes, per * (size_t)i), b = std::min(bytes, a + per);
-        if (b > a) std::memcpy(static_cast<char*>(dst) + a, static_cast<const char*>(src) + a, b - a);
-    });
-}
-
 void host_parallel(fm_ctx* ctx, int tasks, const std::function<void(int)>& fn)
 {
     if (tasks <= 0) return;
@@ -158,10 +142,41 @@ void host_parallel(fm_ctx* ctx, int tasks, const std::function<void(int)>& fn)
     ctx->copy_pool->run(tasks, fn);
 }
 
+void copy_segments(fm_ctx* ctx, const std::vector<Segment>& segs)
+{
+    size_t total = 0;
+    for (const Segment& g : segs) total += g.bytes;
+    constexpr size_t kSlice = size_t(256) << 10;
+    CopyPool* pool = ctx->copy_pool;
+    const int tasks = pool ? (int)std::min<size_t>((total + kSlice - 1) / kSlice, (size_t)pool->size()) : 1;
+    if (tasks <= 1) {
+        for (const Segment& g : segs) std::memcpy(g.dst, g.src, g.bytes);
+        return;
+    }
+    const size_t per = (total + tasks - 1) / tasks;
+    pool->run(tasks, [&](int i) {
+        // bytes [a, b) of the concatenated segments
+        const size_t a = per * (size_t)i, b = std::min(total, a + per);
+        size_t pos = 0;
+        for (const Segment& g : segs) {
+            const size_t lo = std::max(a, pos), hi = std::min(b, pos + g.bytes);
+            if (lo < hi)
+                std::memcpy(static_cast<char*>(g.dst) + (lo - pos), static_cast<const char*>(g.src) + (lo - pos), hi - lo);
+            pos += g.bytes;
+            if (pos >= b) break;
+        }
+    });
+}
+
 void Stager::flush()
 {
-    if (run_len && err == cudaSuccess) err = cudaMemcpyAsync(run_dst, run_src, run_len, cudaMemcpyHostToDevice, s);
-    run_len = 0;
+    if (!host.empty()) {
+        copy_segments(ctx, host);
+        host.clear();
+    }
+    for (const Segment& g : device)
+        if (err == cudaSuccess) err = cudaMemcpyAsync(g.dst, g.src, g.bytes, cudaMemcpyHostToDevice, s);
+    device.clear();
 }
 
 // Closes the current chunk (its copies are issued) and waits until the next chunk's
@@ -184,21 +199,17 @@ void Stager::put(void* dst_dev, const void* src_host, size_t bytes)
         if (err != cudaSuccess) return;
         const size_t k = std::min(bytes, kStageChunk - used);
         char* h = ctx->stage + (size_t)chunk * kStageChunk + used;
-        host_copy(ctx, h, src, k);
-        if (run_len && run_dst + run_len == dst && run_src + run_len == h) {
-            run_len += k;
-        } else {
-            flush();
-            run_dst = dst;
-            run_src = h;
-            run_len = k;
-        }
+        host.push_back(Segment{h, src, k});
+        Segment* last = device.empty() ? nullptr : &device.back();
+        if (last && static_cast<char*>(last->dst) + last->bytes == dst &&
+            static_cast<const char*>(last->src) + last->bytes == h)
+            last->bytes += k;
+        else
+            device.push_back(Segment{dst, h, k});
         used += k;
         dst += k;
         src += k;
         bytes -= k;
-        // a full chunk goes to the copy engine now, not when the next one is needed
-        if (used == kStageChunk) flush();
     }
 }
 
@@ -225,7 +236,9 @@ cudaError_t copy_out(fm_ctx* ctx, cudaStream_t s, const std::vector<OutCopy>& co
         cudaError_t r = cudaEventSynchronize(ctx->stage_events[k]);
         if (r != cudaSuccess) return r;
         const char* base = ctx->stage + (size_t)k * kStageChunk;
-        for (const Part& p : pending[k]) host_copy(ctx, p.dst, base + p.off, p.bytes);
+        std::vector<Segment> segs;
+        for (const Part& p : pending[k]) segs.push_back(Segment{p.dst, base + p.off, p.bytes});
+        copy_segments(ctx, segs);
         pending[k].clear();
         return cudaSuccess;
     };

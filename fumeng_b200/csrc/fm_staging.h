@@ -2,7 +2,7 @@
 //
 // Pageable cudaMemcpyAsync serialises the host with the stream and copies through the
 // driver's own bounce buffer; the ring instead lets the host fill (or drain) one 8 MiB
-// chunk while the copy engine moves another, and host-side copies of large chunks are
+// chunk while the copy engine moves another, and the host-side copies of a chunk are
 // split over a few worker threads.
 #pragma once
 #include <cuda_runtime.h>
@@ -25,31 +25,39 @@ class CopyPool;
 cudaError_t staging_ensure(fm_ctx* ctx);
 void staging_release(fm_ctx* ctx);
 
-// memcpy split over the context's copy threads (plain memcpy below 1 MiB).
-void host_copy(fm_ctx* ctx, void* dst, const void* src, size_t bytes);
-
 // Runs fn(0 .. tasks-1) on the context's copy threads and the caller (serially without
 // them); returns when all are done.  fn must not throw.
 void host_parallel(fm_ctx* ctx, int tasks, const std::function<void(int)>& fn);
 
-// Host -> device: bytes bound for consecutive device addresses go as one copy.
+// One host-side copy of a batch (see copy_segments).
+struct Segment {
+    void* dst;
+    const void* src;
+    size_t bytes;
+};
+
+// Copies every segment, the bytes split evenly over the context's copy threads.
+void copy_segments(fm_ctx* ctx, const std::vector<Segment>& segs);
+
+// Host -> device through the ring, on one stream.  Host bytes are gathered into the ring
+// when a chunk is closed (one parallel copy for all the pieces in it), and bytes bound for
+// consecutive device addresses go as one cudaMemcpyAsync.
 struct Stager {
     fm_ctx* ctx;
     cudaStream_t s;
     int chunk = -1;
     size_t used = kStageChunk;
-    char* run_dst = nullptr;
-    const char* run_src = nullptr;
-    size_t run_len = 0;
+    std::vector<Segment> host;      // pending host -> ring copies
+    std::vector<Segment> device;    // pending ring -> device copies (dst = device)
     cudaError_t err = cudaSuccess;
 
     Stager(fm_ctx* c, cudaStream_t stream) : ctx(c), s(stream) {}
-    // Copies `bytes` from host memory to `dst_dev` (stream-ordered on `s`); the host
-    // buffer may be reused as soon as this returns.
+    // Queues a copy of `bytes` from host memory to `dst_dev` (stream-ordered on `s`); the
+    // host memory must stay valid until the next flush() or close().
     void put(void* dst_dev, const void* src_host, size_t bytes);
-    // Issues the pending copy.
+    // Performs the queued host copies and issues the device copies.
     void flush();
-    // Issues what is pending and marks the current chunk busy until its copies finish.
+    // flush(), then marks the current chunk busy until its copies finish.
     void close();
 
 private:
