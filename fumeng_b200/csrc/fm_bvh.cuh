@@ -70,7 +70,7 @@ FM_D void intersect_node(const uint4* __restrict__ nodes, int node, f3 o, f3 idi
     const float bx = (px - o.x) * idir.x;
     const float by = (py - o.y) * idir.y;
     const float bz = (pz - o.z) * idir.z;
-    uint32_t nbits = 0, pbits = 0;
+    uint32_t nbits = 0, pbits = 0, hmask = 0;
     const float tfar_limit = tmax;
     // Near and far planes per axis chosen once per node from the ray's direction signs
     // (t = q a + b grows with q when a = 2^e / d >= 0), so the per-child slab test needs
@@ -102,13 +102,17 @@ FM_D void intersect_node(const uint4* __restrict__ nodes, int node, f3 o, f3 idi
                                                      min(__float_as_int(tzf), __float_as_int(tfar_limit))));
         // Widen the interval by a few ulps so that rounding in the slab arithmetic can
         // never reject a box that the exact box test accepts.
-        if (tn <= tf * 1.0000010f + 1e-30f) {
-            if ((imask >> i) & 1u)
-                nbits |= 1u << (24 + (i ^ oct));
-            else
-                pbits |= (meta >> 5) << (meta & 31u);
-        }
+        const bool hit = tn <= tf * 1.0000010f + 1e-30f;
+        hmask |= hit ? 1u << i : 0u;
+        pbits |= hit && !((imask >> i) & 1u) ? (meta >> 5) << (meta & 31u) : 0u;
     }
+    // internal children hit, re-keyed slot -> slot ^ oct (three conditional swaps of
+    // bit groups instead of a shift per child)
+    uint32_t m = hmask & imask;
+    if (oct & 1u) m = ((m & 0x55u) << 1) | ((m >> 1) & 0x55u);
+    if (oct & 2u) m = ((m & 0x33u) << 2) | ((m >> 2) & 0x33u);
+    if (oct & 4u) m = ((m & 0x0fu) << 4) | ((m >> 4) & 0x0fu);
+    nbits = m << 24;
     child_base = w1.x;
     prim_base = w1.y;
     node_bits = nbits | imask;
@@ -123,7 +127,10 @@ FM_D void intersect_node(const uint4* __restrict__ nodes, int node, f3 o, f3 idi
 FM_D bool test_prim(const TraceScene& S, const RayPre& rp, f3 o, f3 d, int slot, float tmin, float& tbest,
                     Hit& hit, bool any)
 {
+    // all three records at once (a sphere's slot has them too), so the loads overlap
     const float4 a = __ldg(S.leaf + 3 * (size_t)slot);
+    const float4 b = __ldg(S.leaf + 3 * (size_t)slot + 1);
+    const float4 c = __ldg(S.leaf + 3 * (size_t)slot + 2);
     const uint32_t tag = __float_as_uint(a.w);
     if (tag & kSphereFlag) {
         const int sidx = (int)__float_as_uint(a.x);
@@ -138,8 +145,6 @@ FM_D bool test_prim(const TraceScene& S, const RayPre& rp, f3 o, f3 d, int slot,
         }
         return true;
     }
-    const float4 b = __ldg(S.leaf + 3 * (size_t)slot + 1);
-    const float4 c = __ldg(S.leaf + 3 * (size_t)slot + 2);
     float t, b0, b1, b2;
     if (!intersect_triangle(rp, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, f3{c.x, c.y, c.z}, tmin, tbest, t, b0, b1, b2))
         return false;

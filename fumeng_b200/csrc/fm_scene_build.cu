@@ -698,8 +698,19 @@ fm_status create_scenes(fm_ctx* ctx, int32_t n, const fm_scene_desc* const* desc
         }
         for (size_t t = 0; t < B.tex_pieces.size(); ++t)
             sc->textures[t].texels = reinterpret_cast<const float4*>(B.d_block + B.tex_pieces[t].off);
-        for (const Piece& p : B.pieces) stager.put(B.d_block + p.off, p.src, p.bytes);
-        for (const TexPiece& t : B.tex_pieces) stager.put(B.d_rgb + t.rgb_off, t.src, t.texels * 3 * sizeof(float));
+        // pieces of a block (and of the RGB staging) that only alignment padding separates
+        // go to the device as one copy; the float4 texel regions in between are not copied
+        auto padding = [](size_t end, size_t off) { return off - end < kAlign ? off - end : 0; };
+        size_t end = sizeof(DevScene);
+        for (const Piece& p : B.pieces) {
+            stager.put(B.d_block + p.off, p.src, p.bytes, padding(end, p.off));
+            end = p.off + p.bytes;
+        }
+        end = 0;
+        for (const TexPiece& t : B.tex_pieces) {
+            stager.put(B.d_rgb + t.rgb_off, t.src, t.texels * 3 * sizeof(float), padding(end, t.rgb_off));
+            end = t.rgb_off + t.texels * 3 * sizeof(float);
+        }
         stager.flush();
         if (stager.err != cudaSuccess) return fail_cuda(stager.err, "scene upload");
         // the scene's device work follows its copies, on its builder stream

@@ -190,10 +190,21 @@ void Stager::next_chunk()
     used = 0;
 }
 
-void Stager::put(void* dst_dev, const void* src_host, size_t bytes)
+void Stager::put(void* dst_dev, const void* src_host, size_t bytes, size_t pad_before)
 {
     char* dst = static_cast<char*>(dst_dev);
     const char* src = static_cast<const char*>(src_host);
+    if (pad_before && !device.empty() && used < kStageChunk) {
+        Segment& last = device.back();
+        char* end = static_cast<char*>(last.dst) + last.bytes;
+        const size_t gap = (size_t)(dst - end);
+        if (dst >= end && gap <= pad_before && static_cast<const char*>(last.src) + last.bytes ==
+                                                   ctx->stage + (size_t)chunk * kStageChunk + used &&
+            used + gap < kStageChunk) {
+            used += gap;
+            last.bytes += gap;
+        }
+    }
     while (bytes > 0 && err == cudaSuccess) {
         if (used == kStageChunk) next_chunk();
         if (err != cudaSuccess) return;

@@ -53,8 +53,11 @@ struct Stager {
 
     Stager(fm_ctx* c, cudaStream_t stream) : ctx(c), s(stream) {}
     // Queues a copy of `bytes` from host memory to `dst_dev` (stream-ordered on `s`); the
-    // host memory must stay valid until the next flush() or close().
-    void put(void* dst_dev, const void* src_host, size_t bytes);
+    // host memory must stay valid until the next flush() or close().  `pad_before` device
+    // bytes just below dst_dev are free padding of the same allocation: when the previous
+    // copy ends within them, the ring is padded alike and the two copies become one (the
+    // padding receives unspecified bytes).
+    void put(void* dst_dev, const void* src_host, size_t bytes, size_t pad_before = 0);
     // Performs the queued host copies and issues the device copies.
     void flush();
     // flush(), then marks the current chunk busy until its copies finish.

@@ -72,17 +72,21 @@ FM_D float edge_double(float ax, float ay, float bx, float by)
 // reference's rejection test (t <= tmin || t >= tmax) lets a NaN t through; here a NaN
 // t is rejected as well (it arises only from degenerate input, never on a ray the
 // reference handles with finite arithmetic).
-FM_D bool intersect_triangle(const RayPre& r, f3 v0, f3 v1, f3 v2, float tmin, float tmax, float& t_out,
-                             float& b0, float& b1, float& b2)
+template <bool IDENTITY>
+FM_D bool intersect_triangle_p(const RayPre& r, f3 v0, f3 v1, f3 v2, float tmin, float tmax, float& t_out,
+                               float& b0, float& b1, float& b2)
 {
     // translate
     v0 = f3{__fsub_rn(v0.x, r.o.x), __fsub_rn(v0.y, r.o.y), __fsub_rn(v0.z, r.o.z)};
     v1 = f3{__fsub_rn(v1.x, r.o.x), __fsub_rn(v1.y, r.o.y), __fsub_rn(v1.z, r.o.z)};
     v2 = f3{__fsub_rn(v2.x, r.o.x), __fsub_rn(v2.y, r.o.y), __fsub_rn(v2.z, r.o.z)};
     // permute
-    float p0x = comp(v0, r.kx), p0y = comp(v0, r.ky), p0z = comp(v0, r.kz);
-    float p1x = comp(v1, r.kx), p1y = comp(v1, r.ky), p1z = comp(v1, r.kz);
-    float p2x = comp(v2, r.kx), p2y = comp(v2, r.ky), p2z = comp(v2, r.kz);
+    float p0x = IDENTITY ? v0.x : comp(v0, r.kx), p0y = IDENTITY ? v0.y : comp(v0, r.ky);
+    float p0z = IDENTITY ? v0.z : comp(v0, r.kz);
+    float p1x = IDENTITY ? v1.x : comp(v1, r.kx), p1y = IDENTITY ? v1.y : comp(v1, r.ky);
+    float p1z = IDENTITY ? v1.z : comp(v1, r.kz);
+    float p2x = IDENTITY ? v2.x : comp(v2, r.kx), p2y = IDENTITY ? v2.y : comp(v2, r.ky);
+    float p2z = IDENTITY ? v2.z : comp(v2, r.kz);
     // shear
     p0x = __fadd_rn(p0x, __fmul_rn(r.sx, p0z));
     p0y = __fadd_rn(p0y, __fmul_rn(r.sy, p0z));
@@ -113,6 +117,16 @@ FM_D bool intersect_triangle(const RayPre& r, f3 v0, f3 v1, f3 v2, float tmin, f
     b1 = __fmul_rn(e1, inv_det);
     b2 = __fmul_rn(e2, inv_det);
     return true;
+}
+
+// The permutation is the identity (x, y, z) whenever z is the main axis, which the
+// truncating main-axis choice makes it for almost every ray; that case skips the
+// per-component selects.
+FM_D bool intersect_triangle(const RayPre& r, f3 v0, f3 v1, f3 v2, float tmin, float tmax, float& t_out,
+                             float& b0, float& b1, float& b2)
+{
+    if (r.kz == 2) return intersect_triangle_p<true>(r, v0, v1, v2, tmin, tmax, t_out, b0, b1, b2);
+    return intersect_triangle_p<false>(r, v0, v1, v2, tmin, tmax, t_out, b0, b1, b2);
 }
 
 // Sphere::IntersectSphere (geometry/sphere.cpp:91-129, GetCoef :206-212): the ray is
