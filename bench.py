@@ -46,9 +46,9 @@ METRIC = "Mpaths/s batched wavefront vs plain megakernel at relMSE≤1e-3; adjoi
 WORKLOAD = "batched: 64 scenes x (1-40 displaced icosphere/box meshes, 1k-200k tris), 512x256 HDR env + 1 area light, 128^2-512^2, 4-64 spp, depth 8"
 NSCENES = 64
 # DRAM bytes the trace kernel moves per traced ray (read + write, cold L2 at each
-# launch), from an ncu capture of trace launches of the 8-scene case of this workload;
-# traffic grows with the rays a launch traces.
-TRACE_DRAM_BYTES_PER_RAY = 80.4
+# launch), from an ncu capture of two trace launches of the 8-scene case of this
+# workload (69.0 and 64.0 B per ray); traffic grows with the rays a launch traces.
+TRACE_DRAM_BYTES_PER_RAY = 66.5
 
 
 def measured_peak_hbm():
