@@ -29,7 +29,7 @@ struct fm_ctx {
     // scene creation: streams that build scenes side by side
     std::vector<cudaStream_t> build_streams;
     std::vector<cudaEvent_t> build_events;
-    cudaStream_t capture_stream = nullptr;   // BVH build graphs are captured here, never run
+    std::vector<cudaStream_t> capture_streams;   // one per BVH issuer: graphs are captured there, never run
     int32_t* build_counters = nullptr;   // pinned, 16 per scene of the largest batch
     int64_t build_counters_cap = 0;
     // pinned staging ring for host <-> device transfers (fm_staging.h): kStageChunks

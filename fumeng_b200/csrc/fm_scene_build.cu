@@ -46,6 +46,7 @@ void launch_rgb_to_texels(cudaStream_t stream, const float* src, float4* dst, si
 namespace {
 
 constexpr int kBuildStreams = 16;   // scenes whose device work runs side by side
+constexpr int kIssuers = 1;         // threads issuing BVH builds (more did not shorten a batch: the builds' device time bounds it)
 constexpr size_t kAlign = 256;     // sub-array alignment inside a scene's block
 
 size_t align_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
@@ -510,12 +511,12 @@ fm_status prepare_scene(const fm_scene_desc* d, SceneBuild& B)
 fm_status ensure_builder(fm_ctx* ctx)
 {
     if (ctx->build_streams.empty()) {
-        // streams [0, kBuildStreams) run builds, the last one only captures their graphs;
-        // events: [0] a scene's arrays are on the device, [1 + k] builder stream k is done
+        // streams: kBuildStreams run builds, kIssuers only capture their graphs; events:
+        // [0] a scene's arrays are on the device, [1 + k] builder stream k is done
         std::vector<cudaStream_t> streams;
         std::vector<cudaEvent_t> events;
         cudaError_t e = cudaSuccess;
-        for (int k = 0; k <= kBuildStreams && e == cudaSuccess; ++k) {
+        for (int k = 0; k < kBuildStreams + kIssuers && e == cudaSuccess; ++k) {
             cudaStream_t s = nullptr;
             e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
             if (e == cudaSuccess) streams.push_back(s);
@@ -530,8 +531,8 @@ fm_status ensure_builder(fm_ctx* ctx)
             for (cudaEvent_t ev : events) cudaEventDestroy(ev);
             return cuda_error(ctx, e, "scene builder streams");
         }
-        ctx->capture_stream = streams.back();
-        streams.pop_back();
+        ctx->capture_streams.assign(streams.begin() + kBuildStreams, streams.end());
+        streams.resize(kBuildStreams);
         ctx->build_streams = streams;
         ctx->build_events = events;
     }
@@ -557,14 +558,16 @@ void discard(fm_ctx* ctx, std::vector<SceneBuild>& builds)
     cudaGetLastError();
 }
 
-// Issues the BVH builds on a thread of their own, in scene order, as the main thread
-// hands scenes over; the host cost of a build (allocations, graph capture and
-// instantiation) then overlaps the main thread's uploads.
+// Issues the BVH builds from threads of their own, scenes taken in hand-over order, as
+// the main thread hands them over; the host cost of a build (allocations, graph capture
+// and instantiation, about half a millisecond) then overlaps the main thread's uploads
+// and the other issuers' builds.  Each issuer captures on a stream of its own.
 class BvhIssuer {
 public:
     BvhIssuer(fm_ctx* ctx, std::vector<SceneBuild>& builds) : ctx_(ctx), builds_(builds)
     {
-        thread_ = std::thread([this] { loop(); });
+        for (size_t t = 0; t < ctx->capture_streams.size(); ++t)
+            threads_.emplace_back([this, t] { loop(ctx_->capture_streams[t]); });
     }
     ~BvhIssuer() { finish(); }
     void hand_over(int i, cudaStream_t s)
@@ -577,32 +580,30 @@ public:
     // one failed (the later ones are then not issued).
     bool finish()
     {
-        if (thread_.joinable()) {
-            {
-                std::lock_guard<std::mutex> lk(m_);
-                closed_ = true;
-            }
-            cv_.notify_one();
-            thread_.join();
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            closed_ = true;
         }
+        cv_.notify_all();
+        for (auto& t : threads_)
+            if (t.joinable()) t.join();
         return err_.empty();
     }
     const std::string& error() const { return err_; }
 
 private:
-    void loop()
+    void loop(cudaStream_t capture)
     {
         cudaSetDevice(ctx_->device);
-        size_t next = 0;
         for (;;) {
             std::pair<int, cudaStream_t> job;
             {
                 std::unique_lock<std::mutex> lk(m_);
-                cv_.wait(lk, [&] { return closed_ || next < queue_.size(); });
-                if (next == queue_.size()) return;
-                job = queue_[next++];
+                cv_.wait(lk, [&] { return closed_ || next_ < queue_.size(); });
+                if (next_ == queue_.size()) return;
+                job = queue_[next_++];
+                if (!err_.empty()) continue;
             }
-            if (!err_.empty()) continue;
             SceneBuild& B = builds_[(size_t)job.first];
             const DevScene& S = B.sc->dev;
             PrimSource src;
@@ -613,17 +614,19 @@ private:
             src.rects = S.rects;
             src.spheres = S.spheres;
             std::string err;
-            if (bvh_build_begin(job.second, ctx_->capture_stream, src, B.h_counters, ctx_->num_sms, B.job, B.sc->bvh,
-                                err) != 0)
-                err_ = err.empty() ? std::string("bvh build failed") : err;
+            if (bvh_build_begin(job.second, capture, src, B.h_counters, ctx_->num_sms, B.job, B.sc->bvh, err) != 0) {
+                std::lock_guard<std::mutex> lk(m_);
+                if (err_.empty()) err_ = err.empty() ? std::string("bvh build failed") : err;
+            }
         }
     }
     fm_ctx* ctx_;
     std::vector<SceneBuild>& builds_;
-    std::thread thread_;
+    std::vector<std::thread> threads_;
     std::mutex m_;
     std::condition_variable cv_;
     std::vector<std::pair<int, cudaStream_t>> queue_;
+    size_t next_ = 0;
     bool closed_ = false;
     std::string err_;
 };
@@ -777,8 +780,8 @@ void scene_builder_release(fm_ctx* ctx)
         cudaStreamDestroy(s);
     }
     for (cudaEvent_t e : ctx->build_events) cudaEventDestroy(e);
-    if (ctx->capture_stream) cudaStreamDestroy(ctx->capture_stream);
-    ctx->capture_stream = nullptr;
+    for (cudaStream_t s : ctx->capture_streams) cudaStreamDestroy(s);
+    ctx->capture_streams.clear();
     ctx->build_streams.clear();
     ctx->build_events.clear();
     if (ctx->build_counters) cudaFreeHost(ctx->build_counters);
