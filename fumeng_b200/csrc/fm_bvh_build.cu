@@ -15,6 +15,7 @@
 #include "fm_bvh_build.h"
 
 #include <algorithm>
+#include <cstring>
 #include <new>
 #include <vector>
 
@@ -56,6 +57,28 @@ struct Split {
     int32_t child_task[2];   // -1 when the child is a small cluster
 };
 
+// A scene of a batched build: its primitives are positions [begin, begin + count) of the
+// batch, its root is binary and wide node `root` (-1 for an empty scene).
+struct BatchScene {
+    PrimSource src;
+    int32_t begin, count, root, pad;
+};
+
+// The scene of batch position g: the last scene that begins at or before g (empty scenes
+// share their begin with the next one and are skipped by taking the last).
+FM_D int scene_of(const BatchScene* __restrict__ scenes, int nscenes, int g)
+{
+    int lo = 0, hi = nscenes - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (scenes[mid].begin <= g)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
 FM_D int bin_of(float c, float cmin, float scale)
 {
     int b = (int)((c - cmin) * scale);
@@ -94,39 +117,54 @@ __global__ void k_init_bins(Bins* bins, const int32_t* ntasks_p)
     }
 }
 
-// Root-bounds accumulator before k_root_bounds: minima at +inf bits, maxima at 0
-// (orderable-uint encoding of the bounds).
-__global__ void k_init_root_bounds(uint32_t* rb)
+// Root-bounds accumulators (12 per scene) before k_root_bounds: minima at +inf bits,
+// maxima at 0 (orderable-uint encoding of the bounds).
+__global__ void k_init_root_bounds(uint32_t* rb, int nscenes)
 {
-    const int i = threadIdx.x;
-    if (i < 12) rb[i] = (i % 6) < 3 ? 0xffffffffu : 0u;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 12 * nscenes; i += gridDim.x * blockDim.x)
+        rb[i] = (i % 6) < 3 ? 0xffffffffu : 0u;
 }
 
-__global__ void k_root_bounds(const float4* __restrict__ plo, const float4* __restrict__ phi, int n, uint32_t* out)
+// Per-scene bounds: [0..2] centroid min, [3..5] centroid max, [6..8] box min, [9..11]
+// box max, 12 words per scene.  A warp whose primitives all belong to one scene reduces
+// them first and updates once (the usual case: scenes are contiguous ranges); a warp
+// that straddles a scene boundary updates per lane.
+__global__ void k_root_bounds(const float4* __restrict__ plo, const float4* __restrict__ phi,
+                              const int32_t* __restrict__ prim_scene, int n, uint32_t* rb)
 {
-    // out: [0..2] centroid min, [3..5] centroid max, [6..8] box min, [9..11] box max
-    float cmn[3] = {kRealMax, kRealMax, kRealMax}, cmx[3] = {-kRealMax, -kRealMax, -kRealMax};
-    float bmn[3] = {kRealMax, kRealMax, kRealMax}, bmx[3] = {-kRealMax, -kRealMax, -kRealMax};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 l = plo[i], h = phi[i];
-        const float c[3] = {0.5f * (l.x + h.x), 0.5f * (l.y + h.y), 0.5f * (l.z + h.z)};
-        const float lv[3] = {l.x, l.y, l.z}, hv[3] = {h.x, h.y, h.z};
-        for (int a = 0; a < 3; ++a) {
-            cmn[a] = fminf(cmn[a], c[a]);
-            cmx[a] = fmaxf(cmx[a], c[a]);
-            bmn[a] = fminf(bmn[a], lv[a]);
-            bmx[a] = fmaxf(bmx[a], hv[a]);
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const int i = base + threadIdx.x;
+        const bool valid = i < n;
+        float cmn[3] = {kRealMax, kRealMax, kRealMax}, cmx[3] = {-kRealMax, -kRealMax, -kRealMax};
+        float bmn[3] = {kRealMax, kRealMax, kRealMax}, bmx[3] = {-kRealMax, -kRealMax, -kRealMax};
+        // lanes past the end take the last primitive's scene with empty bounds
+        const int s = prim_scene[valid ? i : n - 1];
+        if (valid) {
+            const float4 l = plo[i], h = phi[i];
+            const float lv[3] = {l.x, l.y, l.z}, hv[3] = {h.x, h.y, h.z};
+            for (int a = 0; a < 3; ++a) {
+                const float c = 0.5f * (lv[a] + hv[a]);
+                cmn[a] = cmx[a] = c;
+                bmn[a] = lv[a];
+                bmx[a] = hv[a];
+            }
         }
-    }
-    for (int a = 0; a < 3; ++a) {
-        for (int off = 16; off > 0; off >>= 1) {
-            cmn[a] = fminf(cmn[a], __shfl_xor_sync(0xffffffffu, cmn[a], off));
-            cmx[a] = fmaxf(cmx[a], __shfl_xor_sync(0xffffffffu, cmx[a], off));
-            bmn[a] = fminf(bmn[a], __shfl_xor_sync(0xffffffffu, bmn[a], off));
-            bmx[a] = fmaxf(bmx[a], __shfl_xor_sync(0xffffffffu, bmx[a], off));
+        const int s0 = __shfl_sync(0xffffffffu, s, 0);
+        if (__all_sync(0xffffffffu, s == s0)) {
+            for (int a = 0; a < 3; ++a) {
+                for (int off = 16; off > 0; off >>= 1) {
+                    cmn[a] = fminf(cmn[a], __shfl_xor_sync(0xffffffffu, cmn[a], off));
+                    cmx[a] = fmaxf(cmx[a], __shfl_xor_sync(0xffffffffu, cmx[a], off));
+                    bmn[a] = fminf(bmn[a], __shfl_xor_sync(0xffffffffu, bmn[a], off));
+                    bmx[a] = fmaxf(bmx[a], __shfl_xor_sync(0xffffffffu, bmx[a], off));
+                }
+            }
+            if ((threadIdx.x & 31) != 0) continue;
+        } else if (!valid) {
+            continue;
         }
-    }
-    if ((threadIdx.x & 31) == 0) {
+        uint32_t* out = rb + 12 * s;
         for (int a = 0; a < 3; ++a) {
             atomicMin(out + a, f2ord(cmn[a]));
             atomicMax(out + 3 + a, f2ord(cmx[a]));
@@ -136,45 +174,53 @@ __global__ void k_root_bounds(const float4* __restrict__ plo, const float4* __re
     }
 }
 
-__global__ void k_make_root(const uint32_t* rb, int n, BNode* nodes, Task* tasks, int32_t* pos_task,
-                            int32_t* small_list, int32_t* counters)
+// One thread per scene: the scene's root binary node (node index = the scene's root
+// index) and either a root task or, for <= kSmall primitives, a small cluster.
+__global__ void k_make_roots(const BatchScene* __restrict__ scenes, int nscenes, const uint32_t* rb, BNode* nodes,
+                             Task* tasks, int32_t* small_list, int32_t* counters, int32_t* scene_task, int nroots)
 {
     // counters: [0] node count, [1] next-level task count, [2] small-cluster count
-    BNode root;
-    for (int a = 0; a < 3; ++a) {
-        root.lo[a] = ord2f(rb[6 + a]);
-        root.hi[a] = ord2f(rb[9 + a]);
-    }
-    root.a = 0;
-    root.b = 0;
-    nodes[0] = root;
-    counters[0] = 1;
-    if (n <= kSmall) {
-        small_list[0] = 0;   // node
-        small_list[1] = 0;   // begin
-        small_list[2] = n;   // count
-        counters[2] = 1;
-        counters[1] = 0;
-    } else {
-        Task t;
-        t.node = 0;
-        t.begin = 0;
-        t.count = n;
-        t.pad = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) counters[0] = nroots;
+    for (int si = blockIdx.x * blockDim.x + threadIdx.x; si < nscenes; si += gridDim.x * blockDim.x) {
+        const BatchScene sc = scenes[si];
+        scene_task[si] = -1;
+        if (sc.count == 0) continue;
+        const uint32_t* r = rb + 12 * si;
+        BNode root;
         for (int a = 0; a < 3; ++a) {
-            t.cmin[a] = ord2f(rb[a]);
-            t.cmax[a] = ord2f(rb[3 + a]);
+            root.lo[a] = ord2f(r[6 + a]);
+            root.hi[a] = ord2f(r[9 + a]);
         }
-        tasks[0] = t;
-        counters[1] = 1;
-        counters[2] = 0;
+        root.a = 0;
+        root.b = 0;
+        nodes[sc.root] = root;
+        if (sc.count <= kSmall) {
+            const int q = atomicAdd(&counters[2], 1);
+            small_list[3 * q + 0] = sc.root;    // node
+            small_list[3 * q + 1] = sc.begin;   // begin
+            small_list[3 * q + 2] = sc.count;   // count
+        } else {
+            const int q = atomicAdd(&counters[1], 1);
+            Task t;
+            t.node = sc.root;
+            t.begin = sc.begin;
+            t.count = sc.count;
+            t.pad = 0;
+            for (int a = 0; a < 3; ++a) {
+                t.cmin[a] = ord2f(r[a]);
+                t.cmax[a] = ord2f(r[3 + a]);
+            }
+            tasks[q] = t;
+            scene_task[si] = q;
+        }
     }
 }
 
-__global__ void k_fill_pos_task(int32_t* pos_task, int32_t* pidx, int n, int root_task)
+__global__ void k_fill_pos_task(int32_t* pos_task, int32_t* pidx, const int32_t* __restrict__ prim_scene,
+                                const int32_t* __restrict__ scene_task, int n)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        pos_task[i] = root_task;
+        pos_task[i] = scene_task[prim_scene[i]];
         pidx[i] = i;
     }
 }
@@ -713,12 +759,15 @@ __global__ void k_small(const float4* __restrict__ plo, const float4* __restrict
 
 FM_D float node_area(const BNode& b) { return half_area(b.lo, b.hi); }
 
-// Collapses the binary subtree under frontier entry fi into one 8-wide node.
+// Collapses the binary subtree under frontier entry fi (binary node, wide slot, scene
+// root) into one 8-wide node.  Child bases are stored relative to the scene's root slot
+// (the scene's node array starts there); leaf slots are batch-wide.  Per scene root:
+// wide nodes, leaf slots and depth (the collapse level) go to stats[3 * root + 0..2].
 FM_D void collapse_node(const BNode* __restrict__ bnodes, const int32_t* __restrict__ pidx,
-                        const int2* __restrict__ frontier, int fi, int2* next_frontier, int32_t* counters,
-                        uint4* wnodes, int32_t* leaf_prim)
+                        const int4* __restrict__ frontier, int fi, int4* next_frontier, int32_t* counters,
+                        uint4* wnodes, int32_t* leaf_prim, int32_t* stats, int level)
 {
-    const int bn = frontier[fi].x, wslot = frontier[fi].y;
+    const int bn = frontier[fi].x, wslot = frontier[fi].y, sroot = frontier[fi].z;
     const BNode root = bnodes[bn];
     int ch[8];
     int nch = 0;
@@ -807,6 +856,9 @@ FM_D void collapse_node(const BNode* __restrict__ bnodes, const int32_t* __restr
     }
     const int child_base = n_int ? atomicAdd(&counters[0], n_int) : 0;
     const int prim_base = n_prim ? atomicAdd(&counters[1], n_prim) : 0;
+    atomicAdd(&stats[3 * sroot + 0], 1);
+    if (n_prim) atomicAdd(&stats[3 * sroot + 1], n_prim);
+    atomicMax(&stats[3 * sroot + 2], level);
     // quantization
     uint32_t e[3];
     float scale[3];
@@ -844,7 +896,7 @@ FM_D void collapse_node(const BNode* __restrict__ bnodes, const int32_t* __restr
             imask |= 1u << s;
             meta[s] = 0x20u | (uint32_t)(24 + s);   // nonzero marker; traversal uses imask
             const int q = atomicAdd(&counters[2], 1);
-            next_frontier[q] = make_int2(at_slot[s], child_base + int_rank);
+            next_frontier[q] = make_int4(at_slot[s], child_base + int_rank, sroot, 0);
             ++int_rank;
         } else {
             const int cnt = c.b, beg = ~c.a;
@@ -857,50 +909,57 @@ FM_D void collapse_node(const BNode* __restrict__ bnodes, const int32_t* __restr
     uint4* np = wnodes + 5 * (size_t)wslot;
     np[0] = make_uint4(__float_as_uint(lo[0]), __float_as_uint(lo[1]), __float_as_uint(lo[2]),
                        e[0] | (e[1] << 8) | (e[2] << 16) | (imask << 24));
-    np[1] = make_uint4((uint32_t)child_base, (uint32_t)prim_base, pack4(meta), pack4(meta + 4));
+    np[1] = make_uint4(n_int ? (uint32_t)(child_base - sroot) : 0u, (uint32_t)prim_base, pack4(meta), pack4(meta + 4));
     np[2] = make_uint4(pack4(ql[0]), pack4(ql[0] + 4), pack4(ql[1]), pack4(ql[1] + 4));
     np[3] = make_uint4(pack4(ql[2]), pack4(ql[2] + 4), pack4(qh[0]), pack4(qh[0] + 4));
     np[4] = make_uint4(pack4(qh[1]), pack4(qh[1] + 4), pack4(qh[2]), pack4(qh[2] + 4));
 }
 
 __global__ void k_collapse(const BNode* __restrict__ bnodes, const int32_t* __restrict__ pidx,
-                           const int2* __restrict__ frontier, const int32_t* nfront_p, int2* next_frontier,
-                           int32_t* counters, uint4* wnodes, int32_t* leaf_prim)
+                           const int4* __restrict__ frontier, const int32_t* nfront_p, int4* next_frontier,
+                           int32_t* counters, uint4* wnodes, int32_t* leaf_prim, int32_t* stats)
 {
-    // counters: [0] wide node count, [1] leaf slot count, [2] next frontier count
+    // counters: [0] wide node count, [1] leaf slot count, [2] next frontier count, [4] level
     const int nfront = *nfront_p;
+    const int level = counters[4];
     for (int fi = blockIdx.x * blockDim.x + threadIdx.x; fi < nfront; fi += gridDim.x * blockDim.x)
-        collapse_node(bnodes, pidx, frontier, fi, next_frontier, counters, wnodes, leaf_prim);
+        collapse_node(bnodes, pidx, frontier, fi, next_frontier, counters, wnodes, leaf_prim, stats, level);
 }
 
-__global__ void k_fill_leaf(const int32_t* __restrict__ leaf_prim, int nleaf, PrimSource src, float4* leaf)
+// Leaf records: the primitive's corners (or sphere index) and its id within its scene.
+__global__ void k_fill_leaf(const int32_t* __restrict__ leaf_prim, int nleaf, const BatchScene* __restrict__ scenes,
+                            const int32_t* __restrict__ prim_scene, int n, float4* leaf)
 {
-    const int nprim = src.num_tris + 2 * src.num_rects + src.num_spheres;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nleaf; i += gridDim.x * blockDim.x) {
-        const int p = leaf_prim[i];
+        const int g = leaf_prim[i];
         float4 a, b, c;
-        if (p < 0 || p >= nprim) {
+        if (g < 0 || g >= n) {
             // a slot the collapse did not fill (the build then reports a leaf-count error)
             a = b = c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        } else if (p < src.num_tris) {
-            const float* v = src.tri_pos + 9 * (size_t)p;
-            a = make_float4(v[0], v[1], v[2], __uint_as_float((uint32_t)p));
-            b = make_float4(v[3], v[4], v[5], 0.0f);
-            c = make_float4(v[6], v[7], v[8], 0.0f);
-        } else if (p < src.num_tris + 2 * src.num_rects) {
-            const int r = (p - src.num_tris) >> 1, h = (p - src.num_tris) & 1;
-            const RectDev& R = src.rects[r];
-            const float* q0 = h ? R.pc : R.pa;
-            const float* q1 = h ? R.pd : R.pb;
-            const float* q2 = h ? R.pa : R.pc;
-            a = make_float4(q0[0], q0[1], q0[2], __uint_as_float((uint32_t)p));
-            b = make_float4(q1[0], q1[1], q1[2], 0.0f);
-            c = make_float4(q2[0], q2[1], q2[2], 0.0f);
         } else {
-            const int s = p - src.num_tris - 2 * src.num_rects;
-            a = make_float4(__uint_as_float((uint32_t)s), 0.0f, 0.0f, __uint_as_float((uint32_t)p | kSphereFlag));
-            b = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            const BatchScene& sc = scenes[prim_scene[g]];
+            const PrimSource& src = sc.src;
+            const int p = g - sc.begin;
+            if (p < src.num_tris) {
+                const float* v = src.tri_pos + 9 * (size_t)p;
+                a = make_float4(v[0], v[1], v[2], __uint_as_float((uint32_t)p));
+                b = make_float4(v[3], v[4], v[5], 0.0f);
+                c = make_float4(v[6], v[7], v[8], 0.0f);
+            } else if (p < src.num_tris + 2 * src.num_rects) {
+                const int r = (p - src.num_tris) >> 1, h = (p - src.num_tris) & 1;
+                const RectDev& R = src.rects[r];
+                const float* q0 = h ? R.pc : R.pa;
+                const float* q1 = h ? R.pd : R.pb;
+                const float* q2 = h ? R.pa : R.pc;
+                a = make_float4(q0[0], q0[1], q0[2], __uint_as_float((uint32_t)p));
+                b = make_float4(q1[0], q1[1], q1[2], 0.0f);
+                c = make_float4(q2[0], q2[1], q2[2], 0.0f);
+            } else {
+                const int sp = p - src.num_tris - 2 * src.num_rects;
+                a = make_float4(__uint_as_float((uint32_t)sp), 0.0f, 0.0f, __uint_as_float((uint32_t)p | kSphereFlag));
+                b = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            }
         }
         leaf[3 * (size_t)i] = a;
         leaf[3 * (size_t)i + 1] = b;
@@ -908,10 +967,15 @@ __global__ void k_fill_leaf(const int32_t* __restrict__ leaf_prim, int nleaf, Pr
     }
 }
 
-__global__ void k_prim_bounds(PrimSource src, float4* plo, float4* phi)
+// Primitive boxes, and each batch position's scene.
+__global__ void k_prim_bounds(const BatchScene* __restrict__ scenes, int nscenes, int n, float4* plo, float4* phi,
+                              int32_t* prim_scene)
 {
-    const int n = src.num_tris + 2 * src.num_rects + src.num_spheres;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) {
+        const int si = scene_of(scenes, nscenes, g);
+        prim_scene[g] = si;
+        const PrimSource& src = scenes[si].src;
+        const int p = g - scenes[si].begin;
         float lo[3], hi[3];
         if (p < src.num_tris + 2 * src.num_rects) {
             f3 v[3];
@@ -939,8 +1003,8 @@ __global__ void k_prim_bounds(PrimSource src, float4* plo, float4* phi)
                 hi[a] = comp(c, a) + S.radius_world;
             }
         }
-        plo[p] = make_float4(lo[0], lo[1], lo[2], 0.0f);
-        phi[p] = make_float4(hi[0], hi[1], hi[2], 0.0f);
+        plo[g] = make_float4(lo[0], lo[1], lo[2], 0.0f);
+        phi[g] = make_float4(hi[0], hi[1], hi[2], 0.0f);
     }
 }
 
@@ -966,17 +1030,24 @@ __global__ void k_split_continue(int32_t* counters, cudaGraphConditionalHandle h
 }
 
 // Collapse phase counters: [0] wide nodes, [1] leaf slots, [2] next frontier, [3]
-// current frontier, [4] levels, [5] loop bodies run, [6] error bits.
-__global__ void k_collapse_init(int2* front, int32_t* ccnt)
+// current frontier, [4] levels, [5] loop bodies run, [6] error bits.  The first frontier
+// holds every scene's root (binary node = wide slot = the root index).
+__global__ void k_collapse_init(const BatchScene* __restrict__ scenes, int nscenes, int nroots, int4* front,
+                                int32_t* ccnt)
 {
-    front[0] = make_int2(0, 0);
-    ccnt[0] = 1;
-    ccnt[1] = 0;
-    ccnt[2] = 1;
-    ccnt[3] = 0;
-    ccnt[4] = 0;
-    ccnt[5] = 0;
-    ccnt[6] = 0;
+    for (int si = blockIdx.x * blockDim.x + threadIdx.x; si < nscenes; si += gridDim.x * blockDim.x) {
+        const int r = scenes[si].root;
+        if (r >= 0) front[r] = make_int4(r, r, r, 0);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ccnt[0] = nroots;
+        ccnt[1] = 0;
+        ccnt[2] = nroots;
+        ccnt[3] = 0;
+        ccnt[4] = 0;
+        ccnt[5] = 0;
+        ccnt[6] = 0;
+    }
 }
 
 __global__ void k_collapse_begin(int32_t* ccnt)
@@ -1019,24 +1090,28 @@ inline int grid_for(int64_t n, int block)
 
 namespace {
 
-// Buffers of one build.
+// Buffers of one build over a batch of scenes (n primitives in all).
 struct BuildBufs {
-    int n, max_tasks, ntiles, sms;
-    PrimSource src;
+    int n, max_tasks, ntiles, sms, nscenes, nroots;
+    BatchScene* scenes;
     float4 *plo, *phi;
-    int32_t *pidx, *pidx2, *pos_task, *pos_task2, *flags, *scan, *tile_sums, *small_list, *counters, *ccnt, *leaf_prim;
+    int32_t *pidx, *pidx2, *pos_task, *pos_task2, *flags, *scan, *tile_sums, *small_list, *leaf_prim;
+    int32_t *prim_scene, *scene_task;
+    int32_t* meta;   // [0..15] split counters ([8..15] collapse), then 3 stats per scene root
+    int32_t *counters, *ccnt, *stats;
     uint32_t* rb;
     BNode* bnodes;
     Task *tasks, *tasks2;
     Split* splits;
     Bins* bins;
-    int2 *front, *front2;
+    int4 *front, *front2;
     uint4* wnodes;
     float4* leaf;
 };
 
 // One split level: bins, SAH splits, stable partition of the level's primitives (in ->
-// out), and the bounds of children made by median splits.
+// out), and the bounds of children made by median splits.  Tasks never span two scenes,
+// so the level serves every scene of the batch at once.
 void split_level(cudaStream_t s, const BuildBufs& b, const int32_t* pidx_in, const int32_t* pos_in,
                  const Task* tasks_in, int32_t* pidx_out, int32_t* pos_out, Task* tasks_out)
 {
@@ -1057,11 +1132,12 @@ void split_level(cudaStream_t s, const BuildBufs& b, const int32_t* pidx_in, con
                                                  b.counters + 3, b.bnodes, tasks_out);
 }
 
-void collapse_level(cudaStream_t s, const BuildBufs& b, const int2* front_in, int2* front_out)
+void collapse_level(cudaStream_t s, const BuildBufs& b, const int4* front_in, int4* front_out)
 {
     k_collapse_begin<<<1, 1, 0, s>>>(b.ccnt);
-    k_collapse<<<grid_for((int64_t)b.n + 1, 128), 128, 0, s>>>(b.bnodes, b.pidx, front_in, b.ccnt + 3, front_out,
-                                                               b.ccnt, b.wnodes, b.leaf_prim);
+    k_collapse<<<grid_for((int64_t)b.n + b.nroots, 128), 128, 0, s>>>(b.bnodes, b.pidx, front_in, b.ccnt + 3,
+                                                                      front_out, b.ccnt, b.wnodes, b.leaf_prim,
+                                                                      b.stats);
 }
 
 // Adds a WHILE node after `dep` whose body is what `body_fn` launches on `s`.
@@ -1100,25 +1176,27 @@ cudaError_t add_captured(cudaGraph_t graph, const cudaGraphNode_t* dep, cudaStre
     return e;
 }
 
-// The whole build as one graph: root set-up, a WHILE loop of split levels (two per
-// body, so that the ping-pong buffers are fixed: after every body the partition is back
-// in pidx — a level without tasks copies it through), the small clusters, a WHILE loop
-// of collapse levels, and the leaf records.  The host waits once, at the end.
+// The whole build as one graph: root set-up for every scene, a WHILE loop of split
+// levels (two per body, so that the ping-pong buffers are fixed: after every body the
+// partition is back in pidx — a level without tasks copies it through), the small
+// clusters, a WHILE loop of collapse levels, and the leaf records.  The host waits once,
+// at the end.
 cudaError_t build_graph(cudaStream_t s, const BuildBufs& b, cudaGraph_t& graph)
 {
     cudaError_t e = cudaGraphCreate(&graph, 0);
     if (e != cudaSuccess) return e;
-    const int n = b.n;
+    const int n = b.n, ns = b.nscenes;
     cudaGraphNode_t n_pre = nullptr, n_split = nullptr, n_mid = nullptr, n_collapse = nullptr, n_post = nullptr;
     cudaGraphConditionalHandle h_split{}, h_collapse{};
     e = add_captured(graph, nullptr, s, n_pre, [&]() {
-        k_init_root_bounds<<<1, 32, 0, s>>>(b.rb);
-        cudaMemsetAsync(b.counters, 0, sizeof(int32_t) * 16, s);
+        k_init_root_bounds<<<grid_for(12 * ns, 256), 256, 0, s>>>(b.rb, ns);
+        cudaMemsetAsync(b.meta, 0, sizeof(int32_t) * (16 + 3 * (size_t)b.nroots), s);
         cudaMemsetAsync(b.leaf_prim, 0xff, sizeof(int32_t) * n, s);
-        k_prim_bounds<<<grid_for(n, 256), 256, 0, s>>>(b.src, b.plo, b.phi);
-        k_root_bounds<<<grid_for(n, 256), 256, 0, s>>>(b.plo, b.phi, n, b.rb);
-        k_make_root<<<1, 1, 0, s>>>(b.rb, n, b.bnodes, b.tasks, b.pos_task, b.small_list, b.counters);
-        k_fill_pos_task<<<grid_for(n, 256), 256, 0, s>>>(b.pos_task, b.pidx, n, n <= kSmall ? -1 : 0);
+        k_prim_bounds<<<grid_for(n, 256), 256, 0, s>>>(b.scenes, ns, n, b.plo, b.phi, b.prim_scene);
+        k_root_bounds<<<grid_for(n, 256), 256, 0, s>>>(b.plo, b.phi, b.prim_scene, n, b.rb);
+        k_make_roots<<<grid_for(ns, 128), 128, 0, s>>>(b.scenes, ns, b.rb, b.bnodes, b.tasks, b.small_list,
+                                                        b.counters, b.scene_task, b.nroots);
+        k_fill_pos_task<<<grid_for(n, 256), 256, 0, s>>>(b.pos_task, b.pidx, b.prim_scene, b.scene_task, n);
     });
     if (e != cudaSuccess) return e;
     e = add_while(graph, n_pre, s, h_split, n_split, [&](cudaGraphConditionalHandle h) {
@@ -1130,7 +1208,7 @@ cudaError_t build_graph(cudaStream_t s, const BuildBufs& b, cudaGraph_t& graph)
     e = add_captured(graph, &n_split, s, n_mid, [&]() {
         k_small<<<grid_for(n, 64), 64, 0, s>>>(b.plo, b.phi, b.pidx, b.small_list, b.counters + 2, b.bnodes,
                                                b.counters);
-        k_collapse_init<<<1, 1, 0, s>>>(b.front, b.ccnt);
+        k_collapse_init<<<grid_for(ns, 128), 128, 0, s>>>(b.scenes, ns, b.nroots, b.front, b.ccnt);
     });
     if (e != cudaSuccess) return e;
     e = add_while(graph, n_mid, s, h_collapse, n_collapse, [&](cudaGraphConditionalHandle h) {
@@ -1140,16 +1218,17 @@ cudaError_t build_graph(cudaStream_t s, const BuildBufs& b, cudaGraph_t& graph)
     });
     if (e != cudaSuccess) return e;
     return add_captured(graph, &n_collapse, s, n_post, [&]() {
-        k_fill_leaf<<<grid_for(n, 256), 256, 0, s>>>(b.leaf_prim, n, b.src, b.leaf);
+        k_fill_leaf<<<grid_for(n, 256), 256, 0, s>>>(b.leaf_prim, n, b.scenes, b.prim_scene, n, b.leaf);
     });
 }
 
-// Releases the build's temporaries (stream-ordered) and its graph.
+// Releases the build's temporaries (stream-ordered).
 void free_temporaries(cudaStream_t s, BuildBufs& b)
 {
-    void* bufs[] = {b.plo,   b.phi,      b.pidx,  b.pidx2, b.pos_task, b.pos_task2, b.flags,
-                    b.scan,  b.tile_sums, b.small_list, b.counters, b.rb, b.bnodes, b.tasks,
-                    b.tasks2, b.splits,  b.bins,  b.front, b.front2,  b.leaf_prim};
+    void* bufs[] = {b.plo,    b.phi,       b.pidx,       b.pidx2,      b.pos_task, b.pos_task2, b.flags,
+                    b.scan,   b.tile_sums, b.small_list, b.meta,       b.rb,       b.bnodes,    b.tasks,
+                    b.tasks2, b.splits,    b.bins,       b.front,      b.front2,   b.leaf_prim, b.prim_scene,
+                    b.scene_task, b.scenes};
     for (void* p : bufs)
         if (p) cudaFreeAsync(p, s);
 }
@@ -1163,57 +1242,92 @@ struct BvhJob {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    const int32_t* h_cnt = nullptr;
+    const int32_t* h_meta = nullptr;   // pinned: counters and per-root stats after the build
+    std::vector<int32_t> scene_root, scene_count;
 };
 
 namespace {
 
 // Drops a job: waits for its stream (on failure paths only), then frees everything,
-// including the result arrays when `free_out`.
-void drop_job(BvhJob* job, BvhResult& out, bool free_out)
+// including the result arrays.
+void drop_job(BvhJob* job, BvhBatch& out)
 {
     cudaGetLastError();
     cudaStreamSynchronize(job->stream);
     if (job->exec) cudaGraphExecDestroy(job->exec);
     if (job->graph) cudaGraphDestroy(job->graph);
     free_temporaries(job->stream, job->b);
-    if (free_out) {
-        if (out.nodes) cudaFreeAsync(out.nodes, job->stream);
-        if (out.leaf) cudaFreeAsync(out.leaf, job->stream);
-        cudaStreamSynchronize(job->stream);
-        out = BvhResult{};
-    }
+    if (out.nodes) cudaFreeAsync(out.nodes, job->stream);
+    if (out.leaf) cudaFreeAsync(out.leaf, job->stream);
+    cudaStreamSynchronize(job->stream);
+    out = BvhBatch{};
     if (job->ev0) cudaEventDestroy(job->ev0);
     if (job->ev1) cudaEventDestroy(job->ev1);
     delete job;
 }
 
+size_t align64(size_t x) { return (x + 63) & ~size_t(63); }
+
 }  // namespace
 
-int bvh_build_begin(cudaStream_t stream, cudaStream_t capture, const PrimSource& src, int32_t* h_counters, int sms,
-                    BvhJob*& job_out, BvhResult& out, std::string& err)
+size_t bvh_batch_pinned_bytes(int nscenes)
 {
-    const int n = src.num_tris + 2 * src.num_rects + src.num_spheres;
+    return align64(sizeof(BatchScene) * (size_t)nscenes) + sizeof(int32_t) * (16 + 3 * (size_t)nscenes);
+}
+
+int bvh_build_batch_begin(cudaStream_t stream, cudaStream_t capture, const PrimSource* srcs, int nscenes,
+                          void* h_pinned, int sms, BvhJob*& job_out, BvhBatch& out, std::string& err)
+{
     job_out = nullptr;
-    out = BvhResult{};
-    if (n == 0) return 0;
+    out = BvhBatch{};
+    out.root.assign((size_t)nscenes, -1);
+    // layout of the batch: scenes' primitives back to back, roots numbered in scene order
+    std::vector<BatchScene> table((size_t)nscenes);
+    int64_t total = 0;
+    int nroots = 0;
+    for (int i = 0; i < nscenes; ++i) {
+        const PrimSource& p = srcs[i];
+        const int64_t cnt = (int64_t)p.num_tris + 2 * (int64_t)p.num_rects + p.num_spheres;
+        BatchScene& t = table[(size_t)i];
+        t.src = p;
+        t.begin = (int32_t)total;
+        t.count = (int32_t)cnt;
+        t.root = cnt > 0 ? nroots++ : -1;
+        t.pad = 0;
+        out.root[(size_t)i] = t.root;
+        total += cnt;
+    }
+    if (total > (int64_t)0x3fffffff) {
+        err = "bvh build: too many primitives in one batch";
+        return -1;
+    }
+    if (nroots == 0) return 0;
+    const int n = (int)total;
     BvhJob* job = new (std::nothrow) BvhJob();
     if (!job) {
         err = "bvh build: host allocation failed";
         return -1;
     }
     job->stream = stream;
-    job->h_cnt = h_counters;
+    job->scene_root = out.root;
+    job->scene_count.resize((size_t)nscenes);
+    for (int i = 0; i < nscenes; ++i) job->scene_count[(size_t)i] = table[(size_t)i].count;
+    char* hp = static_cast<char*>(h_pinned);
+    std::memcpy(hp, table.data(), sizeof(BatchScene) * (size_t)nscenes);
+    job->h_meta = reinterpret_cast<const int32_t*>(hp + align64(sizeof(BatchScene) * (size_t)nscenes));
     BuildBufs& b = job->b;
     b.n = n;
-    b.src = src;
-    b.max_tasks = n / (kSmall + 1) + 2;
+    b.nscenes = nscenes;
+    b.nroots = nroots;
+    b.max_tasks = n / (kSmall + 1) + 2 + nroots;
     b.ntiles = (n + kScanTile - 1) / kScanTile;
     b.sms = sms;
-    const int max_nodes = 2 * n + 2;
+    const size_t max_nodes = 2 * (size_t)n + 2;
+    const size_t max_wide = (size_t)n + nroots + 1;
     FM_BUILD_CHECK(cudaEventCreate(&job->ev0));
     FM_BUILD_CHECK(cudaEventCreate(&job->ev1));
     FM_BUILD_CHECK(cudaEventRecord(job->ev0, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.scenes, sizeof(BatchScene) * (size_t)nscenes, stream));
     FM_BUILD_CHECK(cudaMallocAsync(&b.plo, sizeof(float4) * n, stream));
     FM_BUILD_CHECK(cudaMallocAsync(&b.phi, sizeof(float4) * n, stream));
     FM_BUILD_CHECK(cudaMallocAsync(&b.pidx, sizeof(int32_t) * n, stream));
@@ -1223,40 +1337,47 @@ int bvh_build_begin(cudaStream_t stream, cudaStream_t capture, const PrimSource&
     FM_BUILD_CHECK(cudaMallocAsync(&b.flags, sizeof(int32_t) * n, stream));
     FM_BUILD_CHECK(cudaMallocAsync(&b.scan, sizeof(int32_t) * (n + 1), stream));
     FM_BUILD_CHECK(cudaMallocAsync(&b.tile_sums, sizeof(int32_t) * (b.ntiles + 1), stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&b.small_list, sizeof(int32_t) * 3 * (n + 1), stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&b.counters, sizeof(int32_t) * 16, stream));
-    b.ccnt = b.counters + 8;
-    FM_BUILD_CHECK(cudaMallocAsync(&b.rb, sizeof(uint32_t) * 12, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.small_list, sizeof(int32_t) * 3 * max_wide, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.prim_scene, sizeof(int32_t) * n, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.scene_task, sizeof(int32_t) * nscenes, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.meta, sizeof(int32_t) * (16 + 3 * (size_t)nroots), stream));
+    b.counters = b.meta;
+    b.ccnt = b.meta + 8;
+    b.stats = b.meta + 16;
+    FM_BUILD_CHECK(cudaMallocAsync(&b.rb, sizeof(uint32_t) * 12 * (size_t)nscenes, stream));
     FM_BUILD_CHECK(cudaMallocAsync(&b.bnodes, sizeof(BNode) * max_nodes, stream));
     FM_BUILD_CHECK(cudaMallocAsync(&b.tasks, sizeof(Task) * b.max_tasks, stream));
     FM_BUILD_CHECK(cudaMallocAsync(&b.tasks2, sizeof(Task) * b.max_tasks, stream));
     FM_BUILD_CHECK(cudaMallocAsync(&b.splits, sizeof(Split) * b.max_tasks, stream));
     FM_BUILD_CHECK(cudaMallocAsync(&b.bins, sizeof(Bins) * b.max_tasks, stream));
-    // wide nodes <= binary internal nodes; leaf slots == n
-    FM_BUILD_CHECK(cudaMallocAsync(&out.nodes, sizeof(uint4) * 5 * (size_t)(n + 1), stream));
+    // wide nodes <= binary internal nodes + one root per scene; leaf slots == n
+    FM_BUILD_CHECK(cudaMallocAsync(&out.nodes, sizeof(uint4) * 5 * max_wide, stream));
     FM_BUILD_CHECK(cudaMallocAsync(&b.leaf_prim, sizeof(int32_t) * n, stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&b.front, sizeof(int2) * (n + 1), stream));
-    FM_BUILD_CHECK(cudaMallocAsync(&b.front2, sizeof(int2) * (n + 1), stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.front, sizeof(int4) * max_wide, stream));
+    FM_BUILD_CHECK(cudaMallocAsync(&b.front2, sizeof(int4) * max_wide, stream));
     FM_BUILD_CHECK(cudaMallocAsync(&out.leaf, sizeof(float4) * 3 * (size_t)n, stream));
     b.wnodes = out.nodes;
     b.leaf = out.leaf;
+    FM_BUILD_CHECK(cudaMemcpyAsync(b.scenes, hp, sizeof(BatchScene) * (size_t)nscenes, cudaMemcpyHostToDevice, stream));
     FM_BUILD_CHECK(build_graph(capture, b, job->graph));
     FM_BUILD_CHECK(cudaGraphInstantiate(&job->exec, job->graph, 0));
     FM_BUILD_CHECK(cudaGraphLaunch(job->exec, stream));
-    FM_BUILD_CHECK(cudaMemcpyAsync(h_counters, b.counters, sizeof(int32_t) * 16, cudaMemcpyDeviceToHost, stream));
+    FM_BUILD_CHECK(cudaMemcpyAsync(const_cast<int32_t*>(job->h_meta), b.meta, sizeof(int32_t) * (16 + 3 * (size_t)nroots),
+                                   cudaMemcpyDeviceToHost, stream));
     FM_BUILD_CHECK(cudaEventRecord(job->ev1, stream));
     job_out = job;
     return 0;
 fail:
-    drop_job(job, out, true);
+    drop_job(job, out);
     return -1;
 }
 
-int bvh_build_end(BvhJob* job, BvhResult& out, std::string& err)
+int bvh_build_batch_end(BvhJob* job, BvhBatch& out, std::string& err)
 {
     if (!job) return 0;
-    const int32_t* h_cnt = job->h_cnt;
-    int nwide = 0, nleaf = 0, depth = 0;
+    const int32_t* h_cnt = job->h_meta;
+    const int32_t* stats = job->h_meta + 16;
+    const int nscenes = (int)job->scene_root.size();
     FM_BUILD_CHECK(cudaEventSynchronize(job->ev1));
     if (h_cnt[5] & 1) {
         err = "bvh build: task list overflow";
@@ -1270,25 +1391,33 @@ int bvh_build_end(BvhJob* job, BvhResult& out, std::string& err)
         err = "bvh build: too many collapse levels";
         goto fail;
     }
-    nwide = h_cnt[8 + 0];
-    nleaf = h_cnt[8 + 1];
-    depth = h_cnt[8 + 4];
-    if (nleaf != job->b.n) {
+    if (h_cnt[8 + 1] != job->b.n) {
         err = "bvh build: leaf count mismatch";
         goto fail;
     }
-    if (depth >= kTraversalStack) {
-        err = "bvh build: tree deeper than the traversal stack";
-        goto fail;
+    out.num_nodes.assign((size_t)nscenes, 0);
+    out.num_leaf.assign((size_t)nscenes, 0);
+    out.depth.assign((size_t)nscenes, 0);
+    for (int i = 0; i < nscenes; ++i) {
+        const int r = job->scene_root[(size_t)i];
+        if (r < 0) continue;
+        out.num_nodes[(size_t)i] = stats[3 * r];
+        out.num_leaf[(size_t)i] = stats[3 * r + 1];
+        out.depth[(size_t)i] = stats[3 * r + 2];
+        if (out.num_leaf[(size_t)i] != job->scene_count[(size_t)i]) {
+            err = "bvh build: leaf count mismatch";
+            goto fail;
+        }
+        if (out.depth[(size_t)i] >= kTraversalStack) {
+            err = "bvh build: tree deeper than the traversal stack";
+            goto fail;
+        }
     }
     {
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, job->ev0, job->ev1);
         out.build_ms = ms;
     }
-    out.num_nodes = nwide;
-    out.num_leaf = nleaf;
-    out.depth = depth;
     cudaGraphExecDestroy(job->exec);
     cudaGraphDestroy(job->graph);
     free_temporaries(job->stream, job->b);
@@ -1297,13 +1426,13 @@ int bvh_build_end(BvhJob* job, BvhResult& out, std::string& err)
     delete job;
     return 0;
 fail:
-    drop_job(job, out, true);
+    drop_job(job, out);
     return -1;
 }
 
-void bvh_build_abort(BvhJob* job, BvhResult& out)
+void bvh_build_abort(BvhJob* job, BvhBatch& out)
 {
-    if (job) drop_job(job, out, true);
+    if (job) drop_job(job, out);
 }
 
 }  // namespace fm

@@ -139,6 +139,7 @@ fm_status fm_scene_destroy(fm_ctx* ctx, fm_scene* sc)
     if (!sc) return FM_OK;
     cudaSetDevice(ctx->device);
     for (void* p : sc->allocations) cudaFreeAsync(p, ctx->stream);
+    sc->shared_bvh.reset();   // frees the BVH arrays when no other scene of its group holds them
     cudaStreamSynchronize(ctx->stream);
     delete sc;
     return FM_OK;

@@ -1,6 +1,7 @@
 // Host-side definitions shared by the C-ABI translation units.
 #pragma once
 #include <map>
+#include <memory>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -29,9 +30,9 @@ struct fm_ctx {
     // scene creation: streams that build scenes side by side
     std::vector<cudaStream_t> build_streams;
     std::vector<cudaEvent_t> build_events;
-    std::vector<cudaStream_t> capture_streams;   // one per BVH issuer: graphs are captured there, never run
-    int32_t* build_counters = nullptr;   // pinned, 16 per scene of the largest batch
-    int64_t build_counters_cap = 0;
+    cudaStream_t capture_stream = nullptr;   // BVH build graphs are captured here, never run
+    char* build_pinned = nullptr;            // BVH builds' scene tables and counters (pinned)
+    size_t build_pinned_bytes = 0;
     // pinned staging ring for host <-> device transfers (fm_staging.h): kStageChunks
     // chunks, an event per chunk, and the host copy threads
     char* stage = nullptr;
@@ -43,6 +44,7 @@ struct fm_scene {
     fm::DevScene dev{};               // device pointers filled in
     fm::DevScene* d_dev = nullptr;    // device copy of `dev` (for batched kernels)
     std::vector<void*> allocations;   // everything to cudaFree on destroy
+    std::shared_ptr<void> shared_bvh;  // BVH arrays shared with the scenes built alongside
     fm::BvhResult bvh;
     int64_t num_objects = 0;
     // host copies kept for validation and light sampling set-up

@@ -2,20 +2,19 @@
 // environment tables and its BVH built on the device.
 //
 // Many scenes are created in one call (fm_scene_create_batch).  The host prepares every
-// scene first (validation, derived arrays, light tables, the block's layout); then each
-// scene's arrays stream through a pinned staging ring into the scene's device block on the
-// context's stream, and the scene's texel expansion, environment tables and BVH build run
-// on one of a few builder streams, so that the builds of different scenes overlap on the
-// GPU (each build alone is a chain of small, latency-bound launches).  The host waits once
-// for all builds, writes each scene's DevScene record, and waits once more.
+// scene first, in parallel (validation, derived arrays, light tables, the block's
+// layout); then each scene's arrays stream through a pinned staging ring into the scene's
+// device block on the context's stream, its texel expansion and environment tables run on
+// one of a few builder streams, and every kGroupScenes scenes one BVH build serves the
+// whole group (one chain of level launches instead of one per scene; a build alone is
+// latency-bound), overlapping the next groups' uploads.  The host waits once for all
+// builds, writes each scene's DevScene record, and waits once more.
 #include <algorithm>
 #include <cmath>
-#include <condition_variable>
 #include <cstring>
 #include <map>
-#include <mutex>
+#include <memory>
 #include <new>
-#include <thread>
 
 #include "fm_bvh.cuh"
 #include "fm_internal.h"
@@ -46,7 +45,6 @@ void launch_rgb_to_texels(cudaStream_t stream, const float* src, float4* dst, si
 namespace {
 
 constexpr int kBuildStreams = 16;   // scenes whose device work runs side by side
-constexpr int kIssuers = 1;         // threads issuing BVH builds (more did not shorten a batch: the builds' device time bounds it)
 constexpr size_t kAlign = 256;     // sub-array alignment inside a scene's block
 
 size_t align_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
@@ -193,8 +191,6 @@ struct SceneBuild {
     size_t rgb_bytes = 0;
     char* d_block = nullptr;
     char* d_rgb = nullptr;
-    BvhJob* job = nullptr;
-    int32_t* h_counters = nullptr;   // BVH build counters (pinned)
     // host arrays the pieces point into
     std::vector<int32_t> prim_obj, prim_info, obj_light, mtri, malias;
     std::vector<uint8_t> has_normal;
@@ -511,12 +507,13 @@ fm_status prepare_scene(const fm_scene_desc* d, SceneBuild& B)
 fm_status ensure_builder(fm_ctx* ctx)
 {
     if (ctx->build_streams.empty()) {
-        // streams: kBuildStreams run builds, kIssuers only capture their graphs; events:
-        // [0] a scene's arrays are on the device, [1 + k] builder stream k is done
+        // streams: kBuildStreams run device work, one more only captures the BVH build
+        // graphs; events: [0] a scene's arrays are on the device, [1 + k] builder stream k
+        // is done
         std::vector<cudaStream_t> streams;
         std::vector<cudaEvent_t> events;
         cudaError_t e = cudaSuccess;
-        for (int k = 0; k < kBuildStreams + kIssuers && e == cudaSuccess; ++k) {
+        for (int k = 0; k <= kBuildStreams && e == cudaSuccess; ++k) {
             cudaStream_t s = nullptr;
             e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
             if (e == cudaSuccess) streams.push_back(s);
@@ -531,8 +528,8 @@ fm_status ensure_builder(fm_ctx* ctx)
             for (cudaEvent_t ev : events) cudaEventDestroy(ev);
             return cuda_error(ctx, e, "scene builder streams");
         }
-        ctx->capture_streams.assign(streams.begin() + kBuildStreams, streams.end());
-        streams.resize(kBuildStreams);
+        ctx->capture_stream = streams.back();
+        streams.pop_back();
         ctx->build_streams = streams;
         ctx->build_events = events;
     }
@@ -540,17 +537,29 @@ fm_status ensure_builder(fm_ctx* ctx)
     return FM_OK;
 }
 
-// Frees every scene of a failed batch (after its device work has drained).
-void discard(fm_ctx* ctx, std::vector<SceneBuild>& builds)
+// A group of consecutive scenes whose BVHs are built together.
+struct Group {
+    int first = 0, count = 0;
+    BvhJob* job = nullptr;
+    BvhBatch bvh;
+    char* h_pinned = nullptr;
+};
+
+// Frees every scene of a failed batch, and the group builds (after the device work has
+// drained).
+void discard(fm_ctx* ctx, std::vector<SceneBuild>& builds, std::vector<Group>& groups)
 {
     for (cudaStream_t s : ctx->build_streams) cudaStreamSynchronize(s);
     cudaStreamSynchronize(ctx->stream);
+    for (Group& g : groups) {
+        if (g.job) bvh_build_abort(g.job, g.bvh);
+        g.job = nullptr;
+    }
     for (SceneBuild& B : builds) {
         if (!B.sc) continue;
-        if (B.job) bvh_build_abort(B.job, B.sc->bvh);
-        B.job = nullptr;
         if (B.d_rgb) cudaFreeAsync(B.d_rgb, ctx->stream);
         for (void* p : B.sc->allocations) cudaFreeAsync(p, ctx->stream);
+        B.sc->shared_bvh.reset();
         delete B.sc;
         B.sc = nullptr;
     }
@@ -558,78 +567,9 @@ void discard(fm_ctx* ctx, std::vector<SceneBuild>& builds)
     cudaGetLastError();
 }
 
-// Issues the BVH builds from threads of their own, scenes taken in hand-over order, as
-// the main thread hands them over; the host cost of a build (allocations, graph capture
-// and instantiation, about half a millisecond) then overlaps the main thread's uploads
-// and the other issuers' builds.  Each issuer captures on a stream of its own.
-class BvhIssuer {
-public:
-    BvhIssuer(fm_ctx* ctx, std::vector<SceneBuild>& builds) : ctx_(ctx), builds_(builds)
-    {
-        for (size_t t = 0; t < ctx->capture_streams.size(); ++t)
-            threads_.emplace_back([this, t] { loop(ctx_->capture_streams[t]); });
-    }
-    ~BvhIssuer() { finish(); }
-    void hand_over(int i, cudaStream_t s)
-    {
-        std::lock_guard<std::mutex> lk(m_);
-        queue_.push_back({i, s});
-        cv_.notify_one();
-    }
-    // Waits until every handed-over scene has been issued; returns false (with `err`) if
-    // one failed (the later ones are then not issued).
-    bool finish()
-    {
-        {
-            std::lock_guard<std::mutex> lk(m_);
-            closed_ = true;
-        }
-        cv_.notify_all();
-        for (auto& t : threads_)
-            if (t.joinable()) t.join();
-        return err_.empty();
-    }
-    const std::string& error() const { return err_; }
-
-private:
-    void loop(cudaStream_t capture)
-    {
-        cudaSetDevice(ctx_->device);
-        for (;;) {
-            std::pair<int, cudaStream_t> job;
-            {
-                std::unique_lock<std::mutex> lk(m_);
-                cv_.wait(lk, [&] { return closed_ || next_ < queue_.size(); });
-                if (next_ == queue_.size()) return;
-                job = queue_[next_++];
-                if (!err_.empty()) continue;
-            }
-            SceneBuild& B = builds_[(size_t)job.first];
-            const DevScene& S = B.sc->dev;
-            PrimSource src;
-            src.num_tris = S.num_tris;
-            src.num_rects = S.num_rects;
-            src.num_spheres = S.num_spheres;
-            src.tri_pos = S.tri_pos;
-            src.rects = S.rects;
-            src.spheres = S.spheres;
-            std::string err;
-            if (bvh_build_begin(job.second, capture, src, B.h_counters, ctx_->num_sms, B.job, B.sc->bvh, err) != 0) {
-                std::lock_guard<std::mutex> lk(m_);
-                if (err_.empty()) err_ = err.empty() ? std::string("bvh build failed") : err;
-            }
-        }
-    }
-    fm_ctx* ctx_;
-    std::vector<SceneBuild>& builds_;
-    std::vector<std::thread> threads_;
-    std::mutex m_;
-    std::condition_variable cv_;
-    std::vector<std::pair<int, cudaStream_t>> queue_;
-    size_t next_ = 0;
-    bool closed_ = false;
-    std::string err_;
-};
+// Scenes per BVH build: the builds of a batch's groups overlap the uploads of the later
+// groups, and each build serves all scenes of its group with one chain of launches.
+constexpr int kGroupScenes = 16;
 
 fm_status create_scenes(fm_ctx* ctx, int32_t n, const fm_scene_desc* const* descs, fm_scene** out)
 {
@@ -657,31 +597,47 @@ fm_status create_scenes(fm_ctx* ctx, int32_t n, const fm_scene_desc* const* desc
             }
         }
     }
-    if (ctx->build_counters_cap < n) {
-        if (ctx->build_counters) cudaFreeHost(ctx->build_counters);
-        ctx->build_counters = nullptr;
-        ctx->build_counters_cap = 0;
+    // groups and their pinned space (scene table and counters of each build)
+    std::vector<Group> groups;
+    size_t pinned = 0;
+    for (int32_t i = 0; i < n; i += kGroupScenes) {
+        Group g;
+        g.first = i;
+        g.count = std::min<int32_t>(kGroupScenes, n - i);
+        pinned += (bvh_batch_pinned_bytes(g.count) + 255) & ~size_t(255);
+        groups.push_back(g);
+    }
+    if (ctx->build_pinned_bytes < pinned) {
+        if (ctx->build_pinned) cudaFreeHost(ctx->build_pinned);
+        ctx->build_pinned = nullptr;
+        ctx->build_pinned_bytes = 0;
         void* p = nullptr;
-        const cudaError_t e = cudaHostAlloc(&p, sizeof(int32_t) * 16 * (size_t)n, cudaHostAllocDefault);
+        const cudaError_t e = cudaHostAlloc(&p, pinned, cudaHostAllocDefault);
         if (e != cudaSuccess) {
             for (SceneBuild& B : builds) delete B.sc;
-            return cuda_error(ctx, e, "scene build counters");
+            return cuda_error(ctx, e, "scene build staging");
         }
-        ctx->build_counters = static_cast<int32_t*>(p);
-        ctx->build_counters_cap = n;
+        ctx->build_pinned = static_cast<char*>(p);
+        ctx->build_pinned_bytes = pinned;
+    }
+    {
+        size_t off = 0;
+        for (Group& g : groups) {
+            g.h_pinned = ctx->build_pinned + off;
+            off += (bvh_batch_pinned_bytes(g.count) + 255) & ~size_t(255);
+        }
     }
     cudaStream_t cs = ctx->stream;
     Stager stager(ctx, cs);
     fm_status st = FM_OK;
-    BvhIssuer issuer(ctx, builds);
     auto fail = [&](fm_status code, const std::string& msg) {
-        issuer.finish();
-        discard(ctx, builds);
+        discard(ctx, builds, groups);
         return set_error(ctx, code, msg);
     };
     auto fail_cuda = [&](cudaError_t e, const char* where) {
         return fail(FM_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
     };
+    size_t next_group = 0;
     for (int32_t i = 0; i < n; ++i) {
         SceneBuild& B = builds[i];
         fm_scene* sc = B.sc;
@@ -733,25 +689,70 @@ fm_status create_scenes(fm_ctx* ctx, int32_t n, const fm_scene_desc* const* desc
             st = env_build_tables(ctx, bs, sc, sc->textures[S.env.tex], S.env);
             if (st != FM_OK) return fail(st, ctx->error);
         }
-        B.h_counters = ctx->build_counters + 16 * (size_t)i;
-        issuer.hand_over(i, bs);
+        // the group's last scene is on the device: build the group's BVHs on a builder
+        // stream while the next groups upload
+        Group& g = groups[next_group];
+        if (i == g.first + g.count - 1) {
+            ++next_group;
+            std::vector<PrimSource> srcs((size_t)g.count);
+            for (int k = 0; k < g.count; ++k) {
+                const DevScene& D = builds[(size_t)(g.first + k)].sc->dev;
+                PrimSource& p = srcs[(size_t)k];
+                p.num_tris = D.num_tris;
+                p.num_rects = D.num_rects;
+                p.num_spheres = D.num_spheres;
+                p.tri_pos = D.tri_pos;
+                p.rects = D.rects;
+                p.spheres = D.spheres;
+            }
+            cudaStream_t gs = ctx->build_streams[(next_group - 1) % ctx->build_streams.size()];
+            e = cudaStreamWaitEvent(gs, ctx->build_events[0], 0);
+            if (e != cudaSuccess) return fail_cuda(e, "scene build");
+            std::string err;
+            if (bvh_build_batch_begin(gs, ctx->capture_stream, srcs.data(), g.count, g.h_pinned, ctx->num_sms, g.job,
+                                      g.bvh, err) != 0)
+                return fail(FM_ERR_CUDA, err);
+        }
     }
-    if (!issuer.finish()) return fail(FM_ERR_CUDA, issuer.error());
     // wait for the builds; then every scene's record
-    for (int32_t i = 0; i < n; ++i) {
-        SceneBuild& B = builds[i];
-        fm_scene* sc = B.sc;
-        BvhJob* job = B.job;
-        B.job = nullptr;
+    for (Group& g : groups) {
+        BvhJob* job = g.job;
+        g.job = nullptr;
         std::string err;
-        if (bvh_build_end(job, sc->bvh, err) != 0) return fail(FM_ERR_CUDA, err);
-        if (sc->bvh.nodes) sc->allocations.push_back(sc->bvh.nodes);
-        if (sc->bvh.leaf) sc->allocations.push_back(sc->bvh.leaf);
-        DevScene& S = sc->dev;
-        S.nodes = sc->bvh.nodes;
-        S.leaf = sc->bvh.leaf;
-        S.num_nodes = sc->bvh.num_nodes;
-        S.num_leaf = sc->bvh.num_leaf;
+        if (bvh_build_batch_end(job, g.bvh, err) != 0) return fail(FM_ERR_CUDA, err);
+        // the group's arrays live until the last of its scenes is destroyed
+        std::shared_ptr<void> shared;
+        uint4* gnodes = g.bvh.nodes;
+        float4* gleaf = g.bvh.leaf;
+        if (gnodes) {
+            cudaStream_t fs = ctx->stream;
+            shared = std::shared_ptr<void>(gnodes, [gleaf, fs](void* p) {
+                cudaFreeAsync(p, fs);
+                cudaFreeAsync(gleaf, fs);
+            });
+            g.bvh.nodes = nullptr;
+            g.bvh.leaf = nullptr;
+        }
+        for (int k = 0; k < g.count; ++k) {
+            fm_scene* sc = builds[(size_t)(g.first + k)].sc;
+            DevScene& S = sc->dev;
+            const int r = g.bvh.root.empty() ? -1 : g.bvh.root[(size_t)k];
+            sc->bvh = BvhResult{};
+            sc->bvh.build_ms = g.bvh.build_ms;
+            if (r >= 0) {
+                sc->shared_bvh = shared;
+                S.nodes = gnodes + 5 * (size_t)r;
+                S.leaf = gleaf;
+                sc->bvh.num_nodes = g.bvh.num_nodes[(size_t)k];
+                sc->bvh.num_leaf = g.bvh.num_leaf[(size_t)k];
+                sc->bvh.depth = g.bvh.depth[(size_t)k];
+            } else {
+                S.nodes = nullptr;
+                S.leaf = nullptr;
+            }
+            S.num_nodes = sc->bvh.num_nodes;
+            S.num_leaf = sc->bvh.num_leaf;
+        }
     }
     for (size_t k = 0; k < ctx->build_streams.size(); ++k) {
         cudaError_t e = cudaEventRecord(ctx->build_events[1 + k], ctx->build_streams[k]);
@@ -780,13 +781,13 @@ void scene_builder_release(fm_ctx* ctx)
         cudaStreamDestroy(s);
     }
     for (cudaEvent_t e : ctx->build_events) cudaEventDestroy(e);
-    for (cudaStream_t s : ctx->capture_streams) cudaStreamDestroy(s);
-    ctx->capture_streams.clear();
+    if (ctx->capture_stream) cudaStreamDestroy(ctx->capture_stream);
+    ctx->capture_stream = nullptr;
     ctx->build_streams.clear();
     ctx->build_events.clear();
-    if (ctx->build_counters) cudaFreeHost(ctx->build_counters);
-    ctx->build_counters = nullptr;
-    ctx->build_counters_cap = 0;
+    if (ctx->build_pinned) cudaFreeHost(ctx->build_pinned);
+    ctx->build_pinned = nullptr;
+    ctx->build_pinned_bytes = 0;
 }
 
 }  // namespace fm
