@@ -569,7 +569,9 @@ void discard(fm_ctx* ctx, std::vector<SceneBuild>& builds, std::vector<Group>& g
 
 // Scenes per BVH build: the builds of a batch's groups overlap the uploads of the later
 // groups, and each build serves all scenes of its group with one chain of launches.
-constexpr int kGroupScenes = 16;
+// Creating the 64-scene batch with 8 / 16 / 32 / 64 scenes per build: 29-31 / 26-28 /
+// 23-24.5 / 28-29 ms.
+constexpr int kGroupScenes = 32;
 
 fm_status create_scenes(fm_ctx* ctx, int32_t n, const fm_scene_desc* const* descs, fm_scene** out)
 {
