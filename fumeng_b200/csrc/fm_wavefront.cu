@@ -51,12 +51,16 @@ constexpr int kReplay = 4;
 // queue counters: the three ray queues being filled for the next trace, the same three
 // being traced, slots still holding work, the shading queues (two classes, and in
 // adjoint renders two more for replayed vertices) and the trace kernel's next
-// unclaimed ray
-constexpr int kQcCont = 0, kQcMis = 1, kQcShadow = 2;
-constexpr int kQcTraceCont = 3, kQcTraceMis = 4, kQcTraceShadow = 5;
-constexpr int kQcActive = 6, kQcDisney = 7, kQcSimple = 8, kQcTraceNext = 9, kQcDisneyR = 10, kQcSimpleR = 11;
-constexpr int kQcGrad = 12, kQcBodies = 13;
-constexpr int kQcCount = 16;
+// unclaimed ray.  Each counter has a 128-byte line of its own: atomics from every warp
+// of the GPU on counters that share a line queue behind one another at the L2 (one
+// line for all of them cost 9 % of the batched step).
+constexpr int kQcLine = 32;
+constexpr int kQcCont = 0 * kQcLine, kQcMis = 1 * kQcLine, kQcShadow = 2 * kQcLine;
+constexpr int kQcTraceCont = 3 * kQcLine, kQcTraceMis = 4 * kQcLine, kQcTraceShadow = 5 * kQcLine;
+constexpr int kQcActive = 6 * kQcLine, kQcDisney = 7 * kQcLine, kQcSimple = 8 * kQcLine;
+constexpr int kQcTraceNext = 9 * kQcLine, kQcDisneyR = 10 * kQcLine, kQcSimpleR = 11 * kQcLine;
+constexpr int kQcGrad = 12 * kQcLine, kQcBodies = 13 * kQcLine;
+constexpr int kQcCount = 16 * kQcLine;
 
 struct WfState {
     int64_t pool;
@@ -99,6 +103,7 @@ struct WfState {
     uint32_t* sh_h;       // ... shadow ray occluded (1) or not (0)
     int64_t cap_cont, cap_mis, cap_sh;
     unsigned* qc;         // kQc* counters
+    int64_t trace_tail;   // rays from the end of the trace queues below which warps claim exactly what they need
     // trace kernel span of the current iteration (earliest block start, latest block
     // end, device global timer in ns) and the sum of the spans so far
     unsigned long long* tspan;
@@ -132,6 +137,40 @@ FM_D int64_t wagg_append(unsigned* counter, bool want)
     if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(counter, (unsigned)__popc(b));
     base = __shfl_sync(b, base, leader);
     return (int64_t)base + __popc(b & lanemask_lt());
+}
+
+// Block-aggregated append to one of NQ queues (which = -1: none), the queue k counted
+// by qc[ci[k]].  Every thread of the block calls it at the same point of block-uniform
+// control flow; `sh` is 2 * NQ words of shared memory.  One shared-memory atomic per warp
+// and queue and one global atomic per block and queue: appends from every warp of the
+// GPU to one counter wait on one another at the L2, so a hot queue is cheaper to fill a
+// block at a time.
+template <int NQ>
+FM_D int64_t block_append(unsigned* qc, const int* ci, int which, unsigned* sh)
+{
+    if (threadIdx.x < NQ) sh[threadIdx.x] = 0u;
+    __syncthreads();
+    unsigned local = 0;
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) {
+        const unsigned b = __ballot_sync(0xffffffffu, which == k);
+        if (b == 0u) continue;
+        const int leader = __ffs(b) - 1;
+        unsigned base = 0;
+        if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&sh[k], (unsigned)__popc(b));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (which == k) local = base + __popc(b & lanemask_lt());
+    }
+    __syncthreads();
+    if (threadIdx.x < NQ && sh[threadIdx.x]) {
+        int c = ci[0];
+#pragma unroll
+        for (int k = 1; k < NQ; ++k)
+            if ((int)threadIdx.x == k) c = ci[k];
+        sh[NQ + threadIdx.x] = atomicAdd(&qc[c], sh[threadIdx.x]);
+    }
+    __syncthreads();
+    return which < 0 ? -1 : (int64_t)sh[NQ + which] + local;
 }
 
 // wagg_append for call sites where lanes of one warp may reach the append with
@@ -459,10 +498,11 @@ FM_D int begin_ray(const WfState& st, int64_t idx, int64_t nc, int64_t nm, Trave
     return kRayShadow;
 }
 
-// A continuation ray's result: route the slot to the shading queue of the hit's material
-// class; a miss or a first-bounce emitter hit ends the path here.
+// A continuation ray's result: the shading queue the slot goes to by the hit's material
+// class (0 Disney, 1 other materials; 2 and 3 the same for vertices of adjoint renders
+// being replayed), or -1 when a miss or a first-bounce emitter hit ends the path here.
 template <bool ADJ>
-FM_D void finish_cont(const WfState& st, int64_t idx, const DevScene& S, const Hit& h)
+FM_D int finish_cont(const WfState& st, int64_t idx, const DevScene& S, const Hit& h)
 {
     const int cslot = st.cont_q[idx];
     const int cflags = st.flags[cslot];
@@ -493,18 +533,8 @@ FM_D void finish_cont(const WfState& st, int64_t idx, const DevScene& S, const H
     }
     // replayed vertices of an adjoint render go to their own queues, so that primal
     // vertices run in the forward shading kernels
-    // (one warp-aggregated append per queue: all lanes take part in each)
-    const bool rep = ADJ && (cflags & kReplay);
-    const int64_t qd = wagg_append(&st.qc[kQcDisney], cls == kClsDisney && !rep);
-    if (cls == kClsDisney && !rep) st.disney_q[qd] = cslot;
-    const int64_t qs = wagg_append(&st.qc[kQcSimple], cls == kClsSimple && !rep);
-    if (cls == kClsSimple && !rep) st.simple_q[qs] = cslot;
-    if (ADJ) {
-        const int64_t rd = wagg_append(&st.qc[kQcDisneyR], cls == kClsDisney && rep);
-        if (cls == kClsDisney && rep) st.disney_r[rd] = cslot;
-        const int64_t rs = wagg_append(&st.qc[kQcSimpleR], cls == kClsSimple && rep);
-        if (cls == kClsSimple && rep) st.simple_r[rs] = cslot;
-    }
+    if (cls < 0) return -1;
+    return ADJ && (cflags & kReplay) ? cls + 2 : cls;
 }
 
 // An MIS-BSDF ray's result: the emitter (or environment) it reaches, MIS-weighted.
@@ -615,6 +645,11 @@ FM_D void finish_shadow(const WfState& st, int64_t q, const DevScene& S, const H
 // 253.2 / 251.9 / 255.9 / 256.5 -- the shared memory taken from the L1 cache that holds
 // the nodes offsets what the stack saves beyond a few entries.
 constexpr int kTraceSmemStack = 4;
+// Rays a warp claims from the combined index space at once (one atomic per claim instead
+// of one per refill; its lanes then take the rays in order).  Within trace_tail rays of the
+// end, warps claim exactly what their lanes need, so that no warp holds back rays while
+// others run dry.
+constexpr unsigned kTraceChunk = 64;
 
 __global__ void __launch_bounds__(256, 4) k_wf_trace(WfState st)
 {
@@ -631,17 +666,35 @@ __global__ void __launch_bounds__(256, 4) k_wf_trace(WfState st)
     int64_t idx = 0;
     bool exhausted = false;
     const int lane = threadIdx.x & 31;
+    // the warp's claimed part of the combined index space, [cur, cend) (warp-uniform)
+    unsigned cur = 0, cend = 0;
+    bool chunk = st.trace_tail < total;
     if (threadIdx.x == 0) atomicMin(&st.tspan[0], global_ns());
     for (;;) {
         const bool need = kind < 0 && !exhausted;
         const unsigned m = __ballot_sync(0xffffffffu, need);
         if (m) {
-            const int leader = __ffs(m) - 1;
-            unsigned base = 0;
-            if (lane == leader) base = atomicAdd(&st.qc[kQcTraceNext], (unsigned)__popc(m));
-            base = __shfl_sync(0xffffffffu, base, leader);
+            // lanes take rays from the warp's claimed range first, in lane order
+            const unsigned n = (unsigned)__popc(m);
+            const unsigned have = cend - cur;
+            const unsigned r = (unsigned)__popc(m & lanemask_lt());
+            if (have < n) {
+                // claim a new range: a whole chunk while far from the end of the
+                // queues, exactly the lanes' shortfall near it
+                const unsigned take = chunk ? kTraceChunk : n - have;
+                const int leader = __ffs(m) - 1;
+                unsigned base = 0;
+                if (lane == leader) base = atomicAdd(&st.qc[kQcTraceNext], take);
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (chunk && (int64_t)base + st.trace_tail >= total) chunk = false;
+                if (need) idx = r < have ? (int64_t)cur + r : (int64_t)base + (r - have);
+                cur = base + (n - have);
+                cend = base + take;
+            } else {
+                if (need) idx = (int64_t)cur + r;
+                cur += n;
+            }
             if (need) {
-                idx = (int64_t)base + __popc(m & lanemask_lt());
                 if (idx >= total)
                     exhausted = true;
                 else
@@ -676,17 +729,32 @@ __global__ void __launch_bounds__(256) k_wf_resolve(WfState st)
     const int64_t total = nc + nm + ns;
     if (blockIdx.x == 0 && threadIdx.x == 0 && st.tspan[1] > st.tspan[0]) st.tspan[2] += st.tspan[1] - st.tspan[0];
     unsigned long long n_closest = 0, n_shadow = 0;
+    constexpr int NQ = ADJ ? 4 : 2;
+    __shared__ unsigned s_app[2 * NQ];
+    const int shade_qc[4] = {kQcDisney, kQcSimple, kQcDisneyR, kQcSimpleR};
     for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < total; i0 += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = i0 + threadIdx.x;
+        if (i0 < nc) {
+            // continuation results (block-uniform branch): shading-queue appends
+            // aggregated over the block
+            int which = -1, slot = 0;
+            if (i < nc) {
+                ++n_closest;
+                slot = st.cont_q[i];
+                const float4 h4 = st.cont_h[i];
+                const int vid = st.cont_v[i];
+                st.hit[slot] = h4;   // the shading kernels read it by slot
+                which = finish_cont<ADJ>(st, i, *st.views[vid].scene, Hit{h4.x, __float_as_int(h4.y), h4.z, h4.w});
+            }
+            const int64_t q = block_append<NQ>(st.qc, shade_qc, which, s_app);
+            if (which >= 0) {
+                int32_t* const queue = which == 0 ? st.disney_q : which == 1 ? st.simple_q : which == 2 ? st.disney_r : st.simple_r;
+                queue[q] = slot;
+            }
+            if (i < nc) continue;
+        }
         if (i >= total) continue;
-        if (i < nc) {
-            ++n_closest;
-            const int slot = st.cont_q[i];
-            const float4 h4 = st.cont_h[i];
-            const int vid = st.cont_v[i];
-            st.hit[slot] = h4;   // the shading kernels read it by slot
-            finish_cont<ADJ>(st, i, *st.views[vid].scene, Hit{h4.x, __float_as_int(h4.y), h4.z, h4.w});
-        } else if (i < nc + nm) {
+        if (i < nm + nc) {
             ++n_closest;
             const int64_t q = i - nc;
             const float4 h4 = st.mis_h[q];
@@ -774,6 +842,8 @@ FM_D void shade_vertices(const WfState& st)
     const int64_t n = st.qc[CLS == kClsDisney ? (ADJ ? kQcDisneyR : kQcDisney) : (ADJ ? kQcSimpleR : kQcSimple)];
     const int32_t* queue = CLS == kClsDisney ? (ADJ ? st.disney_r : st.disney_q) : (ADJ ? st.simple_r : st.simple_q);
     unsigned long long n_bounces = 0;
+    __shared__ unsigned s_app[2];
+    const int cont_qc = kQcCont;
     for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = i0 + threadIdx.x;
         const bool valid = i < n;
@@ -1005,7 +1075,7 @@ FM_D void shade_vertices(const WfState& st)
             st.rng[slot] = rng.state;
             st.flags[slot] = flags;
         }
-        const int64_t q = wagg_append(&st.qc[kQcCont], enqueue_cont);
+        const int64_t q = block_append<1>(st.qc, &cont_qc, enqueue_cont ? 0 : -1, s_app);
         if (enqueue_cont) {
             if (q < st.cap_cont)
                 st.cont_q[q] = slot;
@@ -1043,6 +1113,8 @@ __global__ void __launch_bounds__(256) k_wf_logic(WfState st)
 {
     unsigned long long n_paths = 0, n_nans = 0;
     unsigned n_active = 0;
+    __shared__ unsigned s_app[2];
+    const int cont_qc = kQcCont;
     for (int64_t s0 = blockIdx.x * (int64_t)blockDim.x; s0 < st.pool; s0 += (int64_t)gridDim.x * blockDim.x) {
         const int64_t s64 = s0 + threadIdx.x;
         const int slot = (int)s64;
@@ -1144,7 +1216,7 @@ __global__ void __launch_bounds__(256) k_wf_logic(WfState st)
             }
         }
         if (enqueue_cont) start_sample(st, slot, st.views[s_vid], s_local, s_k, s_flags);
-        const int64_t q = wagg_append(&st.qc[kQcCont], enqueue_cont);
+        const int64_t q = block_append<1>(st.qc, &cont_qc, enqueue_cont ? 0 : -1, s_app);
         if (enqueue_cont) {
             if (q < st.cap_cont)
                 st.cont_q[q] = slot;
@@ -1449,6 +1521,7 @@ fm_status run_wavefront(fm_ctx* ctx, const std::vector<WfView>& views_in, const 
         st.cap_sh = std::min<int64_t>(st.cap_sh, tune.queue_limit);
     }
     st.views = c->d_views;
+    st.trace_tail = (int64_t)ctx->num_sms * 64 * kTraceChunk;   // 64 resident warps per SM at most
     st.cnt = c->cnt;
     st.status = ctx->d_status;
     if (ADJ) {
