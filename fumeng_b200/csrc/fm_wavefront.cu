@@ -79,7 +79,8 @@ struct WfState {
     float4* ro;
     float4* rd;
     float4* hit;
-    float4* acc;          // MIS, shadow and emission contributions (atomic adds from the trace kernel)
+    float4* acc;          // adjoint renders: the iteration's MIS, shadow and emission contributions
+                          // (atomic adds from the resolve kernel; forward renders add them to col)
     float4* isum;
     float4* icomp;
     float4* asum;
@@ -191,6 +192,13 @@ FM_D int64_t wagg_append_grouped(unsigned* counter, bool want)
 
 // One vector atomic (each component added atomically) instead of three scalar ones.
 FM_D void acc_add(float4* a, f3 c) { atomicAdd(a, make_float4(c.x, c.y, c.z, 0.0f)); }
+
+// Where hit resolution adds a slot's radiance contributions: the sample's radiance col
+// itself in forward renders; in adjoint renders the iteration's accumulator acc, which
+// the logic kernel adds to col (the replay reads the radiance before this iteration's
+// contributions).
+template <bool ADJ>
+FM_D float4* rad_acc(const WfState& st, int slot) { return ADJ ? &st.acc[slot] : &st.col[slot]; }
 
 FM_D int find_view(const WfState& st, int64_t item)
 {
@@ -517,7 +525,7 @@ FM_D int finish_cont(const WfState& st, int64_t idx, const DevScene& S, const Hi
         // the camera ray's beta is 1
         if (depth == 1 && S.env_light >= 0) {
             const f3 d = ray_dir();
-            acc_add(&st.acc[cslot], env_radiance(S, d));
+            acc_add(rad_acc<ADJ>(st, cslot), env_radiance(S, d));
             if (ADJ && (cflags & kReplay)) scatter_env(st, S, d, pixel_delta(st, cslot, st.views[st.view[cslot]]));
         }
     } else {
@@ -526,7 +534,7 @@ FM_D int finish_cont(const WfState& st, int64_t idx, const DevScene& S, const Hi
         if (li >= 0) {
             const float4 o4 = st.ro[cslot];
             const HitInfo lh = make_hit(S, f3{o4.x, o4.y, o4.z}, ray_dir(), h);
-            if (dot(lh.ng, lh.wo) > 0) acc_add(&st.acc[cslot], ld3(S.lights[li].radiance));
+            if (dot(lh.ng, lh.wo) > 0) acc_add(rad_acc<ADJ>(st, cslot), ld3(S.lights[li].radiance));
         } else {
             cls = (info & 3) - 1;
         }
@@ -576,7 +584,7 @@ FM_D void finish_mis(const WfState& st, int64_t q, const DevScene& S, const Hit&
         }
     }
     if (c.x == 0.0f && c.y == 0.0f && c.z == 0.0f) return;
-    acc_add(&st.acc[slot], c);
+    acc_add(rad_acc<ADJ>(st, slot), c);
     // only rays of replayed vertices carry a gradient payload
     if (ADJ && (st.flags[slot] & kReplay)) {
         const float4* P = st.mis_g + 8 * q;
@@ -614,7 +622,7 @@ FM_D void finish_shadow(const WfState& st, int64_t q, const DevScene& S, const H
     if (h.prim >= 0) return;
     const float4 d4 = st.sh_d[q], c4 = st.sh_c[q];
     const int slot = __float_as_int(d4.w);
-    acc_add(&st.acc[slot], f3{c4.x, c4.y, c4.z});
+    acc_add(rad_acc<ADJ>(st, slot), f3{c4.x, c4.y, c4.z});
     if (ADJ && (st.flags[slot] & kReplay)) {
         const float4* P = st.sh_g + 3 * q;
         const float4 p1 = P[1], p2 = P[2];
@@ -1128,13 +1136,23 @@ __global__ void __launch_bounds__(256) k_wf_logic(WfState st)
         int s_vid = 0, s_k = 0, s_flags = 0;
         int64_t s_local = 0;
         if (item >= 0) {
-            const float4 a4 = st.acc[slot];
-            const float4 c4 = st.col[slot];
-            const f3 col = f3{c4.x + a4.x, c4.y + a4.y, c4.z + a4.z};
-            if (a4.x != 0.0f || a4.y != 0.0f || a4.z != 0.0f) st.acc[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             const int flags = st.flags[slot];
-            if (flags & (kNextCont | kPending)) {
-                st.col[slot] = make_float4(col.x, col.y, col.z, 0.0f);
+            const bool cont = (flags & (kNextCont | kPending)) != 0;
+            // the sample's radiance so far: forward renders add contributions to col
+            // directly, adjoint renders collect this iteration's in acc (the replay needs
+            // the radiance before them), added to col here
+            f3 col = mk(0.0f);
+            if (ADJ) {
+                const float4 a4 = st.acc[slot];
+                const float4 c4 = st.col[slot];
+                col = f3{c4.x + a4.x, c4.y + a4.y, c4.z + a4.z};
+                if (a4.x != 0.0f || a4.y != 0.0f || a4.z != 0.0f) st.acc[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            } else if (!cont) {
+                const float4 c4 = st.col[slot];
+                col = f3{c4.x, c4.y, c4.z};
+            }
+            if (cont) {
+                if (ADJ) st.col[slot] = make_float4(col.x, col.y, col.z, 0.0f);
                 st.flags[slot] = flags & ~(kNextCont | kPending);
                 alive = true;
             } else if (ADJ && !(flags & kReplay)) {
