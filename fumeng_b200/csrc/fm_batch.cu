@@ -94,9 +94,14 @@ fm_status autotune(fm_ctx* ctx, int32_t n, const fm_scene* const* scenes, const 
         imgs[i] = buf + off;
         off += (size_t)out_width(params[i]) * out_height(params[i]) * 3;
     }
-    // trial renders at up to 8 spp: enough samples per view that the pool's refill tail
-    // does not dominate the trial (at 2 spp it favoured small pools)
-    const std::vector<WfView> views = make_views(n, scenes, cams, params, imgs.data(), nullptr, nullptr, 8);
+    // Trial renders of the batch itself when it has at most 2^28 samples (a trial then
+    // takes well under a second), else at up to 8 spp per view.  The best pool depends
+    // on the samples a render has: at 8 spp the 64-scene batch favoured 2^23 slots, its
+    // full render 2^25 (302 against 349 ms); at 2 spp it favoured smaller pools still.
+    double full_samples = 0.0;
+    for (int i = 0; i < n; ++i) full_samples += (double)out_width(params[i]) * out_height(params[i]) * params[i].spp;
+    const int trial_spp = full_samples <= (double)(1 << 28) ? 0 : 8;
+    const std::vector<WfView> views = make_views(n, scenes, cams, params, imgs.data(), nullptr, nullptr, trial_spp);
     double samples = 0.0;
     for (const auto& v : views) samples += (double)v.cfg.width * v.cfg.height * v.cfg.spp;
     fm_tuning best{(int64_t)1 << 21, 128, 128, 8, 0, 0};
@@ -119,13 +124,28 @@ fm_status autotune(fm_ctx* ctx, int32_t n, const fm_scene* const* scenes, const 
         }
         return FM_OK;
     };
+    // Pools up to 2^25 slots: on the 64-scene batch (250 M paths) a render ran 368 /
+    // 333 / 302 / 307 ms at 2^22 / 2^24 / 2^25 / 2^26 slots -- a larger pool means fewer
+    // wavefront iterations, so fewer launches and fewer kernel tails.  A candidate's
+    // workspace (about 284 B plus 52 B per light and direct-lighting round per slot) must
+    // fit in half of the device memory free now.
+    int max_rays = 1;
+    for (const auto& v : views) max_rays = std::max(max_rays, v.num_lights * v.cfg.direct_loop);
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        free_b = 0;
+    }
+    const double slot_bytes = 284.0 + 52.0 * max_rays + 64.0;
+    const double pool_cap = 0.5 * (double)free_b / slot_bytes;
     // warm-up, then coordinate descent over pool size, trace block, shade block, graph depth
     st = trial(best);
     best_rate = -1.0;
-    const int64_t pools[] = {(int64_t)1 << 19, (int64_t)1 << 20, (int64_t)1 << 21, (int64_t)1 << 22};
+    const int64_t pools[] = {(int64_t)1 << 19, (int64_t)1 << 20, (int64_t)1 << 21, (int64_t)1 << 22,
+                             (int64_t)1 << 23, (int64_t)1 << 24, (int64_t)1 << 25};
     for (int64_t p : pools) {
         if (st != FM_OK) break;
-        if ((double)p > samples * 2.0 && p != pools[0]) continue;
+        if (((double)p > samples * 2.0 || (double)p > pool_cap) && p != pools[0]) continue;
         fm_tuning t = best;
         t.pool = p;
         st = trial(t);

@@ -294,8 +294,11 @@ fm_status fm_render_batch(fm_ctx* ctx, int32_t n, const fm_scene* const* scenes,
                           float* const* normal, int32_t flags, const fm_tuning* tuning, fm_render_stats* stats);
 
 /* Replaces: nothing in the reference (its thread pool has no knobs beyond thread_count).
- * Times candidate tunings on a reduced copy of the batch (spp 1) and returns the fastest;
- * the result is cached in the context for the batch's shape class. */
+ * Times candidate tunings by coordinate descent -- path-slot pools of 2^19 to 2^25 slots
+ * (those whose workspace fits in half of the free device memory), trace and shade block
+ * sizes, iterations per graph -- on trial renders of the batch itself when it has at most
+ * 2^28 samples, else of a copy at up to 8 spp per view, and returns the fastest; the
+ * result is cached in the context for the batch's shape class. */
 fm_status fm_autotune_batch(fm_ctx* ctx, int32_t n, const fm_scene* const* scenes, const fm_camera* cameras,
                             const fm_render_params* params, fm_tuning* out);
 
