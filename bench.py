@@ -47,8 +47,8 @@ WORKLOAD = "batched: 64 scenes x (1-40 displaced icosphere/box meshes, 1k-200k t
 NSCENES = 64
 # DRAM bytes the trace kernel moves per traced ray (read + write, cold L2 at each
 # launch), from an ncu capture of two trace launches of the 8-scene case of this
-# workload (69.0 and 64.0 B per ray); traffic grows with the rays a launch traces.
-TRACE_DRAM_BYTES_PER_RAY = 66.5
+# workload (68.8 and 63.1 B per ray); traffic grows with the rays a launch traces.
+TRACE_DRAM_BYTES_PER_RAY = 66.0
 
 
 def measured_peak_hbm():
