@@ -511,9 +511,12 @@ def main():
         h2d = sum(desc_bytes(h) for h in holders)
         d2h = sum(p.width * p.height * 3 * 4 for p in params_wf)
 
+        # the host images are allocated once and written by every step's read-back
+        host_rgb = [np.empty(p.out_shape() + (3,), np.float32) for p in params_wf]
+
         def step_e2e():
             sc = ctx.create_scenes(holders)
-            ctx.render_batch(sc, cams, params_wf, tuning=tuning)
+            ctx.render_batch(sc, cams, params_wf, tuning=tuning, out=host_rgb)
             for s in sc:
                 s.destroy()
         step_e2e()

@@ -227,11 +227,15 @@ class Context:
         return n, sc, ca, pa
 
     def render_batch(self, scenes, cams, params, want_aov: bool = False, tuning: Tuning | None = None,
-                     device_outputs=None, profile: bool = False):
+                     device_outputs=None, profile: bool = False, out=None):
         """Render view i = (scenes[i], cams[i], params[i]) for all i in one call.
 
         device_outputs: optional list of device pointers (ints) for the rgb images, which
-        makes the call skip the device-to-host copies (FM_FLAG_DEVICE_PTRS)."""
+        makes the call skip the device-to-host copies (FM_FLAG_DEVICE_PTRS).
+        out: optional list of host arrays for the rgb images (float32, C-contiguous, of
+        shape params[i].out_shape() + (3,)), written in place and returned; a caller that
+        renders repeatedly passes the same arrays each time instead of having new ones
+        allocated (and their pages faulted in by the copies) on every call."""
         n, sc, ca, pa = self._batch_args(scenes, cams, params)
         stats = RenderStats()
         tp = C.byref(tuning) if tuning is not None else None
@@ -240,7 +244,17 @@ class Context:
             flags = FM_FLAG_DEVICE_PTRS | (FM_FLAG_PROFILE if profile else 0)
             self.check(self.lib.fm_render_batch(self.h, n, sc, ca, pa, rgb_p, None, None, flags, tp, C.byref(stats)))
             return None, None, None, stats
-        rgb = [np.empty(p.out_shape() + (3,), np.float32) for p in params]
+        if out is not None:
+            if len(out) != n:
+                raise ValueError(f"out holds {len(out)} arrays for {n} views")
+            for a, p in zip(out, params):
+                if (not isinstance(a, np.ndarray) or a.dtype != np.float32 or not a.flags.c_contiguous
+                        or not a.flags.writeable or a.shape != p.out_shape() + (3,)):
+                    raise ValueError("out arrays must be writeable C-contiguous float32 arrays of shape "
+                                     "out_shape() + (3,)")
+            rgb = list(out)
+        else:
+            rgb = [np.empty(p.out_shape() + (3,), np.float32) for p in params]
         alb = [np.empty(p.out_shape() + (3,), np.float32) for p in params] if want_aov else None
         nrm = [np.empty(p.out_shape() + (3,), np.float32) for p in params] if want_aov else None
         rgb_p = (C.c_void_p * n)(*[a.ctypes.data for a in rgb])

@@ -49,3 +49,28 @@ def test_reused_workspace_matches_fresh_context():
     for g, a2, r in zip(got, again, ref):
         assert np.all(np.isfinite(g))
         assert _close(g, r) > 0.97 and _close(a2, r) > 0.97
+
+
+@pytest.mark.gpu
+def test_caller_owned_host_images_are_written_in_place(ctx):
+    """render_batch(out=...) writes the read-back into the caller's arrays (reused across
+    calls) and gives the same images as arrays the call allocates itself."""
+    specs = [synth.material_scene(1, res=48), synth.material_scene(2, res=32)]
+    scenes = [ctx.create_scene(s.to_desc()) for s in specs]
+    try:
+        cams = [s.camera_struct() for s in specs]
+        params = [s.render_params(spp=16, seed=3, mode=fb.FM_MODE_WAVEFRONT) for s in specs]
+        ref, _, _, _ = ctx.render_batch(scenes, cams, params)
+        out = [np.full(p.out_shape() + (3,), np.nan, np.float32) for p in params]
+        for _ in range(2):
+            got, _, _, _ = ctx.render_batch(scenes, cams, params, out=out)
+            assert all(g is o for g, o in zip(got, out))
+            for o, r in zip(out, ref):
+                assert np.all(np.isfinite(o)) and _close(o, r) > 0.97
+        with pytest.raises(ValueError):
+            ctx.render_batch(scenes, cams, params, out=out[:1])
+        with pytest.raises(ValueError):
+            ctx.render_batch(scenes, cams, params, out=[out[0].astype(np.float64), out[1]])
+    finally:
+        for sc in scenes:
+            sc.destroy()
