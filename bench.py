@@ -18,7 +18,8 @@ roofline: the trace kernel's algorithmic bytes (fixed per-ray formula, live ray 
          the render runs as one conditional CUDA graph, which admits no event nodes).
 e2e    : the same metric through the C-ABI from host memory: every step creates the 64
          scenes from host descriptors in one fm_scene_create_batch call (upload + device
-         BVH builds + env tables), renders into host images and destroys the scenes.
+         BVH builds + env tables), renders and reads the images back into host arrays
+         (allocated once, written by every step) and destroys the scenes.
 The plain per-pixel megakernel is timed on the same batch for comparison, and the
 path-replay adjoint against its own forward pass on the inverse-rendering workload
 (fumeng_b200.synth.inverse_scene: 120k triangles, 512^2 basecolor and roughness /

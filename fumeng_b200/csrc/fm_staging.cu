@@ -33,7 +33,7 @@ public:
     int size() const { return (int)threads_.size() + 1; }
 
     // Runs fn(0 .. tasks-1) on the workers and the caller; returns when every task is done
-    // and no worker is still inside this round.
+    // and no worker is still inside this call's task loop.
     void run(int tasks, const std::function<void(int)>& fn)
     {
         {
